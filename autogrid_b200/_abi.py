@@ -1,0 +1,125 @@
+"""ctypes mirror of include/autogrid_b200.h (the C ABI).
+
+Structure layouts and function signatures here must match the header; the
+test-suite checks that every function the header declares is exported by the
+library and bound here.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "_build" / "libautogrid_b200.so"
+
+AG_A_DIV = 128
+AG_NEINT = 1024
+AG_NDIEL = 8192
+AG_MAX_MAPS = 128
+AG_MAX_REC_TYPES = 20
+AG_MAX_ATOMS = 100000
+AG_MAX_GRID_PTS = 1025
+
+AG_OK = 0
+STATUS_NAMES = {
+    0: "AG_OK", 1: "AG_ERR_INVALID", 2: "AG_ERR_FATAL_INPUT", 3: "AG_ERR_NO_CLOSEST_H",
+    4: "AG_ERR_UNSUPPORTED", 5: "AG_ERR_CUDA", 6: "AG_ERR_NO_DEVICE", 7: "AG_ERR_TOO_LARGE",
+    8: "AG_ERR_IO", 9: "AG_ERR_TIMEOUT",
+}
+AG_PREC_FP32 = 0
+AG_PREC_FP64 = 1
+AG_TABLE_NEAREST = 0
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int32)
+_fp = C.POINTER(C.c_float)
+_u8p = C.POINTER(C.c_uint8)
+
+
+class ag_problem(C.Structure):
+    _fields_ = [
+        ("n_atoms", C.c_int32),
+        ("coord", _dp), ("charge", _dp), ("vol", _dp), ("solpar", _dp),
+        ("rec_type", _ip), ("hbond", _ip), ("rexp", _ip),
+        ("rvector", _dp), ("rvector2", _dp), ("disorder", _u8p),
+        ("n1", C.c_int32 * 3), ("ne", C.c_int32 * 3), ("spacing", C.c_double),
+        ("n_rec_types", C.c_int32), ("n_atom_maps", C.c_int32), ("n_maps", C.c_int32),
+        ("elec_map", C.c_int32), ("dsolv_map", C.c_int32),
+        ("map_is_covalent", _ip), ("map_is_hbonder", _ip), ("map_hbond", _ip),
+        ("map_solpar_probe", _dp), ("map_vol_probe", _dp),
+        ("e_vdw_hb", _fp), ("sol_fn", _dp), ("r_epsilon_fn", _dp),
+        ("dddiel", C.c_int32), ("invdielcal", C.c_double), ("coeff_estat", C.c_double),
+        ("solpar_q", C.c_double), ("disorder_h", C.c_int32), ("hydrogen_type", C.c_int32),
+        ("separate_desolvation_maps", C.c_int32),
+        ("cov_pos", C.c_double * 3), ("cov_half_width", C.c_double), ("cov_barrier", C.c_double),
+        ("floating_grid", C.c_int32), ("constriction_grid", C.c_int32),
+        ("constriction_cutoff", C.c_double),
+    ]
+
+
+class ag_opts(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("table_mode", C.c_int32), ("reserved", C.c_int32 * 6)]
+
+
+class ag_stats(C.Structure):
+    _fields_ = [("near_pairs", C.c_int64), ("fp64_fallbacks", C.c_int64), ("far_pairs", C.c_int64),
+                ("gpu_launches", C.c_int32), ("reserved", C.c_int32), ("kernel_ms", C.c_double),
+                ("far_ms", C.c_double)]
+
+
+# name -> (restype, argtypes); every entry point declared in include/autogrid_b200.h
+SIGNATURES = {
+    "ag_last_error": (C.c_char_p, []),
+    "ag_abi_version": (C.c_int32, []),
+    "ag_context_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
+    "ag_context_destroy": (C.c_int, [C.c_void_p]),
+    "ag_context_stats": (C.c_int, [C.c_void_p, C.POINTER(ag_stats)]),
+    "ag_maps_compute": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_void_p]),
+    "ag_maps_compute_f64": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_void_p]),
+    "ag_plan_create": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),
+    "ag_plan_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_plan_device_maps": (C.c_void_p, [C.c_void_p]),
+    "ag_plan_points": (C.c_size_t, [C.c_void_p]),
+    "ag_plan_download": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_plan_destroy": (C.c_int, [C.c_void_p]),
+    "ag_job_load": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
+    "ag_job_problem": (C.POINTER(ag_problem), [C.c_void_p]),
+    "ag_job_write_maps_f32": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_job_write_maps_f64": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_job_fail": (None, [C.c_void_p, C.c_char_p]),
+    "ag_job_free": (None, [C.c_void_p]),
+}
+
+_lib = None
+
+
+def load_library(path: Path | None = None) -> C.CDLL:
+    """Load the native library; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(
+            f"autogrid_b200 native library missing at {p}; build it with `python -m autogrid_b200.build`")
+    lib = C.CDLL(str(p))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+class AutoGridError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+def check(status: int) -> None:
+    if status != AG_OK:
+        msg = load_library().ag_last_error()
+        raise AutoGridError(status, msg.decode() if msg else "")

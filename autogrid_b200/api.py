@@ -1,0 +1,281 @@
+"""Python host API over the C ABI.
+
+Mirrors the reference's one operation -- `autogrid4 -p x.gpf -l x.glg`
+(main.cpp:214-3582) -- as `run_gpf()`, and exposes its hot path
+(main.cpp:2805-3464) as `Context.compute()` on a `Problem`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _abi
+from ._abi import AutoGridError, ag_opts, ag_problem, ag_stats, check, load_library
+
+_PREC = {"fp32": _abi.AG_PREC_FP32, "fp64": _abi.AG_PREC_FP64}
+
+
+def _ptr(a: np.ndarray | None, ctype):
+    if a is None:
+        return C.cast(None, C.POINTER(ctype))
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+class Problem:
+    """Owner of the numpy arrays behind one ag_problem.
+
+    Build it from a loaded GPF job (`Job.problem()`), or from arrays.  Array
+    names and meaning follow include/autogrid_b200.h.
+    """
+
+    ARRAYS = {
+        "coord": np.float64, "charge": np.float64, "vol": np.float64, "solpar": np.float64,
+        "rec_type": np.int32, "hbond": np.int32, "rexp": np.int32, "rvector": np.float64,
+        "rvector2": np.float64, "disorder": np.uint8, "map_is_covalent": np.int32,
+        "map_is_hbonder": np.int32, "map_hbond": np.int32, "map_solpar_probe": np.float64,
+        "map_vol_probe": np.float64, "e_vdw_hb": np.float32, "sol_fn": np.float64,
+        "r_epsilon_fn": np.float64,
+    }
+    SCALARS = ("n_rec_types", "n_atom_maps", "n_maps", "elec_map", "dsolv_map", "spacing", "dddiel",
+               "invdielcal", "coeff_estat", "solpar_q", "disorder_h", "hydrogen_type",
+               "separate_desolvation_maps", "cov_half_width", "cov_barrier", "floating_grid",
+               "constriction_grid", "constriction_cutoff")
+
+    def __init__(self, **kw):
+        self.arrays = {}
+        for name, dt in self.ARRAYS.items():
+            v = kw.get(name)
+            self.arrays[name] = None if v is None else np.ascontiguousarray(np.asarray(v, dtype=dt))
+        self.n1 = tuple(int(v) for v in kw["n1"])
+        self.ne = tuple(int(v) for v in kw.get("ne", [(n - 1) // 2 for n in self.n1]))
+        self.scalars = {k: kw[k] for k in self.SCALARS if k in kw}
+        self.cov_pos = tuple(float(v) for v in kw.get("cov_pos", (0.0, 0.0, 0.0)))
+        self.n_atoms = 0 if self.arrays["charge"] is None else int(self.arrays["charge"].shape[0])
+        self._struct = None
+
+    @property
+    def n_maps(self) -> int:
+        return int(self.scalars["n_maps"])
+
+    @property
+    def points(self) -> int:
+        return self.n1[0] * self.n1[1] * self.n1[2]
+
+    @property
+    def map_shape(self) -> tuple:
+        return (self.n_maps, self.n1[2], self.n1[1], self.n1[0])
+
+    def struct(self) -> ag_problem:
+        a = self.arrays
+        s = ag_problem()
+        s.n_atoms = self.n_atoms
+        s.coord = _ptr(a["coord"], C.c_double)
+        s.charge = _ptr(a["charge"], C.c_double)
+        s.vol = _ptr(a["vol"], C.c_double)
+        s.solpar = _ptr(a["solpar"], C.c_double)
+        s.rec_type = _ptr(a["rec_type"], C.c_int32)
+        s.hbond = _ptr(a["hbond"], C.c_int32)
+        s.rexp = _ptr(a["rexp"], C.c_int32)
+        s.rvector = _ptr(a["rvector"], C.c_double)
+        s.rvector2 = _ptr(a["rvector2"], C.c_double)
+        s.disorder = _ptr(a["disorder"], C.c_uint8)
+        for i in range(3):
+            s.n1[i] = self.n1[i]
+            s.ne[i] = self.ne[i]
+            s.cov_pos[i] = self.cov_pos[i]
+        s.map_is_covalent = _ptr(a["map_is_covalent"], C.c_int32)
+        s.map_is_hbonder = _ptr(a["map_is_hbonder"], C.c_int32)
+        s.map_hbond = _ptr(a["map_hbond"], C.c_int32)
+        s.map_solpar_probe = _ptr(a["map_solpar_probe"], C.c_double)
+        s.map_vol_probe = _ptr(a["map_vol_probe"], C.c_double)
+        s.e_vdw_hb = _ptr(a["e_vdw_hb"], C.c_float)
+        s.sol_fn = _ptr(a["sol_fn"], C.c_double)
+        s.r_epsilon_fn = _ptr(a["r_epsilon_fn"], C.c_double)
+        for k, v in self.scalars.items():
+            setattr(s, k, v)
+        self._struct = s  # arrays stay alive with self
+        return s
+
+    def bytes_h2d(self) -> int:
+        return int(sum(v.nbytes for v in self.arrays.values() if v is not None))
+
+    @classmethod
+    def from_struct(cls, s: ag_problem) -> "Problem":
+        """Copy a problem the front end built (ag_job_problem) into numpy arrays."""
+        n = s.n_atoms
+        nam = s.n_atom_maps
+        nrt = max(s.n_rec_types, 1)
+
+        def arr(ptr, count, dt):
+            if count == 0 or not ptr:
+                return np.zeros(count, dtype=dt)
+            return np.ctypeslib.as_array(ptr, shape=(count,)).astype(dt, copy=True)
+
+        kw = dict(
+            coord=arr(s.coord, 3 * n, np.float64).reshape(n, 3), charge=arr(s.charge, n, np.float64),
+            vol=arr(s.vol, n, np.float64), solpar=arr(s.solpar, n, np.float64),
+            rec_type=arr(s.rec_type, n, np.int32), hbond=arr(s.hbond, n, np.int32),
+            rexp=arr(s.rexp, n, np.int32), rvector=arr(s.rvector, 3 * n, np.float64).reshape(n, 3),
+            rvector2=arr(s.rvector2, 3 * n, np.float64).reshape(n, 3),
+            disorder=arr(s.disorder, n, np.uint8),
+            map_is_covalent=arr(s.map_is_covalent, max(nam, 1), np.int32),
+            map_is_hbonder=arr(s.map_is_hbonder, max(nam, 1), np.int32),
+            map_hbond=arr(s.map_hbond, max(nam, 1), np.int32),
+            map_solpar_probe=arr(s.map_solpar_probe, max(nam, 1), np.float64),
+            map_vol_probe=arr(s.map_vol_probe, max(nam, 1), np.float64),
+            e_vdw_hb=arr(s.e_vdw_hb, nrt * max(nam, 1) * _abi.AG_NEINT, np.float32),
+            sol_fn=arr(s.sol_fn, _abi.AG_NDIEL, np.float64),
+            r_epsilon_fn=arr(s.r_epsilon_fn, _abi.AG_NDIEL, np.float64),
+            n1=list(s.n1), ne=list(s.ne), cov_pos=list(s.cov_pos),
+        )
+        for k in cls.SCALARS:
+            kw[k] = getattr(s, k)
+        return cls(**kw)
+
+
+class Job:
+    """A parsed GPF: front end of `autogrid4 -p gpf -l glg` (ag_job_load)."""
+
+    def __init__(self, gpf: str, glg: str | None = None):
+        lib = load_library()
+        h = C.c_void_p()
+        check(lib.ag_job_load(os.fsencode(gpf), os.fsencode(glg) if glg else None, C.byref(h)))
+        self._h = h
+        self._lib = lib
+
+    def problem(self) -> Problem:
+        return Problem.from_struct(self._lib.ag_job_problem(self._h).contents)
+
+    def write_maps(self, maps: np.ndarray) -> None:
+        m = np.ascontiguousarray(maps)
+        if m.dtype == np.float64:
+            check(self._lib.ag_job_write_maps_f64(self._h, m.ctypes.data_as(C.c_void_p)))
+        else:
+            m = np.ascontiguousarray(m, dtype=np.float32)
+            check(self._lib.ag_job_write_maps_f32(self._h, m.ctypes.data_as(C.c_void_p)))
+
+    def fail(self, message: str) -> None:
+        self._lib.ag_job_fail(self._h, message.encode())
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.ag_job_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class Stats:
+    near_pairs: int
+    fp64_fallbacks: int
+    far_pairs: int
+    gpu_launches: int
+    kernel_ms: float
+    far_ms: float
+
+
+class Context:
+    """A CUDA device context of the map engine (ag_context)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load_library()
+        h = C.c_void_p()
+        check(self._lib.ag_context_create(int(device), C.byref(h)))
+        self._h = h
+
+    def compute(self, problem: Problem, precision: str = "fp32", out: np.ndarray | None = None) -> np.ndarray:
+        """Compute every map of `problem`; returns [n_maps, n1z, n1y, n1x]."""
+        prec = _PREC[precision]
+        dt = np.float64 if prec == _abi.AG_PREC_FP64 else np.float32
+        if out is None:
+            out = np.empty(problem.map_shape, dtype=dt)
+        if out.dtype != dt or not out.flags.c_contiguous or out.size != int(np.prod(problem.map_shape)):
+            raise ValueError("out must be a C-contiguous array of the map shape and precision")
+        opts = ag_opts(precision=prec, table_mode=_abi.AG_TABLE_NEAREST)
+        s = problem.struct()
+        fn = self._lib.ag_maps_compute_f64 if prec == _abi.AG_PREC_FP64 else self._lib.ag_maps_compute
+        check(fn(self._h, C.byref(s), C.byref(opts), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def stats(self) -> Stats:
+        st = ag_stats()
+        check(self._lib.ag_context_stats(self._h, C.byref(st)))
+        return Stats(st.near_pairs, st.fp64_fallbacks, st.far_pairs, st.gpu_launches, st.kernel_ms, st.far_ms)
+
+    def plan(self, problem: Problem) -> "Plan":
+        return Plan(self, problem)
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.ag_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """Device-resident problem: upload once, run many times (ag_plan)."""
+
+    def __init__(self, ctx: Context, problem: Problem):
+        self.ctx = ctx
+        self.problem = problem
+        self._lib = ctx._lib
+        h = C.c_void_p()
+        opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST)
+        s = problem.struct()
+        check(self._lib.ag_plan_create(ctx._h, C.byref(s), C.byref(opts), C.byref(h)))
+        self._h = h
+
+    def run(self, stream: int | None = None) -> None:
+        check(self._lib.ag_plan_run(self._h, C.c_void_p(stream) if stream else None))
+
+    def device_maps_ptr(self) -> int:
+        return int(self._lib.ag_plan_device_maps(self._h) or 0)
+
+    def download(self, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.problem.map_shape, dtype=np.float32)
+        check(self._lib.ag_plan_download(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.ag_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def run_gpf(gpf: str, glg: str | None = None, precision: str = "fp32", device: int = 0) -> np.ndarray:
+    """Drop-in for `autogrid4 -p gpf -l glg`: parse, compute on the GPU, write the maps."""
+    job = Job(gpf, glg)
+    try:
+        prob = job.problem()
+        ctx = Context(device)
+        try:
+            maps = ctx.compute(prob, precision)
+        finally:
+            ctx.close()
+        job.write_maps(maps)
+        return maps
+    except AutoGridError as e:
+        job.fail(e.message)
+        raise
+    finally:
+        job.close()

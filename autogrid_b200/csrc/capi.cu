@@ -1,0 +1,624 @@
+// C ABI of the hot path: contexts, plans and the kernel sequence that
+// replaces the reference's grid-point loop (main.cpp:2805-3464).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "autogrid_b200.h"
+#include "kernels/kernels.h"
+
+namespace agb {
+void set_last_error(const std::string &m);
+}
+
+using namespace agb;
+
+namespace {
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+// Grow-only device buffers keyed by role; a context keeps one set so repeated
+// one-shot calls do not re-allocate.
+struct BufferSet {
+    std::map<std::string, DevBuf> bufs;
+    ~BufferSet()
+    {
+        for (auto &kv : bufs)
+            if (kv.second.p) cudaFree(kv.second.p);
+    }
+    cudaError_t ensure(const std::string &name, size_t bytes, void **out)
+    {
+        DevBuf &b = bufs[name];
+        if (bytes == 0) bytes = 16;
+        if (b.cap < bytes) {
+            if (b.p) cudaFree(b.p);
+            b.p = nullptr;
+            b.cap = 0;
+            cudaError_t e = cudaMalloc(&b.p, bytes);
+            if (e != cudaSuccess) return e;
+            b.cap = bytes;
+        }
+        *out = b.p;
+        return cudaSuccess;
+    }
+};
+
+ag_status cuda_fail(cudaError_t e, const char *what)
+{
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return AG_ERR_CUDA;
+}
+
+#define AGB_CK(call)                                   \
+    do {                                               \
+        cudaError_t e_ = (call);                       \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+ag_status invalid(const std::string &m)
+{
+    set_last_error(m);
+    return AG_ERR_INVALID;
+}
+
+}  // namespace
+
+struct ag_context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf0 = nullptr, evf1 = nullptr;
+    ag_stats stats{};
+    BufferSet pool;
+    unsigned long long *d_counters = nullptr;
+    // the last run, whose statistics ag_context_stats() settles
+    bool pending = false, had_far = false;
+    int last_launches = 0;
+    int64_t last_far_pairs = 0;
+};
+
+struct ag_plan {
+    ag_context *ctx = nullptr;
+    std::unique_ptr<BufferSet> own;
+    BufferSet *bufs = nullptr;
+    ag_opts opts{};
+    DevProblem dp{};
+    std::vector<NearGroup> groups;
+    int mpad = 4, n_chunks = 0, chunk_atoms = 0;
+    bool any_cov = false;
+    float *maps32 = nullptr;
+    double *maps64 = nullptr;
+    int *closest = nullptr;
+    double *cov = nullptr;
+    float *far_partial = nullptr;
+    double *x128 = nullptr, *y128 = nullptr, *z128 = nullptr;
+    float *qw = nullptr, *far_tab = nullptr, *etab = nullptr, *solf = nullptr, *rvf = nullptr, *rv2f = nullptr,
+          *vdwT = nullptr;
+    size_t h2d_bytes = 0;
+    int last_launches = 0;
+};
+
+namespace {
+
+// Validate an ag_problem against the limits of the reference build.
+ag_status validate(const ag_problem *p)
+{
+    if (!p) return invalid("null problem");
+    if (p->n_atoms < 0 || p->n_atoms > AG_MAX_ATOMS) {
+        set_last_error("n_atoms out of range [0, AG_MAX_ATOMS]");
+        return AG_ERR_TOO_LARGE;
+    }
+    for (int i = 0; i < 3; i++) {
+        if (p->n1[i] < 1 || p->n1[i] > AG_MAX_GRID_PTS + 1 || (p->n1[i] % 2) != 1)
+            return invalid("n1 must be odd and within [1, MAX_GRID_PTS+1]");
+        if (p->ne[i] != (p->n1[i] - 1) / 2) return invalid("ne must equal (n1-1)/2");
+    }
+    if (!(p->spacing > 0.0) || !std::isfinite(p->spacing)) return invalid("spacing must be positive");
+    if (p->n_maps < 1 || p->n_maps > AG_MAX_MAPS) return invalid("n_maps out of range [1, MAX_MAPS]");
+    if (p->n_atom_maps < 0 || p->n_atom_maps > p->n_maps) return invalid("n_atom_maps out of range");
+    if (p->elec_map >= p->n_maps || (p->elec_map >= 0 && p->elec_map < p->n_atom_maps))
+        return invalid("elec_map index out of range");
+    if (p->dsolv_map >= p->n_maps || (p->dsolv_map >= 0 && p->dsolv_map < p->n_atom_maps))
+        return invalid("dsolv_map index out of range");
+    if (p->elec_map >= 0 && p->elec_map == p->dsolv_map) return invalid("elec_map == dsolv_map");
+    if (p->n_atom_maps + (p->elec_map >= 0) + (p->dsolv_map >= 0) != p->n_maps)
+        return invalid("n_maps != n_atom_maps + elec + dsolv");
+    if (p->n_rec_types < 0 || p->n_rec_types > AG_MAX_REC_TYPES) return invalid("n_rec_types out of range");
+    if (p->floating_grid || p->constriction_grid) {
+        set_last_error("floating (fmap) and constriction (cmap) grids are not provided by this build");
+        return AG_ERR_UNSUPPORTED;
+    }
+    const int N = p->n_atoms;
+    if (N > 0 && (!p->coord || !p->charge || !p->vol || !p->solpar || !p->rec_type || !p->hbond || !p->rexp ||
+                  !p->rvector || !p->rvector2 || !p->disorder))
+        return invalid("null atom array");
+    if (p->n_atom_maps > 0 && (!p->map_is_covalent || !p->map_is_hbonder || !p->map_hbond ||
+                               !p->map_solpar_probe || !p->map_vol_probe || !p->e_vdw_hb))
+        return invalid("null map array");
+    if (!p->sol_fn || (p->dddiel && !p->r_epsilon_fn)) return invalid("null table");
+    int n_h = 0;
+    for (int a = 0; a < N; a++) {
+        if (p->rec_type[a] < 0 || p->rec_type[a] >= std::max(p->n_rec_types, 1)) return invalid("rec_type out of range");
+        if (p->hbond[a] < 0 || p->hbond[a] > 6) return invalid("hbond class out of range");
+        for (int k = 0; k < 3; k++)
+            if (!std::isfinite(p->coord[3 * a + k])) return invalid("non-finite coordinate");
+        if (!std::isfinite(p->charge[a])) return invalid("non-finite charge");
+        if (p->hbond[a] == 1 || p->hbond[a] == 2) n_h++;
+    }
+    if (p->disorder_h && p->hydrogen_type >= std::max(p->n_rec_types, 1)) return invalid("hydrogen_type out of range");
+    if (p->n_atom_maps > 0 && n_h == 0) {
+        set_last_error("no closestH atom was found");  // main.cpp:3011-3014
+        return AG_ERR_NO_CLOSEST_H;
+    }
+    return AG_OK;
+}
+
+template <class T>
+cudaError_t upload(BufferSet *b, const char *name, const T *src, size_t n, T **dst, cudaStream_t s, size_t *acc)
+{
+    void *d = nullptr;
+    cudaError_t e = b->ensure(name, n * sizeof(T), &d);
+    if (e != cudaSuccess) return e;
+    *dst = (T *)d;
+    if (n) {
+        e = cudaMemcpyAsync(d, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+        if (acc) *acc += n * sizeof(T);
+    }
+    return e;
+}
+
+// Build the device image of a problem (host work is O(atoms + tables)).
+ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
+{
+    ag_status st = validate(p);
+    if (st != AG_OK) return st;
+    BufferSet *B = pl->bufs;
+    DevProblem &d = pl->dp;
+    std::memset(&d, 0, sizeof d);
+    const int N = p->n_atoms, nAM = p->n_atom_maps;
+    d.n_atoms = N; d.n_maps = p->n_maps; d.n_atom_maps = nAM; d.n_rec_types = p->n_rec_types;
+    d.elec_map = p->elec_map; d.dsolv_map = p->dsolv_map;
+    d.n1x = p->n1[0]; d.n1y = p->n1[1]; d.n1z = p->n1[2];
+    d.nex = p->ne[0]; d.ney = p->ne[1]; d.nez = p->ne[2];
+    d.P = (long long)d.n1x * d.n1y * d.n1z;
+    d.spacing = p->spacing;
+    d.dddiel = p->dddiel; d.disorder_h = p->disorder_h; d.hydrogen_type = p->hydrogen_type;
+    d.sep_desolv = p->separate_desolvation_maps;
+    d.invdielcal = p->invdielcal; d.coeff_estat = p->coeff_estat; d.solpar_q = p->solpar_q;
+    for (int i = 0; i < 3; i++) d.cov_pos[i] = p->cov_pos[i];
+    d.cov_half_width = p->cov_half_width; d.cov_barrier = p->cov_barrier;
+    pl->h2d_bytes = 0;
+    size_t *acc = &pl->h2d_bytes;
+
+    // atoms: SoA doubles, x*A_DIV copies for the far kernel, float bond vectors
+    std::vector<double> x(N), y(N), z(N), x128(N), y128(N), z128(N);
+    std::vector<float> qw(N), rvf(3 * (size_t)N), rv2f(3 * (size_t)N);
+    for (int a = 0; a < N; a++) {
+        x[a] = p->coord[3 * a]; y[a] = p->coord[3 * a + 1]; z[a] = p->coord[3 * a + 2];
+        x128[a] = x[a] * AG_A_DIV; y128[a] = y[a] * AG_A_DIV; z128[a] = z[a] * AG_A_DIV;
+        qw[a] = (float)(p->charge[a] * p->coeff_estat * AG_A_DIV);
+        for (int k = 0; k < 3; k++) {
+            rvf[3 * a + k] = (float)p->rvector[3 * a + k];
+            rv2f[3 * a + k] = (float)p->rvector2[3 * a + k];
+        }
+    }
+    std::vector<int> h_index;
+    for (int a = 0; a < N; a++)
+        if (p->hbond[a] == 1 || p->hbond[a] == 2) h_index.push_back(a);
+
+    // cell list over the grid box grown by the near radius
+    const double rc = AGB_NEAR_RADIUS, cs = AGB_CELL;
+    double lo[3], hi[3];
+    int nc[3];
+    for (int i = 0; i < 3; i++) {
+        lo[i] = (double)(-p->ne[i]) * p->spacing - rc;
+        hi[i] = (double)(p->n1[i] - 1 - p->ne[i]) * p->spacing + rc;
+        nc[i] = std::max(1, (int)std::ceil((hi[i] - lo[i]) / cs));
+        d.cell0[i] = lo[i];
+    }
+    d.ncx = nc[0]; d.ncy = nc[1]; d.ncz = nc[2];
+    d.cell_size = cs;
+    const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
+    std::vector<int> cell_of(N, -1), cell_start(ncell + 1, 0), cell_atoms;
+    for (int a = 0; a < N; a++) {
+        const double c3[3] = {x[a], y[a], z[a]};
+        int ci[3];
+        bool in = true;
+        for (int i = 0; i < 3; i++) {
+            if (!(c3[i] >= lo[i] && c3[i] <= hi[i])) { in = false; break; }
+            ci[i] = std::min(nc[i] - 1, (int)std::floor((c3[i] - lo[i]) / cs));
+        }
+        if (!in) continue;
+        cell_of[a] = (ci[2] * nc[1] + ci[1]) * nc[0] + ci[0];
+        cell_start[cell_of[a] + 1]++;
+    }
+    for (size_t c = 0; c < ncell; c++) cell_start[c + 1] += cell_start[c];
+    cell_atoms.resize(cell_start[ncell]);
+    {
+        std::vector<int> fill(cell_start.begin(), cell_start.end() - 1);
+        for (int a = 0; a < N; a++)  // stable: file order inside a cell
+            if (cell_of[a] >= 0) cell_atoms[fill[cell_of[a]]++] = a;
+    }
+
+    // tables
+    pl->mpad = std::max(4, (nAM + 3) / 4 * 4);
+    const int nT = std::max(1, p->n_rec_types);
+    std::vector<float> vdwT((size_t)nT * AG_NEINT * pl->mpad, 0.f);
+    for (int t = 0; t < p->n_rec_types; t++)
+        for (int m = 0; m < nAM; m++)
+            for (int k = 0; k < AG_NEINT; k++)
+                vdwT[((size_t)t * AG_NEINT + k) * pl->mpad + m] = p->e_vdw_hb[((size_t)t * nAM + m) * AG_NEINT + k];
+    std::vector<float> far_tab(AG_NDIEL, 0.f), etab(AG_NDIEL), solf(AG_NDIEL);
+    std::vector<double> reps(AG_NDIEL, 0.0);
+    for (int k = 0; k < AG_NDIEL; k++) {
+        const double f = p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal;
+        if (p->dddiel) reps[k] = p->r_epsilon_fn[k];
+        far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
+        etab[k] = (float)(f * p->coeff_estat);
+        solf[k] = (float)p->sol_fn[k];
+    }
+
+    // map groups (act table after main.cpp:3286-3379)
+    std::vector<int> is_partner(std::max(nAM, 1), 0);
+    if (p->separate_desolvation_maps) {
+        for (int m = 0; m < nAM; m++) {
+            if (p->map_is_covalent[m]) continue;
+            if (m + 1 < nAM) is_partner[m + 1] = 1;
+            m++;
+        }
+    }
+    pl->groups.clear();
+    pl->any_cov = false;
+    for (int g0 = 0; g0 < nAM || (g0 == 0 && pl->groups.empty()); g0 += NG_MAX) {
+        NearGroup g;
+        std::memset(&g, 0, sizeof g);
+        g.g0 = g0;
+        g.ng = std::max(0, std::min(NG_MAX, nAM - g0));
+        g.write_special = (g0 == 0);
+        g.has_hrow = p->disorder_h ? 1 : 0;
+        for (int j = 0; j < g.ng; j++) {
+            const int m = g0 + j;
+            g.cov[j] = (uint8_t)(p->map_is_covalent[m] ? 1 : 0);
+            if (g.cov[j]) pl->any_cov = true;
+            const bool aff = !g.cov[j] && !is_partner[m];
+            for (int hb = 0; hb < 8; hb++) {
+                uint8_t a = ACT_PLAIN;
+                if (!aff) a = ACT_SKIP;
+                else if (p->map_is_hbonder[m]) {
+                    const int mh = p->map_hbond[m];
+                    if ((mh == 3 || mh == 5 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) a = ACT_SUMA;
+                    else if ((mh == 4 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) a = ACT_MMA;
+                    else if ((mh == 1 || mh == 2 || mh == 6) && (hb > 2 || hb == 6)) a = ACT_MMD;
+                }
+                g.act[j][hb] = a;
+            }
+            // desolvation lands on the affinity map, or on its partner when maps are separate
+            const bool gets_desolv = !g.cov[j] && (p->separate_desolvation_maps ? (bool)is_partner[m] : true);
+            g.sp[j] = gets_desolv ? p->map_solpar_probe[m] : 0.0;
+            g.vp[j] = gets_desolv ? p->map_vol_probe[m] : 0.0;
+        }
+        pl->groups.push_back(g);
+        if (nAM == 0) break;
+    }
+
+    // far-field chunking: enough CTAs for ~8 waves
+    const long long frames = (long long)frames_x(d.n1x) * frames_y(d.n1y) * frames_z(d.n1z);
+    const int tile = 512;
+    if (p->elec_map >= 0 && N > 0) {
+        const long long target = 148LL * 3 * 8;
+        int nch = (int)std::max(1LL, (target + frames - 1) / frames);
+        nch = std::min(nch, (N + tile - 1) / tile);
+        pl->chunk_atoms = ((N + nch - 1) / nch + tile - 1) / tile * tile;
+        pl->n_chunks = (N + pl->chunk_atoms - 1) / pl->chunk_atoms;
+    } else {
+        pl->chunk_atoms = 0;
+        pl->n_chunks = 0;
+    }
+
+    // uploads
+    double *dx, *dy, *dz, *dq, *dvol, *dsol, *drv, *drv2;
+    int *dtype, *dhb, *drexp, *dh, *dcs, *dca, *dmc, *dmh, *dmhb;
+    uint8_t *ddis;
+    double *dms, *dmv, *dsolfn, *dreps;
+    AGB_CK(upload(B, "x", x.data(), N, &dx, s, acc));
+    AGB_CK(upload(B, "y", y.data(), N, &dy, s, acc));
+    AGB_CK(upload(B, "z", z.data(), N, &dz, s, acc));
+    AGB_CK(upload(B, "x128", x128.data(), N, &pl->x128, s, acc));
+    AGB_CK(upload(B, "y128", y128.data(), N, &pl->y128, s, acc));
+    AGB_CK(upload(B, "z128", z128.data(), N, &pl->z128, s, acc));
+    AGB_CK(upload(B, "q", p->charge, N, &dq, s, acc));
+    AGB_CK(upload(B, "vol", p->vol, N, &dvol, s, acc));
+    AGB_CK(upload(B, "solpar", p->solpar, N, &dsol, s, acc));
+    AGB_CK(upload(B, "rv", p->rvector, 3 * (size_t)N, &drv, s, acc));
+    AGB_CK(upload(B, "rv2", p->rvector2, 3 * (size_t)N, &drv2, s, acc));
+    AGB_CK(upload(B, "type", p->rec_type, N, &dtype, s, acc));
+    AGB_CK(upload(B, "hbond", p->hbond, N, &dhb, s, acc));
+    AGB_CK(upload(B, "rexp", p->rexp, N, &drexp, s, acc));
+    AGB_CK(upload(B, "disorder", p->disorder, N, &ddis, s, acc));
+    AGB_CK(upload(B, "qw", qw.data(), N, &pl->qw, s, acc));
+    AGB_CK(upload(B, "rvf", rvf.data(), rvf.size(), &pl->rvf, s, acc));
+    AGB_CK(upload(B, "rv2f", rv2f.data(), rv2f.size(), &pl->rv2f, s, acc));
+    AGB_CK(upload(B, "h_index", h_index.data(), h_index.size(), &dh, s, acc));
+    AGB_CK(upload(B, "cell_start", cell_start.data(), cell_start.size(), &dcs, s, acc));
+    AGB_CK(upload(B, "cell_atoms", cell_atoms.data(), cell_atoms.size(), &dca, s, acc));
+    std::vector<int> mc(std::max(nAM, 1), 0), mh(std::max(nAM, 1), 0), mhb(std::max(nAM, 1), 0);
+    std::vector<double> ms(std::max(nAM, 1), 0.0), mv(std::max(nAM, 1), 0.0);
+    for (int m = 0; m < nAM; m++) {
+        mc[m] = p->map_is_covalent[m]; mh[m] = p->map_is_hbonder[m]; mhb[m] = p->map_hbond[m];
+        ms[m] = p->map_solpar_probe[m]; mv[m] = p->map_vol_probe[m];
+    }
+    AGB_CK(upload(B, "m_cov", mc.data(), mc.size(), &dmc, s, acc));
+    AGB_CK(upload(B, "m_hb", mh.data(), mh.size(), &dmh, s, acc));
+    AGB_CK(upload(B, "m_hbond", mhb.data(), mhb.size(), &dmhb, s, acc));
+    AGB_CK(upload(B, "m_solpar", ms.data(), ms.size(), &dms, s, acc));
+    AGB_CK(upload(B, "m_vol", mv.data(), mv.size(), &dmv, s, acc));
+    AGB_CK(upload(B, "vdwT", vdwT.data(), vdwT.size(), &pl->vdwT, s, acc));
+    AGB_CK(upload(B, "far_tab", far_tab.data(), far_tab.size(), &pl->far_tab, s, acc));
+    AGB_CK(upload(B, "etab", etab.data(), etab.size(), &pl->etab, s, acc));
+    AGB_CK(upload(B, "solf", solf.data(), solf.size(), &pl->solf, s, acc));
+    AGB_CK(upload(B, "sol_fn", p->sol_fn, AG_NDIEL, &dsolfn, s, acc));
+    AGB_CK(upload(B, "reps", reps.data(), reps.size(), &dreps, s, acc));
+
+    d.x = dx; d.y = dy; d.z = dz; d.q = dq; d.vol = dvol; d.solpar = dsol; d.rv = drv; d.rv2 = drv2;
+    d.type = dtype; d.hbond = dhb; d.rexp = drexp; d.disorder = ddis;
+    d.n_h = (int)h_index.size(); d.h_index = dh;
+    d.cell_start = dcs; d.cell_atoms = dca;
+    d.m_cov = dmc; d.m_hb = dmh; d.m_hbond = dmhb; d.m_solpar = dms; d.m_vol = dmv;
+    d.vdw = pl->vdwT; d.sol_fn = dsolfn; d.reps = dreps; d.far_tab = pl->far_tab;
+
+    // outputs and scratch
+    void *v = nullptr;
+    const size_t P = (size_t)d.P;
+    if (pl->opts.precision == AG_PREC_FP64) {
+        AGB_CK(B->ensure("maps64", (size_t)p->n_maps * P * sizeof(double), &v));
+        pl->maps64 = (double *)v;
+        pl->maps32 = nullptr;
+    } else {
+        AGB_CK(B->ensure("maps32", (size_t)p->n_maps * P * sizeof(float), &v));
+        pl->maps32 = (float *)v;
+        pl->maps64 = nullptr;
+    }
+    AGB_CK(B->ensure("closest", P * sizeof(int), &v));
+    pl->closest = (int *)v;
+    if (pl->any_cov) {
+        AGB_CK(B->ensure("cov", P * sizeof(double), &v));
+        pl->cov = (double *)v;
+    } else {
+        pl->cov = nullptr;
+    }
+    if (pl->n_chunks > 0 && pl->opts.precision != AG_PREC_FP64) {
+        AGB_CK(B->ensure("far_partial", (size_t)pl->n_chunks * P * sizeof(float), &v));
+        pl->far_partial = (float *)v;
+    } else {
+        pl->far_partial = nullptr;
+    }
+    d.far_chunks = (pl->opts.precision == AG_PREC_FP64) ? 0 : pl->n_chunks;
+    d.far_partial = pl->far_partial;
+    return AG_OK;
+}
+
+ag_status run_plan(ag_plan *pl, cudaStream_t s)
+{
+    ag_context *c = pl->ctx;
+    const DevProblem &d = pl->dp;
+    const bool exact = pl->opts.precision == AG_PREC_FP64;
+    int launches = 0;
+    AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+    AGB_CK(cudaEventRecord(c->ev0, s));
+    if (d.elec_map >= 0) {
+        if (exact) {
+            AGB_CK(launch_emap_exact(d, pl->maps64 + (size_t)d.elec_map * d.P, s));
+            launches++;
+        } else if (pl->n_chunks > 0) {
+            AGB_CK(cudaEventRecord(c->evf0, s));
+            AGB_CK(launch_emap_far(pl->x128, pl->y128, pl->z128, pl->qw, d.n_atoms, pl->chunk_atoms, pl->n_chunks,
+                                   pl->far_tab, d.spacing * AG_A_DIV, d.n1x, d.n1y, d.n1z, d.nex, d.ney, d.nez,
+                                   d.P, pl->far_partial, s));
+            AGB_CK(cudaEventRecord(c->evf1, s));
+            launches++;
+        }
+    }
+    if (pl->any_cov) {
+        AGB_CK(launch_covalent(d, pl->cov, s));
+        launches++;
+    }
+    if (d.n_atom_maps > 0) {
+        AGB_CK(launch_closest_h(d, pl->closest, s));
+        launches++;
+    }
+    const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || (!exact && d.elec_map >= 0);
+    if (need_near) {
+        for (const NearGroup &g : pl->groups) {
+            AGB_CK(launch_near(exact, d, g, pl->closest, pl->rvf, pl->rv2f, pl->vdwT, pl->mpad, pl->etab, pl->solf,
+                               pl->cov, pl->maps32, pl->maps64, c->d_counters, s));
+            launches++;
+        }
+    }
+    AGB_CK(cudaEventRecord(c->ev1, s));
+    pl->last_launches = launches;
+    c->pending = true;
+    c->had_far = !exact && d.elec_map >= 0 && pl->n_chunks > 0;
+    c->last_launches = launches;
+    c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
+    return AG_OK;
+}
+
+ag_status settle_stats(ag_context *c)
+{
+    if (!c->pending) return AG_OK;
+    AGB_CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.f, fms = 0.f;
+    AGB_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (c->had_far) AGB_CK(cudaEventElapsedTime(&fms, c->evf0, c->evf1));
+    unsigned long long h[4] = {0, 0, 0, 0};
+    AGB_CK(cudaMemcpy(h, c->d_counters, sizeof h, cudaMemcpyDeviceToHost));
+    c->stats.near_pairs = (int64_t)h[0];
+    c->stats.fp64_fallbacks = (int64_t)h[1];
+    c->stats.far_pairs = c->last_far_pairs;
+    c->stats.gpu_launches = c->last_launches;
+    c->stats.kernel_ms = ms;
+    c->stats.far_ms = fms;
+    c->pending = false;
+    return AG_OK;
+}
+
+ag_status finish_stats(ag_plan *pl) { return settle_stats(pl->ctx); }
+
+ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out)
+{
+    if (!ctx || !p || !out) return invalid("null argument");
+    ag_opts opts{};
+    if (o) opts = *o;
+    if (opts.precision != AG_PREC_FP32 && opts.precision != AG_PREC_FP64) return invalid("unknown precision");
+    if (opts.table_mode != AG_TABLE_NEAREST) {
+        set_last_error("only nearest-bin tables are provided by this build");
+        return AG_ERR_UNSUPPORTED;
+    }
+    AGB_CK(cudaSetDevice(ctx->device));
+    std::unique_ptr<ag_plan> pl(new ag_plan());
+    pl->ctx = ctx;
+    pl->opts = opts;
+    if (own) {
+        pl->own.reset(new BufferSet());
+        pl->bufs = pl->own.get();
+    } else {
+        pl->bufs = &ctx->pool;
+    }
+    ag_status st = build_plan(pl.get(), p, ctx->stream);
+    if (st != AG_OK) return st;
+    *out = pl.release();
+    return AG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ag_status ag_context_create(int32_t device, ag_context **out)
+{
+    if (!out) return invalid("null argument");
+    *out = nullptr;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        set_last_error(std::string("no CUDA device: ") + (e == cudaSuccess ? "count is 0" : cudaGetErrorString(e)));
+        return AG_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= n) return invalid("device index out of range");
+    std::unique_ptr<ag_context> c(new ag_context());
+    c->device = device;
+    AGB_CK(cudaSetDevice(device));
+    AGB_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    AGB_CK(cudaEventCreate(&c->ev0));
+    AGB_CK(cudaEventCreate(&c->ev1));
+    AGB_CK(cudaEventCreate(&c->evf0));
+    AGB_CK(cudaEventCreate(&c->evf1));
+    AGB_CK(cudaMalloc(&c->d_counters, 4 * sizeof(unsigned long long)));
+    *out = c.release();
+    return AG_OK;
+}
+
+ag_status ag_context_destroy(ag_context *ctx)
+{
+    if (!ctx) return AG_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->d_counters) cudaFree(ctx->d_counters);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->evf0) cudaEventDestroy(ctx->evf0);
+    if (ctx->evf1) cudaEventDestroy(ctx->evf1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return AG_OK;
+}
+
+ag_status ag_context_stats(const ag_context *ctx, ag_stats *out)
+{
+    if (!ctx || !out) return invalid("null argument");
+    ag_status st = settle_stats(const_cast<ag_context *>(ctx));
+    if (st != AG_OK) return st;
+    *out = ctx->stats;
+    return AG_OK;
+}
+
+static ag_status compute_common(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, void *maps,
+                                size_t elem)
+{
+    if (!maps) return invalid("null maps");
+    ag_plan *pl = nullptr;
+    ag_status st = make_plan(ctx, problem, opts, false, &pl);
+    if (st != AG_OK) return st;
+    std::unique_ptr<ag_plan> guard(pl);
+    st = run_plan(pl, ctx->stream);
+    if (st != AG_OK) return st;
+    const void *src = elem == 8 ? (const void *)pl->maps64 : (const void *)pl->maps32;
+    AGB_CK(cudaMemcpyAsync(maps, src, (size_t)problem->n_maps * (size_t)pl->dp.P * elem, cudaMemcpyDefault,
+                           ctx->stream));
+    AGB_CK(cudaStreamSynchronize(ctx->stream));
+    return finish_stats(pl);
+}
+
+ag_status ag_maps_compute(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, float *maps)
+{
+    if (opts && opts->precision != AG_PREC_FP32) return invalid("ag_maps_compute needs AG_PREC_FP32");
+    return compute_common(ctx, problem, opts, maps, 4);
+}
+
+ag_status ag_maps_compute_f64(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, double *maps)
+{
+    if (!opts || opts->precision != AG_PREC_FP64) return invalid("ag_maps_compute_f64 needs AG_PREC_FP64");
+    return compute_common(ctx, problem, opts, maps, 8);
+}
+
+ag_status ag_plan_create(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, ag_plan **out)
+{
+    ag_opts o{};
+    if (opts) o = *opts;
+    if (o.precision != AG_PREC_FP32) return invalid("plans run the FP32 path; use ag_maps_compute_f64 for FP64");
+    ag_status st = make_plan(ctx, problem, &o, true, out);
+    if (st != AG_OK) return st;
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamSynchronize");
+    return AG_OK;
+}
+
+ag_status ag_plan_run(ag_plan *plan, void *stream)
+{
+    if (!plan) return invalid("null plan");
+    cudaStream_t s = stream ? (cudaStream_t)stream : plan->ctx->stream;
+    return run_plan(plan, s);
+}
+
+const float *ag_plan_device_maps(const ag_plan *plan) { return plan ? plan->maps32 : nullptr; }
+
+size_t ag_plan_points(const ag_plan *plan) { return plan ? (size_t)plan->dp.P : 0; }
+
+ag_status ag_plan_download(ag_plan *plan, float *host_maps)
+{
+    if (!plan || !host_maps) return invalid("null argument");
+    ag_context *c = plan->ctx;
+    AGB_CK(cudaMemcpyAsync(host_maps, plan->maps32, (size_t)plan->dp.n_maps * (size_t)plan->dp.P * sizeof(float),
+                           cudaMemcpyDefault, c->stream));
+    AGB_CK(cudaStreamSynchronize(c->stream));
+    return finish_stats(plan);
+}
+
+ag_status ag_plan_destroy(ag_plan *plan)
+{
+    if (!plan) return AG_OK;
+    cudaSetDevice(plan->ctx->device);
+    cudaStreamSynchronize(plan->ctx->stream);
+    delete plan;
+    return AG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,200 @@
+// Electrostatic map kernels (replace LOOP 1 of the reference, main.cpp:2940-2982).
+//
+// k_emap_far  -- production FP32 far field: every (point, atom) pair whose
+//                canonical FP32 distance t = A_DIV*r is >= AG_NEINT bins
+//                (r >= 8 A).  Pairs nearer than that are left to the near-field
+//                kernel, which evaluates them with exact bins.  Per pair:
+//                1 rsqrt (MUFU), packed FP32x2 arithmetic, one shared-memory
+//                table gather.  Atoms are streamed through shared memory in
+//                tiles; each thread keeps 8 grid points of one x-row in
+//                registers (two-level summation: per-tile partial + total).
+//                The atom list is split into chunks for load balance; chunk
+//                partial sums land in far_partial[chunk][point] and are added
+//                in fixed chunk order by the near-field kernel (deterministic).
+// k_emap_exact -- FP64 twin: every pair, exactly the reference expression
+//                (nested hypot, double table), file order summation.
+#include "agb_device.cuh"
+
+namespace agb {
+
+constexpr int EF_THREADS = 256;
+constexpr int EF_TILE = 512;      // atoms per shared-memory tile
+constexpr int EF_PAIRS = 4;       // float2 pairs of points per thread (8 points)
+
+__device__ __forceinline__ float lds_f32(uint32_t addr)
+{
+    float v;
+    asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(addr));
+    return v;
+}
+
+// Atom tile entry: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
+__global__ void __launch_bounds__(EF_THREADS, 3)
+k_emap_far(const double *__restrict__ ax128, const double *__restrict__ ay128,
+           const double *__restrict__ az128, const float *__restrict__ qw, int n_atoms,
+           int chunk_atoms, const float *__restrict__ far_tab, double spacing_adiv,
+           int n1x, int n1y, int n1z, int nex, int ney, int nez, int nfx, int nfy,
+           long long P, float *__restrict__ partial)
+{
+    extern __shared__ float4 ef_smem[];
+    float4 *s_tab4 = ef_smem;                         // AG_NDIEL floats
+    float4 *s_atom = ef_smem + AG_NDIEL / 4;          // EF_TILE entries
+    const int tid = threadIdx.x;
+    for (int i = tid; i < AG_NDIEL / 4; i += EF_THREADS) s_tab4[i] = __ldg(((const float4 *)far_tab) + i);
+
+    const int f = blockIdx.x;
+    const int fx = f % nfx, fy = (f / nfx) % nfy, fz = f / (nfx * nfy);
+    const int ox = fx * FRAME_X, oy = fy * FRAME_Y, oz = fz * FRAME_Z;
+    // frame origin in bins, exactly (ox-nex)*spacing*A_DIV as the reference forms c (main.cpp:2859)
+    const double X0 = frame_origin_bins(ox, nex, spacing_adiv);
+    const double Y0 = frame_origin_bins(oy, ney, spacing_adiv);
+    const double Z0 = frame_origin_bins(oz, nez, spacing_adiv);
+
+    // compact 4x4x2 lane footprint per warp (fewest table bank conflicts)
+    const int lane = tid & 31, w = tid >> 5;
+    const int tx = lane & 3;
+    const int ty = ((lane >> 2) & 3) + 4 * (w & 1);
+    const int tz = (lane >> 4) + 2 * (w >> 1);
+    const float py = frame_point_coord(ty, spacing_adiv);
+    const float pz = frame_point_coord(tz, spacing_adiv);
+    float2 npx[EF_PAIRS];
+#pragma unroll
+    for (int j = 0; j < EF_PAIRS; j++)
+        npx[j] = make_float2(-frame_point_coord(tx + 8 * j, spacing_adiv),
+                             -frame_point_coord(tx + 8 * j + 4, spacing_adiv));
+    const float2 npyz = make_float2(-py, -pz);
+    float2 tot[EF_PAIRS];
+#pragma unroll
+    for (int j = 0; j < EF_PAIRS; j++) tot[j] = make_float2(0.f, 0.f);
+
+    // 32-bit shared address of s_tab, pre-biased so that the bit pattern of
+    // (t + 2^23) rounded toward zero indexes the table directly:
+    // bits(t + 2^23) = 0x4B000000 + floor(t) for 0 <= t < 2^23.
+    const uint32_t tab_base = (uint32_t)__cvta_generic_to_shared(s_tab4) - (0x4B000000u << 2);
+    const float2 magic = make_float2(8388608.f, 8388608.f);
+    const float2 tmax = make_float2(FAR_MAX_T, FAR_MAX_T);
+
+    const int a_begin = blockIdx.y * chunk_atoms;
+    const int a_end = min(n_atoms, a_begin + chunk_atoms);
+    for (int a0 = a_begin; a0 < a_end; a0 += EF_TILE) {
+        const int na = min(EF_TILE, a_end - a0);
+        __syncthreads();
+        for (int i = tid; i < EF_TILE; i += EF_THREADS) {
+            float4 v;
+            if (i < na) {
+                const int a = a0 + i;
+                v.x = frame_atom_coord(__ldg(ax128 + a), X0);
+                v.y = frame_atom_coord(__ldg(ay128 + a), Y0);
+                v.z = frame_atom_coord(__ldg(az128 + a), Z0);
+                v.w = __ldg(qw + a);
+            } else {
+                v = make_float4(1.0e6f, 1.0e6f, 1.0e6f, 0.f);  // far, zero weight
+            }
+            s_atom[i] = v;
+        }
+        __syncthreads();
+        float2 acc[EF_PAIRS];
+#pragma unroll
+        for (int j = 0; j < EF_PAIRS; j++) acc[j] = make_float2(0.f, 0.f);
+#pragma unroll 2
+        for (int i = 0; i < na; i++) {
+            const float4 A = s_atom[i];
+            const float2 dyz = __fadd2_rn(make_float2(A.y, A.z), npyz);
+            const float s = __fmaf_rn(dyz.x, dyz.x, __fmaf_rn(dyz.y, dyz.y, TINY_T2));
+            const float2 s2 = make_float2(s, s);
+            const float2 ax2 = make_float2(A.x, A.x);
+            const float2 q2 = make_float2(A.w, A.w);
+#pragma unroll
+            for (int j = 0; j < EF_PAIRS; j++) {
+                const float2 dx = __fadd2_rn(ax2, npx[j]);
+                const float2 t2 = __ffma2_rn(dx, dx, s2);
+                const float2 rs = make_float2(rsqrt_approx(t2.x), rsqrt_approx(t2.y));
+                float2 t = __fmul2_rn(t2, rs);
+                t = make_float2(fminf(t.x, tmax.x), fminf(t.y, tmax.y));
+                const float2 mg = __fadd2_rz(t, magic);
+                const float T0 = lds_f32(tab_base + (__float_as_uint(mg.x) << 2));
+                const float T1 = lds_f32(tab_base + (__float_as_uint(mg.y) << 2));
+                const float2 wv = __fmul2_rn(q2, rs);
+                acc[j] = __ffma2_rn(wv, make_float2(T0, T1), acc[j]);
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < EF_PAIRS; j++) tot[j] = __fadd2_rn(tot[j], acc[j]);
+    }
+
+    const int iy = oy + ty, iz = oz + tz;
+    if (iy < n1y && iz < n1z) {
+        float *out = partial + (size_t)blockIdx.y * (size_t)P + ((size_t)iz * n1y + iy) * (size_t)n1x;
+#pragma unroll
+        for (int j = 0; j < EF_PAIRS; j++) {
+            const int ix0 = ox + tx + 8 * j, ix1 = ix0 + 4;
+            if (ix0 < n1x) out[ix0] = tot[j].x;
+            if (ix1 < n1x) out[ix1] = tot[j].y;
+        }
+    }
+}
+
+// FP64 twin of LOOP 1: one thread per point, all atoms in file order.
+constexpr int EX_THREADS = 128;
+constexpr int EX_TILE = 256;
+
+__global__ void __launch_bounds__(EX_THREADS)
+k_emap_exact(DevProblem p, double *__restrict__ emap)
+{
+    __shared__ double s_x[EX_TILE], s_y[EX_TILE], s_z[EX_TILE], s_q[EX_TILE];
+    const long long lin = (long long)blockIdx.x * EX_THREADS + threadIdx.x;
+    const bool valid = lin < p.P;
+    const int ix = (int)(lin % p.n1x), iy = (int)((lin / p.n1x) % p.n1y), iz = (int)(lin / ((long long)p.n1x * p.n1y));
+    const double cx = (double)(ix - p.nex) * p.spacing;
+    const double cy = (double)(iy - p.ney) * p.spacing;
+    const double cz = (double)(iz - p.nez) * p.spacing;
+    double e = 0.0;
+    for (int a0 = 0; a0 < p.n_atoms; a0 += EX_TILE) {
+        const int na = min(EX_TILE, p.n_atoms - a0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < na; i += EX_THREADS) {
+            s_x[i] = p.x[a0 + i]; s_y[i] = p.y[a0 + i]; s_z[i] = p.z[a0 + i]; s_q[i] = p.q[a0 + i];
+        }
+        __syncthreads();
+        for (int i = 0; i < na; i++) {
+            double r = hypot(__dsub_rn(s_x[i], cx), hypot(__dsub_rn(s_y[i], cy), __dsub_rn(s_z[i], cz)));
+            if (r < 1.0e-6) r = 1.0e-6;
+            const double inv_rmax = __ddiv_rn(1.0, r > 0.5 ? r : 0.5);
+            int k = (int)__dmul_rn(r, (double)AG_A_DIV);
+            if (k > AG_NDIEL - 1) k = AG_NDIEL - 1;
+            const double f = p.dddiel ? p.reps[k] : p.invdielcal;
+            e = __dadd_rn(e, __dmul_rn(__dmul_rn(__dmul_rn(s_q[i], inv_rmax), f), p.coeff_estat));
+        }
+    }
+    if (valid) emap[lin] = e;
+}
+
+}  // namespace agb
+
+namespace agb {
+
+int frames_x(int n1x) { return (n1x + FRAME_X - 1) / FRAME_X; }
+int frames_y(int n1y) { return (n1y + FRAME_Y - 1) / FRAME_Y; }
+int frames_z(int n1z) { return (n1z + FRAME_Z - 1) / FRAME_Z; }
+
+cudaError_t launch_emap_far(const double *ax128, const double *ay128, const double *az128, const float *qw,
+                            int n_atoms, int chunk_atoms, int n_chunks, const float *far_tab,
+                            double spacing_adiv, int n1x, int n1y, int n1z, int nex, int ney, int nez,
+                            long long P, float *partial, cudaStream_t s)
+{
+    const int nfx = frames_x(n1x), nfy = frames_y(n1y), nfz = frames_z(n1z);
+    const size_t smem = AG_NDIEL * sizeof(float) + EF_TILE * sizeof(float4);
+    dim3 grid((unsigned)(nfx * nfy * nfz), (unsigned)n_chunks);
+    k_emap_far<<<grid, EF_THREADS, smem, s>>>(ax128, ay128, az128, qw, n_atoms, chunk_atoms, far_tab,
+                                              spacing_adiv, n1x, n1y, n1z, nex, ney, nez, nfx, nfy, P, partial);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s)
+{
+    const unsigned nb = (unsigned)((p.P + EX_THREADS - 1) / EX_THREADS);
+    k_emap_exact<<<nb, EX_THREADS, 0, s>>>(p, emap);
+    return cudaGetLastError();
+}
+
+}  // namespace agb

@@ -1,0 +1,560 @@
+// Near-field kernels: everything of the reference grid loop except the
+// far-field electrostatics.
+//
+//   k_closest_h  closest DS/D1 hydrogen per point (main.cpp:2986-3015): FP32
+//                prefilter over all DS/D1 atoms, then an FP64 pass in file
+//                order over the candidates within the FP32 error bound, with
+//                the reference's strict '<' so ties keep the first atom.
+//   k_near<EXACT> one thread per grid point, bricks of 8x8x4 points.  Candidate
+//                atoms come from a cell list (cells of AGB_CELL A over the box
+//                grown by 8.05 A) and are staged through shared memory.
+//                Per pair: short-range AD4 terms of LOOP 2 (main.cpp:3030-3404),
+//                the d map, and (FP32 path only) the near part of the e map,
+//                i.e. the pairs the far-field kernel leaves out.
+//       EXACT=true : FP64 twin, every quantity in FP64 exactly as the reference.
+//       EXACT=false: FP32 production path.  Distances come from the same
+//                canonical frame-relative FP32 arithmetic as the far-field
+//                kernel.  Whenever an FP32 quantity lies within its error bound
+//                of a discontinuity of the reference (table-bin edge, the
+//                8 A cutoff, the cos=0 branch of the D1 and A2 factors, a
+//                disordered-hydrogen bin edge) the pair is re-evaluated in FP64
+//                with the reference formulas, so table bins equal the FP64
+//                reference's.
+//   Desolvation is factored: sum_a sol(r)(sp_m vol_a + (solpar_a+qasp|q_a|) vp_m)
+//   = sp_m*D1 + vp_m*D2 with D1 = sum vol_a sol, D2 = sum (solpar_a+qasp|q_a|) sol,
+//   and the d map is qasp*D1 (main.cpp:3381-3404).
+#include <type_traits>
+
+#include "agb_device.cuh"
+#include "near_params.h"
+
+namespace agb {
+
+constexpr int NB_X = 8, NB_Y = 8, NB_Z = 4, NB_THREADS = 256;
+constexpr int NB_CHUNK = 256;
+constexpr int NB_SEGS = 64;
+constexpr float GUARD_BIN = 2.0e-3f;   // bins: > 3x the FP32 distance error bound
+constexpr float GUARD_COS = 5.0e-5f;
+constexpr double APPROX_ZERO_D = 1.0e-6;
+constexpr double PI_D = 3.14159265358979323846;
+
+// ------------------------------------------------------------ pair state ---
+template <class R>
+struct PairQ {
+    int ad4_in;   // inside 8 A and not a skipped disordered hydrogen
+    int bin;      // (int)(r*A_DIV), unclamped
+    int bin_e;    // LOOP 1 bin (nested hypot), unclamped
+    int ih;       // disordered-hydrogen row bin, clamped to [0, NEINT-1]
+    R r, inv_rmax, racc, rdon, Hramp;
+};
+
+// FP64, expression-for-expression restatement of main.cpp:3037-3272 for one
+// (point, atom) pair.  Explicit _rn intrinsics keep nvcc from contracting.
+__device__ __noinline__ void pair_exact(const DevProblem &p, int ia, double cx, double cy, double cz,
+                                        int ch, PairQ<double> &o)
+{
+    const double d0 = __dsub_rn(p.x[ia], cx), d1 = __dsub_rn(p.y[ia], cy), d2 = __dsub_rn(p.z[ia], cz);
+    double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
+    double re = hypot(d0, hypot(d1, d2));
+    o.ad4_in = !(r > AG_NBC);
+    if (p.disorder_h && p.disorder[ia] && p.type[ia] == p.hydrogen_type) o.ad4_in = 0;
+    if (r < APPROX_ZERO_D) r = APPROX_ZERO_D;
+    if (re < APPROX_ZERO_D) re = APPROX_ZERO_D;
+    o.r = r;
+    o.inv_rmax = __ddiv_rn(1.0, re > 0.5 ? re : 0.5);
+    o.bin = __double2int_rz(__dmul_rn(r, (double)AG_A_DIV));
+    o.bin_e = __double2int_rz(__dmul_rn(re, (double)AG_A_DIV));
+    int ih = __double2int_rz(__dmul_rn(__dsub_rn(r, 1.10), (double)AG_A_DIV));
+    ih = ih < 0 ? 0 : ih;
+    o.ih = ih > AG_NEINT - 1 ? AG_NEINT - 1 : ih;
+    o.racc = 1.0; o.rdon = 1.0; o.Hramp = 1.0;
+    const double inv_r = __ddiv_rn(1.0, r);
+    const double dn0 = __dmul_rn(d0, inv_r), dn1 = __dmul_rn(d1, inv_r), dn2 = __dmul_rn(d2, inv_r);
+    const int hb = p.hbond[ia];
+    const double *rv = p.rv + 3 * (size_t)ia;
+    const double PI_halved = PI_D / 2.;
+    auto negdot = [&](const double *v) {
+        double c = 0.;
+        c = __dsub_rn(c, __dmul_rn(dn0, v[0]));
+        c = __dsub_rn(c, __dmul_rn(dn1, v[1]));
+        c = __dsub_rn(c, __dmul_rn(dn2, v[2]));
+        return c;
+    };
+    if (hb == 2) {
+        const double cos_theta = negdot(rv);
+        if (cos_theta <= 0.) {
+            o.racc = 0.;
+        } else {
+            const int e = p.rexp[ia];
+            if (e == 2) o.racc = __dmul_rn(cos_theta, cos_theta);
+            else if (e == 4) { const double t = __dmul_rn(cos_theta, cos_theta); o.racc = __dmul_rn(t, t); }
+            else o.racc = cos_theta;
+            if (ia == ch) {
+                o.Hramp = 1.;
+            } else {
+                const double *rh = p.rv + 3 * (size_t)ch;
+                double ct = 0.;
+                ct = __dadd_rn(ct, __dmul_rn(rh[0], rv[0]));
+                ct = __dadd_rn(ct, __dmul_rn(rh[1], rv[1]));
+                ct = __dadd_rn(ct, __dmul_rn(rh[2], rv[2]));
+                ct = ct < 1.0 ? ct : 1.0;
+                ct = ct > -1.0 ? ct : -1.0;
+                const double theta = acos(ct);
+                o.Hramp = __dsub_rn(0.5, __dmul_rn(0.5, cos(__ddiv_rn(__dmul_rn(theta, 120.), 90.))));
+            }
+        }
+    } else if (hb == 4) {
+        const double cos_theta = negdot(rv);
+        o.rdon = (cos_theta <= 0.) ? 0. : __dmul_rn(cos_theta, cos_theta);
+    } else if (hb == 5 && !p.disorder[ia]) {
+        const double *rv2 = p.rv2 + 3 * (size_t)ia;
+        const double cos_theta = negdot(rv);
+        double t0 = 0.;
+        t0 = __dadd_rn(t0, __dmul_rn(dn0, rv2[0]));
+        t0 = __dadd_rn(t0, __dmul_rn(dn1, rv2[1]));
+        t0 = __dadd_rn(t0, __dmul_rn(dn2, rv2[2]));
+        if (t0 > 1.) t0 = 1.; else if (t0 < -1.) t0 = -1.;
+        t0 = __dsub_rn(PI_halved, acos(t0));
+        const double c0 = __dsub_rn(__dmul_rn(dn1, rv2[2]), __dmul_rn(dn2, rv2[1]));
+        const double c1 = __dsub_rn(__dmul_rn(dn2, rv2[0]), __dmul_rn(dn0, rv2[2]));
+        const double c2 = __dsub_rn(__dmul_rn(dn0, rv2[1]), __dmul_rn(dn1, rv2[0]));
+        double rd2 = __dadd_rn(__dadd_rn(__dmul_rn(c0, c0), __dmul_rn(c1, c1)), __dmul_rn(c2, c2));
+        if (rd2 < APPROX_ZERO_D) rd2 = APPROX_ZERO_D;
+        const double inv_rd = __ddiv_rn(1.0, __dsqrt_rn(rd2));
+        double ti = 0.;
+        ti = __dadd_rn(ti, __dmul_rn(__dmul_rn(c0, inv_rd), rv[0]));
+        ti = __dadd_rn(ti, __dmul_rn(__dmul_rn(c1, inv_rd), rv[1]));
+        ti = __dadd_rn(ti, __dmul_rn(__dmul_rn(c2, inv_rd), rv[2]));
+        o.rdon = 0.;
+        if (cos_theta >= 0.) {
+            if (ti > 1.) ti = 1.; else if (ti < -1.) ti = -1.;
+            ti = __dsub_rn(acos(ti), PI_halved);
+            if (ti < 0.) ti = -ti;
+            o.rdon = __dmul_rn(__dadd_rn(0.9, __dmul_rn(0.1, sin(__dadd_rn(ti, ti)))), cos(t0));
+        } else if (cos_theta >= -0.34202) {
+            const double b = __dsub_rn(0.116978, __dmul_rn(cos_theta, cos_theta));
+            o.rdon = __dmul_rn(__dmul_rn(562.25, pow(b, 3.)), cos(t0));
+        }
+    } else if (p.disorder[ia] && hb == 5) {
+        double cos_theta = negdot(rv);
+        if (cos_theta > 1.) cos_theta = 1.; else if (cos_theta < -1.) cos_theta = -1.;
+        const double theta = acos(cos_theta);
+        o.racc = 0.; o.rdon = 0.;
+        if (theta <= 1.24791 + PI_halved) {
+            o.rdon = pow(cos(__dsub_rn(theta, 1.24791)), 4.);
+            o.racc = o.rdon;
+        }
+    }
+}
+
+// FP32 pair quantities from the canonical frame-relative distance.  Returns
+// false when any quantity is within its error bound of a discontinuity; the
+// caller then uses pair_exact().
+__device__ __forceinline__ bool pair_fast(const DevProblem &p, const float *__restrict__ rvf,
+                                          const float *__restrict__ rv2f, int ia, float dX, float dY,
+                                          float dZ, float t, float rs, int ch, float3 rvh,
+                                          PairQ<float> &o)
+{
+    const float tf = floorf(t);
+    if (t - tf < GUARD_BIN || (tf + 1.f) - t < GUARD_BIN || t < 1.0f) return false;
+    o.bin = (int)tf;
+    o.bin_e = o.bin;
+    o.ad4_in = t < FAR_T0;  // t not within GUARD_BIN of 1024 here: equals r <= 8
+    const int dis = p.disorder[ia];
+    if (p.disorder_h && dis && p.type[ia] == p.hydrogen_type) o.ad4_in = 0;
+    o.r = t * (1.0f / AG_A_DIV);
+    o.inv_rmax = fminf((float)AG_A_DIV * rs, 2.0f);
+    o.racc = 1.f; o.rdon = 1.f; o.Hramp = 1.f;
+    o.ih = 0;
+    if (!o.ad4_in) return true;
+    if (dis) {
+        const float xh = t - 140.8f;  // (r - 1.10) * A_DIV
+        if (xh > 0.5f) {
+            const float xf = floorf(xh);
+            if (xh - xf < GUARD_BIN || (xf + 1.f) - xh < GUARD_BIN) return false;
+            o.ih = min((int)xf, AG_NEINT - 1);
+        }
+    }
+    const int hb = p.hbond[ia];
+    if (hb != 2 && hb != 4 && hb != 5) return true;
+    const float dn0 = dX * rs, dn1 = dY * rs, dn2 = dZ * rs;
+    const float rv0 = rvf[3 * ia], rv1 = rvf[3 * ia + 1], rv2 = rvf[3 * ia + 2];
+    const float cos_theta = ((0.f - dn0 * rv0) - dn1 * rv1) - dn2 * rv2;
+    const float PIH = 1.57079632679489662f;
+    // An atom without bonded neighbours keeps a zero bond vector; its cos_theta
+    // is exactly 0 in every precision, so the branch at 0 is not ambiguous.
+    const bool rv_zero = (rv0 == 0.f) & (rv1 == 0.f) & (rv2 == 0.f);
+    if (hb == 2) {
+        if (fabsf(cos_theta) < GUARD_COS && !rv_zero) return false;
+        if (cos_theta <= 0.f) {
+            o.racc = 0.f;
+        } else {
+            const int e = p.rexp[ia];
+            o.racc = (e == 2) ? cos_theta * cos_theta
+                   : (e == 4) ? (cos_theta * cos_theta) * (cos_theta * cos_theta) : cos_theta;
+            if (ia != ch) {
+                float ct = rvh.x * rv0 + rvh.y * rv1 + rvh.z * rv2;
+                ct = fminf(fmaxf(ct, -1.f), 1.f);
+                o.Hramp = 0.5f - 0.5f * cosf(acosf(ct) * (120.f / 90.f));
+            }
+        }
+    } else if (hb == 4) {
+        o.rdon = (cos_theta <= 0.f) ? 0.f : cos_theta * cos_theta;
+    } else if (!dis) {  // A2 ordered
+        if (fabsf(cos_theta) < GUARD_COS && !rv_zero) return false;
+        const float w0 = rv2f[3 * ia], w1 = rv2f[3 * ia + 1], w2 = rv2f[3 * ia + 2];
+        float t0 = dn0 * w0 + dn1 * w1 + dn2 * w2;
+        t0 = fminf(fmaxf(t0, -1.f), 1.f);
+        t0 = PIH - acosf(t0);
+        const float c0 = dn1 * w2 - dn2 * w1, c1 = dn2 * w0 - dn0 * w2, c2 = dn0 * w1 - dn1 * w0;
+        float rd2 = c0 * c0 + c1 * c1 + c2 * c2;
+        rd2 = fmaxf(rd2, 1.0e-6f);
+        const float inv_rd = rsqrtf(rd2);
+        float ti = (c0 * rv0 + c1 * rv1 + c2 * rv2) * inv_rd;
+        o.rdon = 0.f;
+        if (cos_theta >= 0.f) {
+            ti = fminf(fmaxf(ti, -1.f), 1.f);
+            ti = fabsf(acosf(ti) - PIH);
+            o.rdon = (0.9f + 0.1f * sinf(ti + ti)) * cosf(t0);
+        } else if (cos_theta >= -0.34202f) {
+            const float b = 0.116978f - cos_theta * cos_theta;
+            o.rdon = 562.25f * (b * b * b) * cosf(t0);
+        }
+    } else {  // A2 disordered (cylindrical hydroxyl)
+        const float ct = fminf(fmaxf(cos_theta, -1.f), 1.f);
+        const float theta = acosf(ct);
+        o.racc = 0.f; o.rdon = 0.f;
+        if (theta <= 1.24791f + PIH) {
+            const float c = cosf(theta - 1.24791f);
+            o.rdon = (c * c) * (c * c);
+            o.racc = o.rdon;
+        }
+    }
+    return true;
+}
+
+// ------------------------------------------------------------ closest H ---
+__global__ void __launch_bounds__(NB_THREADS)
+k_closest_h(DevProblem p, int *__restrict__ closest)
+{
+    __shared__ float4 s_h[NB_CHUNK];
+    const int tid = threadIdx.x;
+    const int nbx = (p.n1x + NB_X - 1) / NB_X, nby = (p.n1y + NB_Y - 1) / NB_Y;
+    const int b = blockIdx.x;
+    const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+    const int ix = bx * NB_X + (tid & 7), iy = by * NB_Y + ((tid >> 3) & 7), iz = bz * NB_Z + (tid >> 6);
+    const bool valid = ix < p.n1x && iy < p.n1y && iz < p.n1z;
+    const double sp128 = p.spacing * AG_A_DIV;
+    const double X0 = frame_origin_bins(bx * NB_X, p.nex, sp128);
+    const double Y0 = frame_origin_bins(by * NB_Y, p.ney, sp128);
+    const double Z0 = frame_origin_bins(bz * NB_Z, p.nez, sp128);
+    const float PX = frame_point_coord(tid & 7, sp128), PY = frame_point_coord((tid >> 3) & 7, sp128),
+                PZ = frame_point_coord(tid >> 6, sp128);
+    const double cx = (double)(ix - p.nex) * p.spacing, cy = (double)(iy - p.ney) * p.spacing,
+                 cz = (double)(iz - p.nez) * p.spacing;
+    float best2 = 3.0e38f;
+    for (int pass = 0; pass < 2; pass++) {
+        const float lim = best2 * (1.0f + 2.0e-5f) + 4.0f;
+        double rmin = 999999.;
+        int best = -1;
+        for (int h0 = 0; h0 < p.n_h; h0 += NB_CHUNK) {
+            const int nh = min(NB_CHUNK, p.n_h - h0);
+            __syncthreads();
+            if (tid < nh) {
+                const int a = p.h_index[h0 + tid];
+                s_h[tid] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0),
+                                       frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
+                                       frame_atom_coord(p.z[a] * AG_A_DIV, Z0), __int_as_float(a));
+            }
+            __syncthreads();
+            if (!valid) continue;
+            if (pass == 0) {
+                for (int j = 0; j < nh; j++) {
+                    const float4 A = s_h[j];
+                    const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
+                    best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
+                }
+            } else {
+                for (int j = 0; j < nh; j++) {
+                    const float4 A = s_h[j];
+                    const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
+                    if (dx * dx + dy * dy + dz * dz > lim) continue;
+                    const int a = __float_as_int(A.w);
+                    const double d0 = __dsub_rn(p.x[a], cx), d1 = __dsub_rn(p.y[a], cy), d2 = __dsub_rn(p.z[a], cz);
+                    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
+                    if (r < rmin) { rmin = r; best = a; }
+                }
+            }
+        }
+        if (pass == 1 && valid) closest[((long long)iz * p.n1y + iy) * p.n1x + ix] = best;
+    }
+}
+
+// ----------------------------------------------------------------- near ---
+template <bool EXACT>
+__global__ void __launch_bounds__(NB_THREADS)
+k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *__restrict__ rvf,
+       const float *__restrict__ rv2f, const float *__restrict__ vdwT, int mpad,
+       const float *__restrict__ etab, const float *__restrict__ solf, const double *__restrict__ cov_map,
+       float *__restrict__ out32, double *__restrict__ out64, unsigned long long *__restrict__ counters)
+{
+    using R = typename std::conditional<EXACT, double, float>::type;
+    __shared__ float4 s_pos[NB_CHUNK];
+    __shared__ int s_idx[NB_CHUNK];
+    __shared__ int s_seg_start[NB_SEGS], s_seg_off[NB_SEGS + 1];
+    __shared__ unsigned long long s_cnt[2];
+
+    const int tid = threadIdx.x;
+    if (tid < 2) s_cnt[tid] = 0ull;
+    const int nbx = (p.n1x + NB_X - 1) / NB_X, nby = (p.n1y + NB_Y - 1) / NB_Y;
+    const int b = blockIdx.x;
+    const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
+    const int ix = bx * NB_X + (tid & 7), iy = by * NB_Y + ((tid >> 3) & 7), iz = bz * NB_Z + (tid >> 6);
+    const bool valid = ix < p.n1x && iy < p.n1y && iz < p.n1z;
+    const long long lin = ((long long)iz * p.n1y + iy) * p.n1x + ix;
+
+    // far-kernel frame of this brick and the point's canonical coordinates
+    const double sp128 = p.spacing * AG_A_DIV;
+    const int ox = ((bx * NB_X) / FRAME_X) * FRAME_X, oy = ((by * NB_Y) / FRAME_Y) * FRAME_Y,
+              oz = ((bz * NB_Z) / FRAME_Z) * FRAME_Z;
+    const double X0 = frame_origin_bins(ox, p.nex, sp128), Y0 = frame_origin_bins(oy, p.ney, sp128),
+                 Z0 = frame_origin_bins(oz, p.nez, sp128);
+    const float PX = frame_point_coord(ix - ox, sp128), PY = frame_point_coord(iy - oy, sp128),
+                PZ = frame_point_coord(iz - oz, sp128);
+    const double cx = (double)(ix - p.nex) * p.spacing, cy = (double)(iy - p.ney) * p.spacing,
+                 cz = (double)(iz - p.nez) * p.spacing;
+    const int ch = (valid && p.n_atom_maps > 0) ? closest[lin] : -1;
+    float3 rvh = make_float3(0.f, 0.f, 0.f);
+    if (!EXACT && ch >= 0) rvh = make_float3(rvf[3 * ch], rvf[3 * ch + 1], rvf[3 * ch + 2]);
+
+    R E[NG_MAX], hmin[NG_MAX], hmax[NG_MAX];
+#pragma unroll
+    for (int m = 0; m < NG_MAX; m++) { E[m] = 0; hmin[m] = 999999.; hmax[m] = -999999.; }
+    uint32_t hflag = 0;
+    R D1 = 0, D2 = 0, e_near = 0;
+    unsigned long long n_near = 0, n_fb = 0;
+    const bool need_pairs = g.ng > 0 || (g.write_special && (p.dsolv_map >= 0 || (!EXACT && p.elec_map >= 0)));
+
+    // candidate cells: brick bounding box grown by the candidate radius
+    const double rc = AGB_NEAR_RADIUS;
+    const double bx0 = (double)(bx * NB_X - p.nex) * p.spacing, bx1 = (double)(min(bx * NB_X + NB_X - 1, p.n1x - 1) - p.nex) * p.spacing;
+    const double by0 = (double)(by * NB_Y - p.ney) * p.spacing, by1 = (double)(min(by * NB_Y + NB_Y - 1, p.n1y - 1) - p.ney) * p.spacing;
+    const double bz0 = (double)(bz * NB_Z - p.nez) * p.spacing, bz1 = (double)(min(bz * NB_Z + NB_Z - 1, p.n1z - 1) - p.nez) * p.spacing;
+    auto cell_lo = [&](double v, double o, int n) { int c = (int)floor((v - rc - o) / p.cell_size); return max(0, min(n - 1, c)); };
+    auto cell_hi = [&](double v, double o, int n) { int c = (int)floor((v + rc - o) / p.cell_size); return max(0, min(n - 1, c)); };
+    const int cxl = cell_lo(bx0, p.cell0[0], p.ncx), cxh = cell_hi(bx1, p.cell0[0], p.ncx);
+    const int cyl = cell_lo(by0, p.cell0[1], p.ncy), cyh = cell_hi(by1, p.cell0[1], p.ncy);
+    const int czl = cell_lo(bz0, p.cell0[2], p.ncz), czh = cell_hi(bz1, p.cell0[2], p.ncz);
+    const int nrow_y = cyh - cyl + 1;
+    const int nseg_total = need_pairs ? nrow_y * (czh - czl + 1) : 0;
+
+    for (int sb = 0; sb < nseg_total; sb += NB_SEGS) {
+        const int nseg = min(NB_SEGS, nseg_total - sb);
+        __syncthreads();
+        if (tid == 0) {
+            int off = 0;
+            for (int s = 0; s < nseg; s++) {
+                const int k = sb + s;
+                const int cyy = cyl + k % nrow_y, czz = czl + k / nrow_y;
+                const int c0 = (czz * p.ncy + cyy) * p.ncx + cxl, c1 = (czz * p.ncy + cyy) * p.ncx + cxh;
+                const int st = p.cell_start[c0], en = p.cell_start[c1 + 1];
+                s_seg_start[s] = st;
+                s_seg_off[s] = off;
+                off += en - st;
+            }
+            s_seg_off[nseg] = off;
+        }
+        __syncthreads();
+        const int total = s_seg_off[nseg];
+        for (int c0 = 0; c0 < total; c0 += NB_CHUNK) {
+            const int nc = min(NB_CHUNK, total - c0);
+            __syncthreads();
+            if (tid < nc) {
+                const int c = c0 + tid;
+                int s = 0;
+                while (s_seg_off[s + 1] <= c) s++;
+                const int a = p.cell_atoms[s_seg_start[s] + (c - s_seg_off[s])];
+                s_idx[tid] = a;
+                s_pos[tid] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0),
+                                         frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
+                                         frame_atom_coord(p.z[a] * AG_A_DIV, Z0), 0.f);
+            }
+            __syncthreads();
+            if (!valid) continue;
+            for (int j = 0; j < nc; j++) {
+                const int ia = s_idx[j];
+                PairQ<R> q;
+                bool e_pair;
+                if (EXACT) {
+                    const double d0 = __dsub_rn(p.x[ia], cx), d1 = __dsub_rn(p.y[ia], cy), d2 = __dsub_rn(p.z[ia], cz);
+                    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+                    if (r2 > AG_NBC * AG_NBC * 1.0001) continue;
+                    PairQ<double> qd;
+                    pair_exact(p, ia, cx, cy, cz, ch, qd);
+                    if (!qd.ad4_in) continue;
+                    q.ad4_in = 1; q.bin = qd.bin; q.bin_e = qd.bin_e; q.ih = qd.ih;
+                    q.r = (R)qd.r; q.inv_rmax = (R)qd.inv_rmax; q.racc = (R)qd.racc; q.rdon = (R)qd.rdon; q.Hramp = (R)qd.Hramp;
+                    e_pair = false;
+                } else {
+                    const float4 A = s_pos[j];
+                    const float dY = __fsub_rn(A.y, PY), dZ = __fsub_rn(A.z, PZ);
+                    const float s = __fmaf_rn(dY, dY, __fmaf_rn(dZ, dZ, TINY_T2));
+                    const float dX = __fsub_rn(A.x, PX);
+                    const float t2 = __fmaf_rn(dX, dX, s);
+                    const float rs = rsqrt_approx(t2);
+                    const float t = __fmul_rn(t2, rs);
+                    if (t >= FAR_T0 + GUARD_BIN) continue;
+                    e_pair = t < FAR_T0;  // the far-field kernel skips exactly these pairs
+                    PairQ<float> qf;
+                    if (!pair_fast(p, rvf, rv2f, ia, dX, dY, dZ, t, rs, ch, rvh, qf)) {
+                        PairQ<double> qd;
+                        pair_exact(p, ia, cx, cy, cz, ch, qd);
+                        qf.ad4_in = qd.ad4_in; qf.bin = qd.bin; qf.bin_e = qd.bin_e; qf.ih = qd.ih;
+                        qf.r = (float)qd.r; qf.inv_rmax = (float)qd.inv_rmax; qf.racc = (float)qd.racc;
+                        qf.rdon = (float)qd.rdon; qf.Hramp = (float)qd.Hramp;
+                        n_fb++;
+                    }
+                    q.ad4_in = qf.ad4_in; q.bin = qf.bin; q.bin_e = qf.bin_e; q.ih = qf.ih;
+                    q.r = qf.r; q.inv_rmax = qf.inv_rmax; q.racc = qf.racc; q.rdon = qf.rdon; q.Hramp = qf.Hramp;
+                    if (e_pair && g.write_special && p.elec_map >= 0) {
+                        const int ke = min(q.bin_e, AG_NDIEL - 1);
+                        e_near += (R)(etab[ke] * (float)p.q[ia]) * q.inv_rmax;
+                    }
+                    if (!q.ad4_in) continue;
+                }
+                n_near++;
+                const int kr = min(q.bin, AG_NDIEL - 1);
+                const int kn = min(q.bin, AG_NEINT - 1);
+                const R sol = EXACT ? (R)p.sol_fn[kr] : (R)solf[kr];
+                D1 += (R)p.vol[ia] * sol;
+                D2 += (R)(p.solpar[ia] + p.solpar_q * fabs(p.q[ia])) * sol;
+                if (g.ng == 0) continue;
+                const int hb = p.hbond[ia];
+                const int dis = p.disorder[ia];
+                const int ta = p.type[ia];
+                const float *Trow = vdwT + ((size_t)ta * AG_NEINT + kn) * mpad + g.g0;
+                const float *Hrow = (g.has_hrow && dis && p.hydrogen_type >= 0)
+                                        ? vdwT + ((size_t)p.hydrogen_type * AG_NEINT + q.ih) * mpad + g.g0 : Trow;
+#pragma unroll
+                for (int m = 0; m < NG_MAX; m++) {
+                    if (m >= g.ng) break;
+                    const int act = g.act[m][hb];
+                    if (act == ACT_SKIP) continue;
+                    const R T = (R)__ldg(Trow + m);
+                    if (act == ACT_PLAIN) { E[m] += T; continue; }
+                    R rsph = T / (R)100.;
+                    rsph = rsph > (R)0 ? rsph : (R)0;
+                    rsph = rsph < (R)1 ? rsph : (R)1;
+                    if (act == ACT_SUMA) {
+                        const R Tv = dis ? (R)__ldg(Hrow + m) : T;
+                        E[m] += Tv * q.Hramp * (q.racc + ((R)1 - q.racc) * rsph);
+                    } else if (act == ACT_MMA) {
+                        const R v = T * (q.racc + ((R)1 - q.racc) * rsph);
+                        hmin[m] = hmin[m] < v ? hmin[m] : v;
+                        hmax[m] = hmax[m] > v ? hmax[m] : v;
+                        hflag |= 1u << m;
+                    } else {  // ACT_MMD
+                        if (dis) {
+                            E[m] += (R)__ldg(Hrow + m) * q.Hramp * (q.rdon + ((R)1 - q.rdon) * rsph);
+                        } else {
+                            const R v = T * (q.rdon + ((R)1 - q.rdon) * rsph);
+                            hmin[m] = hmin[m] < v ? hmin[m] : v;
+                            hmax[m] = hmax[m] > v ? hmax[m] : v;
+                            hflag |= 1u << m;
+                        }
+                    }
+                }
+            }
+        }
+    }
+
+    // finalise (main.cpp:3420-3431) and store
+    if (valid) {
+#pragma unroll
+        for (int m = 0; m < NG_MAX; m++) {
+            if (m >= g.ng) break;
+            R v = E[m];
+            if (hflag & (1u << m)) v += hmin[m] + (hmax[m] > (R)0 ? hmax[m] : (R)0);
+            v += (R)g.sp[m] * D1 + (R)g.vp[m] * D2;
+            const size_t o = (size_t)(g.g0 + m) * (size_t)p.P + (size_t)lin;
+            if (g.cov[m]) {
+                if (EXACT) out64[o] = cov_map[lin]; else out32[o] = (float)cov_map[lin];
+            } else {
+                if (EXACT) out64[o] = (double)v; else out32[o] = (float)v;
+            }
+        }
+        if (g.write_special) {
+            if (p.dsolv_map >= 0) {
+                const size_t o = (size_t)p.dsolv_map * (size_t)p.P + (size_t)lin;
+                const R d = (R)p.solpar_q * D1;
+                if (EXACT) out64[o] = (double)d; else out32[o] = (float)d;
+            }
+            if (!EXACT && p.elec_map >= 0) {
+                float e = 0.f;
+                for (int c = 0; c < p.far_chunks; c++) e += p.far_partial[(size_t)c * (size_t)p.P + (size_t)lin];
+                out32[(size_t)p.elec_map * (size_t)p.P + (size_t)lin] = e + (float)e_near;
+            }
+        }
+    }
+    if (counters) {
+        atomicAdd(&s_cnt[0], n_near);
+        atomicAdd(&s_cnt[1], n_fb);
+        __syncthreads();
+        if (tid == 0) {
+            atomicAdd(counters + 0, s_cnt[0]);
+            atomicAdd(counters + 1, s_cnt[1]);
+        }
+    }
+}
+
+// Covalent map(s), main.cpp:2866-2879, in FP64 (a handful of flops per point).
+__global__ void k_covalent(DevProblem p, double *__restrict__ cov)
+{
+    const long long lin = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (lin >= p.P) return;
+    const int ix = (int)(lin % p.n1x), iy = (int)((lin / p.n1x) % p.n1y), iz = (int)(lin / ((long long)p.n1x * p.n1y));
+    const double d0 = __dsub_rn(p.cov_pos[0], (double)(ix - p.nex) * p.spacing);
+    const double d1 = __dsub_rn(p.cov_pos[1], (double)(iy - p.ney) * p.spacing);
+    const double d2 = __dsub_rn(p.cov_pos[2], (double)(iz - p.nez) * p.spacing);
+    double rcov = __ddiv_rn(__dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2))),
+                            p.cov_half_width);
+    if (rcov < APPROX_ZERO_D) rcov = APPROX_ZERO_D;
+    cov[lin] = __dmul_rn(p.cov_barrier, __dsub_rn(1., exp(__dmul_rn(__dmul_rn(log(0.5), rcov), rcov))));
+}
+
+}  // namespace agb
+
+namespace agb {
+
+static unsigned near_blocks(const DevProblem &p)
+{
+    return (unsigned)(((p.n1x + NB_X - 1) / NB_X) * ((p.n1y + NB_Y - 1) / NB_Y) * ((p.n1z + NB_Z - 1) / NB_Z));
+}
+
+cudaError_t launch_closest_h(const DevProblem &p, int *closest, cudaStream_t s)
+{
+    k_closest_h<<<near_blocks(p), NB_THREADS, 0, s>>>(p, closest);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s)
+{
+    k_covalent<<<(unsigned)((p.P + 255) / 256), 256, 0, s>>>(p, cov);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const int *closest,
+                        const float *rvf, const float *rv2f, const float *vdwT, int mpad, const float *etab,
+                        const float *solf, const double *cov_map, float *out32, double *out64,
+                        unsigned long long *counters, cudaStream_t s)
+{
+    if (exact)
+        k_near<true><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, closest, rvf, rv2f, vdwT, mpad, etab, solf,
+                                                         cov_map, out32, out64, counters);
+    else
+        k_near<false><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, closest, rvf, rv2f, vdwT, mpad, etab, solf,
+                                                          cov_map, out32, out64, counters);
+    return cudaGetLastError();
+}
+
+}  // namespace agb

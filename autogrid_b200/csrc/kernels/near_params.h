@@ -1,0 +1,30 @@
+// Parameters shared by the host orchestration and the near-field kernel.
+#pragma once
+#include <cstdint>
+
+namespace agb {
+
+constexpr int NG_MAX = 16;                 // ligand maps per near-kernel launch
+constexpr double AGB_NEAR_RADIUS = 8.05;   // A; > 8 A cutoff + FP32 distance error
+constexpr double AGB_CELL = 4.0;           // A; cell-list edge
+
+// What one (ligand map, receptor-atom hbond class) pair contributes, after
+// main.cpp:3286-3379.  Desolvation is handled separately (factored).
+enum : uint8_t {
+    ACT_SKIP = 0,  // covalent map, or the desolvation partner of a separate_desolvation_maps pair
+    ACT_PLAIN,     // E += T
+    ACT_SUMA,      // probe acceptor vs receptor donor: E += T*Hramp*(racc+(1-racc)rsph)
+    ACT_MMA,       // A1/AD probe vs donor: hbondmin/max of T*(racc+(1-racc)rsph)
+    ACT_MMD        // donor probe vs acceptor: hbondmin/max of T*(rdon+(1-rdon)rsph)
+};
+
+struct NearGroup {
+    int g0, ng;               // ligand maps [g0, g0+ng)
+    int write_special;        // this launch also writes the d and e maps
+    int has_hrow;             // some action reads the hydrogen row (disorder_h)
+    uint8_t act[NG_MAX][8];   // by receptor hbond class 0..6
+    uint8_t cov[NG_MAX];
+    double sp[NG_MAX], vp[NG_MAX];  // desolvation factors applied to this map's output
+};
+
+}  // namespace agb

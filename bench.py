@@ -1,0 +1,338 @@
+"""Benchmark of the AutoGrid4 map hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
+
+Metric: grid-point x map-type evaluations per second (P * M / time) for the
+plain large map set: a seeded synthetic 10,000-atom receptor in a 45 A sphere,
+npts 126^3 (127^3 = 2,048,383 points), 14 ligand types + e + d = 16 maps,
+spacing 0.375 A, distance-dependent dielectric.  One step = one full map set.
+
+  value    device-resident: ag_plan_run over inputs already in HBM; L2 is
+           flushed (256 MiB write) before every timed step; CUDA events.
+  e2e      the public C ABI call ag_maps_compute with host inputs and a pinned
+           host output: host preparation, H2D, kernels and D2H every step.
+  roofline the dominant kernel (far-field e map, k_emap_far): algorithmic pair
+           terms per second (1 rsqrt each) against the measured MUFU rsqrt rate
+           of this GPU.
+  cpu_baseline  the reference's own OpenMP build (oracle/_ref/autogrid4,
+           compiled from the reference sources) on a bounded sample of the same
+           workload: same receptor and 16 maps, fewer z-planes.
+
+Multi-GPU (torchrun): one independent map set per rank (weak scaling, no
+collective on the data path); time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+WORKLOAD = "ad4_10000_127cube_16maps"
+METRIC = "grid-pt*type evals/s (plain 127^3 x 16-map AD4 set, 10k-atom receptor)"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_info():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=self.out, stderr=subprocess.DEVNULL)
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.flush()
+        rows = [r.split(",") for r in Path(self.out.name).read_text().strip().splitlines() if r.strip()]
+        os.unlink(self.out.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1])); mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_problem(workload: str, seed: int, workdir: Path):
+    from autogrid_b200 import Job, synth
+    rec, spec = synth.workload(workload, seed=seed)
+    gpf = synth.write_case(workdir, "bench", rec, spec)
+    cwd = os.getcwd()
+    os.chdir(workdir)
+    try:
+        job = Job(gpf.name, "bench.glg")
+        prob = job.problem()
+    finally:
+        os.chdir(cwd)
+    return rec, spec, job, prob
+
+
+def reference_sample(rec, spec, workdir: Path, threads: int):
+    """Run the reference OpenMP binary on a z-slab of the workload; returns
+    (evals/s, seconds, points, maps, description)."""
+    from autogrid_b200 import synth
+    from oracle.oracle import REF_BIN
+    if not REF_BIN.exists():
+        return None
+    nz = max(2, 4 * threads)  # about 4 planes per thread (schedule(static,4))
+    sub = synth.GridSpec(npts=(spec.npts[0], spec.npts[1], nz), spacing=spec.spacing,
+                         ligand_types=list(spec.ligand_types))
+    d = workdir / "ref"
+    synth.write_case(d, "ref", rec, sub)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    t0 = time.perf_counter()
+    r = subprocess.run([str(REF_BIN), "-p", "ref.gpf", "-l", "ref.glg"], cwd=d, env=env,
+                       capture_output=True, text=True)
+    dt = time.perf_counter() - t0
+    if r.returncode != 0 or "Successful Completion" not in (d / "ref.glg").read_text():
+        return None
+    P = (sub.npts[0] + 1) * (sub.npts[1] + 1) * (nz + 1)
+    M = len(spec.ligand_types) + 2
+    desc = (f"reference autogrid4 (OpenMP, {threads} threads) on the same receptor and {M} maps, "
+            f"npts {sub.npts[0]}x{sub.npts[1]}x{nz} ({P} points); whole-process wall time")
+    return P * M / dt, dt, P, M, desc
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_info()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    from autogrid_b200 import Context, load_library
+    from autogrid_b200._abi import ag_stats  # noqa: F401
+
+    work = Path(tempfile.mkdtemp(prefix=f"agb_bench_r{rank}_"))
+    rec, spec, job, prob = make_problem(args.workload, seed=rank, workdir=work)
+    P, M = prob.points, prob.n_maps
+    ctx = Context(local)
+    plan = ctx.plan(prob)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    for _ in range(args.warmup):
+        plan.run(sptr)
+    torch.cuda.synchronize()
+
+    # ---------------- device-resident timed region ----------------
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record(stream)
+        plan.run(sptr)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = float(np.mean(step_ms))
+    plan.download()
+    st = ctx.stats()
+    launches_per_step = st.gpu_launches
+
+    # dominant kernel alone: far-field e map (events around its launch)
+    lib = load_library()
+    ker_ms = far_kernel_ms(ctx, plan, stream, args.steps)
+
+    # ---------------- end to end through the C ABI ----------------
+    out = torch.empty(prob.map_shape, dtype=torch.float32, pin_memory=True).numpy()
+    ctx.compute(prob, "fp32", out=out)  # warm the context's buffers
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e2e_t = []
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        ctx.compute(prob, "fp32", out=out)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_s = float(np.mean(e2e_t))
+
+    t = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_s = float(t[0]), float(t[1])
+
+    if rank == 0:
+        evals = P * M * world
+        rate_r, rate_f, clk_nominal = peak_rates(lib, local)
+        pairs = prob.points * prob.n_atoms  # far-field pair terms (near pairs excluded are < 1%)
+        achieved = pairs / (ker_ms * 1e-3) if ker_ms else None
+        roof = {
+            "bound": "sfu", "kernel": "k_emap_far",
+            "achieved": achieved / 1e9 if achieved else None, "peak": rate_r / 1e9 if rate_r else None,
+            "unit": "Grsqrt/s", "frac": (achieved / rate_r) if (achieved and rate_r) else None,
+            "traffic": profile_traffic("k_emap_far"),
+            "peak_source": "measured on this GPU: rsqrt.approx.f32 microbenchmark (ag_diag_peak_rates)",
+            "units_per_launch": f"{pairs} (point, atom) pair terms, 1 rsqrt each",
+            "kernel_ms": ker_ms, "fp32_peak_tflops_measured": rate_f / 1e12 if rate_f else None,
+        }
+        line = {
+            "metric": METRIC, "value": evals / (ms * 1e-3), "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 fallback near table-bin edges)",
+            "data": "synthetic (seeded receptor, shapes of the plain large map set)",
+            "config": {"workload": args.workload, "atoms": prob.n_atoms, "points": P, "maps": M,
+                       "npts": list(spec.npts), "spacing": spec.spacing, "parallelism": f"replica x{world}",
+                       "l2": "flushed (256 MiB write) before every timed step"},
+            "e2e": {"value": evals / e2e_s, "unit": "evals/s", "ms_per_step": e2e_s * 1e3,
+                    "h2d_bytes_per_step": prob.bytes_h2d(), "d2h_bytes_per_step": P * M * 4},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": roof,
+            "clocks": clk,
+            "diagnostics": {"near_pairs_per_step": st.near_pairs, "fp64_fallbacks_per_step": st.fp64_fallbacks},
+        }
+        if not args.no_cpu_baseline and world == 1:
+            threads = min(32, os.cpu_count() or 1)
+            res = reference_sample(rec, spec, work, threads)
+            if res:
+                rate, dt, Ps, Ms, desc = res
+                line["cpu_baseline"] = {"value": rate, "unit": "evals/s", "cores": threads,
+                                        "kind": "reference", "sample": desc, "seconds": dt}
+        print(json.dumps(line))
+    plan.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    shutil.rmtree(work, ignore_errors=True)
+
+
+def far_kernel_ms(ctx, plan, stream, steps):
+    """Device time of k_emap_far (events recorded around its launch by the
+    library), averaged over L2-flushed runs."""
+    import torch
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    vals = []
+    for _ in range(max(3, min(steps, 10))):
+        flush.zero_()
+        plan.run(stream.cuda_stream)
+        vals.append(ctx.stats().far_ms)
+    return float(np.mean(vals))
+
+
+def peak_rates(lib, device):
+    import ctypes as C
+    try:
+        fn = lib.ag_diag_peak_rates
+    except AttributeError:
+        return None, None, None
+    fn.restype = C.c_int
+    fn.argtypes = [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    r, f, c = C.c_double(), C.c_double(), C.c_double()
+    if fn(device, C.byref(r), C.byref(f), C.byref(c)) != 0:
+        return None, None, None
+    return r.value, f.value, c.value
+
+
+def profile_traffic(kernel: str):
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        return json.loads(p.read_text()).get(kernel, {}).get("dram_bytes_per_launch")
+    except (ValueError, OSError):
+        return None
+
+
+def run_reference(args, rank, world):
+    """The reference's own CPU implementation (OpenMP build from its sources),
+    rank 0 only, each step a bounded z-slab sample of the workload."""
+    if rank != 0:
+        return
+    from oracle.oracle import REF_BIN
+    if not REF_BIN.exists():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/autogrid4 was not built"}))
+        return
+    from autogrid_b200 import synth
+    rec, spec = synth.workload(args.workload, seed=0)
+    work = Path(tempfile.mkdtemp(prefix="agb_ref_"))
+    threads = min(32, os.cpu_count() or 1)
+    for _ in range(args.warmup):
+        reference_sample(rec, spec, work, threads)
+    rates, secs = [], []
+    desc = ""
+    for _ in range(args.steps):
+        res = reference_sample(rec, spec, work, threads)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
+            return
+        rate, dt, P, M, desc = res
+        rates.append(rate)
+        secs.append(dt)
+    v = float(np.mean(rates))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.mean(secs)) * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded receptor, shapes of the plain large map set)",
+            "config": {"workload": args.workload, "sample": desc},
+            "cpu_baseline": {"value": v, "unit": "evals/s", "cores": threads, "kind": "reference", "sample": desc},
+            "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    shutil.rmtree(work, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,209 @@
+/*
+ * autogrid_b200.h -- C ABI of the B200-native AutoGrid4 map engine.
+ *
+ * The reference (AutoGrid 4.2.8) has no library interface: its hot path is the
+ * inline per-grid-point loop of main() (main.cpp:2785-3464), fed by globals
+ * that the GPF/PDBQT/parameter front end fills (main.cpp:778-2736) and read by
+ * the map writers (main.cpp:3481-3546).  This header is the seam a maintainer
+ * would cut there:
+ *
+ *   front end  : ag_job_load()          <- main.cpp:214-2776 (GPF, parameter
+ *                                          library, receptor, tables, bond vectors)
+ *   hot path   : ag_maps_compute*()     <- main.cpp:2805-3464 (grid-point loop)
+ *   back end   : ag_job_write_maps_*()  <- main.cpp:3481-3565 (map files, summary)
+ *
+ * Plain C types only; every pointer is host memory unless a function says
+ * otherwise.  Errors are returned as ag_status codes (the reference calls
+ * exit(1) through print_error(FATAL_ERROR), main.cpp:172-176); the message is
+ * available from ag_last_error().  One host thread per context.
+ */
+#ifndef AUTOGRID_B200_H
+#define AUTOGRID_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AG_ABI_VERSION 1
+
+/* Table geometry of the reference build (-DUSE_8A_NBCUTOFF):
+ * NEINT = NBC*A_DIV = 8*128 (constants.h:149-160), NDIEL = 64*128
+ * (constants.h:170-171).  Bin of a distance r is (int)(r*A_DIV)
+ * (autogrid.h:89). */
+#define AG_A_DIV        128
+#define AG_NEINT        1024
+#define AG_NDIEL        8192
+#define AG_NBC          8.0
+#define AG_MAX_MAPS     128      /* autocomm.h:93-94 */
+#define AG_MAX_REC_TYPES 20      /* autogrid.h:98 NUM_RECEPTOR_TYPES */
+#define AG_MAX_ATOMS    100000   /* autogrid.h:58 AG_MAX_ATOMS */
+#define AG_MAX_GRID_PTS 1025     /* autocomm.h:87 */
+
+typedef enum ag_status {
+    AG_OK               = 0,
+    AG_ERR_INVALID      = 1,  /* inconsistent problem / bad argument            */
+    AG_ERR_FATAL_INPUT  = 2,  /* a reference FATAL_ERROR condition (GPF, PDBQT,
+                                 parameters); message in ag_last_error()        */
+    AG_ERR_NO_CLOSEST_H = 3,  /* main.cpp:3011-3014 "no closestH atom was found" */
+    AG_ERR_UNSUPPORTED  = 4,  /* requested a mode this build does not provide   */
+    AG_ERR_CUDA         = 5,  /* CUDA runtime error; message names the call      */
+    AG_ERR_NO_DEVICE    = 6,  /* no CUDA device / extension not usable          */
+    AG_ERR_TOO_LARGE    = 7,  /* size beyond a stated limit                      */
+    AG_ERR_IO           = 8,  /* file could not be opened or written            */
+    AG_ERR_TIMEOUT      = 9   /* bounded wait on the device expired              */
+} ag_status;
+
+/* hbond classes, parameters.h:36-37 enum hbond_type */
+enum { AG_HB_NON = 0, AG_HB_DS = 1, AG_HB_D1 = 2, AG_HB_AS = 3, AG_HB_A1 = 4,
+       AG_HB_A2 = 5, AG_HB_AD = 6 };
+
+/*
+ * One receptor/box instance: a flat structure-of-arrays image of the globals
+ * the reference's grid loop reads (main.cpp:360-379 atoms, :289-315 MapObject,
+ * ad4_shared/structs.h:257-268 EnergyTables).  All arrays are owned by the
+ * caller.  Coordinates are already centred on the grid centre, exactly as the
+ * reference leaves coord[][] after the gridcenter keyword (main.cpp:1135-1139).
+ */
+typedef struct ag_problem {
+    /* receptor atoms, in PDBQT file order */
+    int32_t        n_atoms;
+    const double  *coord;        /* [n_atoms*3]  x,y,z (Angstrom, centred)        */
+    const double  *charge;       /* [n_atoms]                                      */
+    const double  *vol;          /* [n_atoms]    atomic fragmental volume          */
+    const double  *solpar;       /* [n_atoms]    atomic solvation parameter        */
+    const int32_t *rec_type;     /* [n_atoms]    receptor type index               */
+    const int32_t *hbond;        /* [n_atoms]    AG_HB_*                           */
+    const int32_t *rexp;         /* [n_atoms]    D1 directionality exponent        */
+    const double  *rvector;      /* [n_atoms*3]  bond vector (main.cpp:2301-2659)  */
+    const double  *rvector2;     /* [n_atoms*3]  lone-pair plane normal (A2)       */
+    const uint8_t *disorder;     /* [n_atoms]    disorder_h flags (main.cpp:2684)  */
+
+    /* grid: n1 = npts+1 (odd) points per axis, icoord = i - ne, c = icoord*spacing */
+    int32_t n1[3];
+    int32_t ne[3];
+    double  spacing;
+
+    /* maps: indices 0..n_atom_maps-1 are ligand-type maps (with their
+     * desolvation partner maps when separate_desolvation_maps is on); the
+     * electrostatic and desolvation maps sit at elec_map / dsolv_map
+     * (GPF order, main.cpp:1505-1544), -1 when not requested. */
+    int32_t        n_rec_types;
+    int32_t        n_atom_maps;
+    int32_t        n_maps;
+    int32_t        elec_map;
+    int32_t        dsolv_map;
+    const int32_t *map_is_covalent;  /* [n_atom_maps] */
+    const int32_t *map_is_hbonder;   /* [n_atom_maps] */
+    const int32_t *map_hbond;        /* [n_atom_maps] AG_HB_* of the probe type */
+    const double  *map_solpar_probe; /* [n_atom_maps] */
+    const double  *map_vol_probe;    /* [n_atom_maps] */
+
+    /* lookup tables, as the reference stores them */
+    const float   *e_vdw_hb;     /* [n_rec_types][n_atom_maps][AG_NEINT] float    */
+    const double  *sol_fn;       /* [AG_NDIEL] coeff_desolv*exp(-r^2/(2*3.6^2))   */
+    const double  *r_epsilon_fn; /* [AG_NDIEL] 332/eps(r) (dddiel only)            */
+
+    /* scalars */
+    int32_t dddiel;              /* distance-dependent dielectric (GPF dielectric <0) */
+    double  invdielcal;          /* 332/diel for a constant dielectric            */
+    double  coeff_estat;         /* AD4.coeff_estat                                */
+    double  solpar_q;            /* qasp                                           */
+    int32_t disorder_h;
+    int32_t hydrogen_type;       /* receptor index of type "HD", -1 if absent      */
+    int32_t separate_desolvation_maps;
+    double  cov_pos[3];          /* covalent attachment point (centred)           */
+    double  cov_half_width;
+    double  cov_barrier;
+    int32_t floating_grid;       /* fmap requested (not provided by this build)  */
+    int32_t constriction_grid;   /* cmap requested (not provided by this build)  */
+    double  constriction_cutoff;
+} ag_problem;
+
+enum { AG_PREC_FP32 = 0,   /* production path                                  */
+       AG_PREC_FP64 = 1 }; /* FP64 GPU twin: the stated error oracle           */
+enum { AG_TABLE_NEAREST = 0 }; /* reference nearest-bin tables (drop-in)       */
+
+typedef struct ag_opts {
+    int32_t precision;   /* AG_PREC_*                                          */
+    int32_t table_mode;  /* AG_TABLE_*                                         */
+    int32_t reserved[6]; /* zero                                               */
+} ag_opts;
+
+/* Diagnostics of the last compute or plan run on a context (FP32 path);
+ * ag_context_stats() waits for that run to finish. */
+typedef struct ag_stats {
+    int64_t near_pairs;        /* (point, atom) pairs inside 8 A evaluated       */
+    int64_t fp64_fallbacks;    /* pairs re-evaluated in FP64 because an FP32
+                                  distance fell within its error bound of a
+                                  bin edge, the cutoff or an angular branch     */
+    int64_t far_pairs;         /* e-map pairs evaluated by the far-field kernel  */
+    int32_t gpu_launches;      /* kernels launched by the call                   */
+    int32_t reserved;
+    double  kernel_ms;         /* device time of the call's kernels (events)    */
+    double  far_ms;            /* device time of the far-field e-map kernel      */
+} ag_stats;
+
+typedef struct ag_context ag_context;
+
+/* Library / device --------------------------------------------------------- */
+const char *ag_last_error(void);
+int32_t     ag_abi_version(void);
+ag_status   ag_context_create(int32_t device, ag_context **out);
+ag_status   ag_context_destroy(ag_context *ctx);
+ag_status   ag_context_stats(const ag_context *ctx, ag_stats *out);
+
+/*
+ * Hot path (replaces main.cpp:2805-3464).
+ *
+ * maps: [problem->n_maps][n1[2]][n1[1]][n1[0]] with X fastest, one contiguous
+ * array per map, in the reference's gridmap order (main.cpp:321-322).  The
+ * problem arrays are host memory; `maps` may be host (pinned or pageable) or
+ * device memory (CUDA unified addressing decides).  Device buffers are owned by
+ * the context and reused across calls; the call returns when the maps are in
+ * place.
+ */
+ag_status ag_maps_compute(ag_context *ctx, const ag_problem *problem,
+                          const ag_opts *opts, float *maps);
+/* Same, FP64 output (opts->precision must be AG_PREC_FP64). */
+ag_status ag_maps_compute_f64(ag_context *ctx, const ag_problem *problem,
+                              const ag_opts *opts, double *maps);
+
+/*
+ * Device-resident plan: the problem is validated and uploaded once, device
+ * scratch (cell list, sorted atom tiles, padded tables) is allocated once,
+ * and ag_plan_run() only launches kernels on `stream` (a cudaStream_t, or
+ * NULL for the context's stream); results stay in plan-owned device memory.
+ */
+typedef struct ag_plan ag_plan;
+ag_status    ag_plan_create(ag_context *ctx, const ag_problem *problem,
+                            const ag_opts *opts, ag_plan **out);
+ag_status    ag_plan_run(ag_plan *plan, void *stream);
+const float *ag_plan_device_maps(const ag_plan *plan);   /* device pointer  */
+size_t       ag_plan_points(const ag_plan *plan);        /* n1x*n1y*n1z     */
+ag_status    ag_plan_download(ag_plan *plan, float *host_maps);
+ag_status    ag_plan_destroy(ag_plan *plan);
+
+/* Front / back end (replaces main.cpp:214-2776 and :3481-3565) ------------- */
+typedef struct ag_job ag_job;
+
+/* Parse a GPF exactly as autogrid4 -p gpf -l glg would (relative file names
+ * resolve against the current directory), read the receptor and parameter
+ * library, build energy tables and bond vectors, open the map files and
+ * write the .fld/.xyz files.  glg_path may be NULL (log to stdout). */
+ag_status          ag_job_load(const char *gpf_path, const char *glg_path, ag_job **out);
+const ag_problem  *ag_job_problem(const ag_job *job);
+/* Write the map files (main.cpp:3481-3519) and the GLG extrema summary and
+ * completion line (main.cpp:3530-3565) from FP32 or FP64 maps. */
+ag_status          ag_job_write_maps_f32(ag_job *job, const float *maps);
+ag_status          ag_job_write_maps_f64(ag_job *job, const double *maps);
+/* Record a fatal error in the job's GLG ("Unsuccessful Completion"). */
+void               ag_job_fail(ag_job *job, const char *message);
+void               ag_job_free(ag_job *job);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AUTOGRID_B200_H */
