@@ -89,7 +89,7 @@ __device__ __noinline__ void pair_exact(const DevProblem &p, int ia, double cx, 
             if (e == 2) o.racc = __dmul_rn(cos_theta, cos_theta);
             else if (e == 4) { const double t = __dmul_rn(cos_theta, cos_theta); o.racc = __dmul_rn(t, t); }
             else o.racc = cos_theta;
-            if (ia == ch) {
+            if (ia == ch || ch < 0) {  // ch < 0 only when no ligand map needs Hramp
                 o.Hramp = 1.;
             } else {
                 const double *rh = p.rv + 3 * (size_t)ch;
@@ -192,7 +192,7 @@ __device__ __forceinline__ bool pair_fast(const DevProblem &p, const float *__re
             const int e = p.rexp[ia];
             o.racc = (e == 2) ? cos_theta * cos_theta
                    : (e == 4) ? (cos_theta * cos_theta) * (cos_theta * cos_theta) : cos_theta;
-            if (ia != ch) {
+            if (ia != ch && ch >= 0) {
                 float ct = rvh.x * rv0 + rvh.y * rv1 + rvh.z * rv2;
                 ct = fminf(fmaxf(ct, -1.f), 1.f);
                 o.Hramp = 0.5f - 0.5f * cosf(acosf(ct) * (120.f / 90.f));
