@@ -119,14 +119,15 @@ def make_problem(workload: str, seed: int, workdir: Path):
     return rec, spec, job, prob
 
 
-def reference_sample(rec, spec, workdir: Path, threads: int):
+def reference_sample(rec, spec, workdir: Path, threads: int, planes_per_thread: int = 4):
     """Run the reference OpenMP binary on a z-slab of the workload; returns
     (evals/s, seconds, points, maps, description)."""
     from autogrid_b200 import synth
     from oracle.oracle import REF_BIN
     if not REF_BIN.exists():
         return None
-    nz = max(2, 4 * threads)  # about 4 planes per thread (schedule(static,4))
+    # the reference hands out z-planes in blocks of 4 (schedule(static,4), main.cpp:2805)
+    nz = max(2, planes_per_thread * threads)
     sub = synth.GridSpec(npts=(spec.npts[0], spec.npts[1], nz), spacing=spec.spacing,
                          ligand_types=list(spec.ligand_types))
     d = workdir / "ref"
@@ -311,11 +312,11 @@ def run_reference(args, rank, world):
     work = Path(tempfile.mkdtemp(prefix="agb_ref_"))
     threads = min(32, os.cpu_count() or 1)
     for _ in range(args.warmup):
-        reference_sample(rec, spec, work, threads)
+        reference_sample(rec, spec, work, 1, planes_per_thread=2)
     rates, secs = [], []
     desc = ""
     for _ in range(args.steps):
-        res = reference_sample(rec, spec, work, threads)
+        res = reference_sample(rec, spec, work, threads, planes_per_thread=1)
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
             return
