@@ -119,17 +119,17 @@ def make_problem(workload: str, seed: int, workdir: Path):
     return rec, spec, job, prob
 
 
-def reference_sample(rec, spec, workdir: Path, threads: int, planes_per_thread: int = 4):
-    """Run the reference OpenMP binary on a z-slab of the workload; returns
-    (evals/s, seconds, points, maps, description)."""
+def reference_sample(rec, spec, workdir: Path, threads: int, nxy: int = 48):
+    """Run the reference OpenMP binary on a centred sub-box of the workload
+    (nxy x nxy x 4*threads npts; the reference hands out z-planes in blocks of
+    4, schedule(static,4) at main.cpp:2805, so 4 planes per thread keeps every
+    thread busy).  Returns (evals/s, seconds, points, maps, description)."""
     from autogrid_b200 import synth
     from oracle.oracle import REF_BIN
     if not REF_BIN.exists():
         return None
-    # the reference hands out z-planes in blocks of 4 (schedule(static,4), main.cpp:2805)
-    nz = max(2, planes_per_thread * threads)
-    sub = synth.GridSpec(npts=(spec.npts[0], spec.npts[1], nz), spacing=spec.spacing,
-                         ligand_types=list(spec.ligand_types))
+    nz = max(2, 4 * threads)
+    sub = synth.GridSpec(npts=(nxy, nxy, nz), spacing=spec.spacing, ligand_types=list(spec.ligand_types))
     d = workdir / "ref"
     synth.write_case(d, "ref", rec, sub)
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
@@ -165,8 +165,11 @@ def main():
     ctx = Context(local)
     plan = ctx.plan(prob)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it, and the events below are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sptr = stream.cuda_stream
+    assert sptr, "need a non-default CUDA stream"
 
     for _ in range(args.warmup):
         plan.run(sptr)
@@ -312,11 +315,11 @@ def run_reference(args, rank, world):
     work = Path(tempfile.mkdtemp(prefix="agb_ref_"))
     threads = min(32, os.cpu_count() or 1)
     for _ in range(args.warmup):
-        reference_sample(rec, spec, work, 1, planes_per_thread=2)
+        reference_sample(rec, spec, work, 1, nxy=4)
     rates, secs = [], []
     desc = ""
     for _ in range(args.steps):
-        res = reference_sample(rec, spec, work, threads, planes_per_thread=1)
+        res = reference_sample(rec, spec, work, threads, nxy=24)
         if res is None:
             print(json.dumps({"impl": "reference", "unavailable": "reference run failed"}))
             return

@@ -1,0 +1,119 @@
+"""Pin the FP64 oracle (oracle/ag_oracle.c) -- together with the C++ front end
+that builds its input -- against the reference itself:
+
+  * tests/golden/*.npz: maps the reference's own build printed at full float
+    precision (tests/golden/make_golden.py) for seeded synthetic cases covering
+    disorder_h, separate desolvation maps, a covalent map, constant dielectric,
+    nbp_r_eps / nbp_coeffs overrides, odd npts and a single-point grid;
+  * the reference test-suite's golden maps Tests/py_hsg1_sm.*.map, with the
+    reference's own comparison rule (test_autogrid4.py:157-186);
+  * live runs of oracle/_ref/autogrid4_fullprec on the reference's test inputs.
+"""
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import REFERENCE, ROOT
+
+GOLDEN = sorted((ROOT / "tests" / "golden").glob("*.npz"))
+
+
+def load_golden(path, tmp_path):
+    """Recreate a golden case's files and load them with the front end."""
+    from autogrid_b200 import Job
+    z = np.load(path, allow_pickle=False)
+    (tmp_path / "g.gpf").write_text(str(z["gpf"]))
+    (tmp_path / "g.pdbqt").write_text(str(z["pdbqt"]))
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        job = Job("g.gpf", "g.glg")
+        prob = job.problem()
+    finally:
+        os.chdir(cwd)
+    return z, job, prob
+
+
+def full_precision_ok(got, ref):
+    """Reference values were printed as floats (%.9g); values below 1e-4 as '0'."""
+    tol = np.where(ref == 0.0, 1e-4, 1.5e-7 * np.abs(ref) + 1e-12)
+    return np.abs(got - ref) <= tol
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
+def test_oracle_matches_reference_golden(path, tmp_path, built):
+    from oracle.oracle import oracle_points
+    z, job, prob = load_golden(path, tmp_path)
+    ref = z["maps_full"]
+    assert prob.n_maps == ref.shape[0]
+    got, flags = oracle_points(prob)
+    ok = full_precision_ok(got, ref)
+    bad = np.argwhere(~ok)
+    assert bad.size == 0, f"{len(bad)} values differ, first {bad[:3].tolist()}"
+
+
+def test_golden_set_is_present():
+    assert len(GOLDEN) >= 6
+
+
+needs_reference = pytest.mark.skipif(not (REFERENCE / "Tests").exists(), reason="reference sources absent")
+
+
+def _copy_tests(tmp_path):
+    for f in (REFERENCE / "Tests").iterdir():
+        if f.suffix in (".gpf", ".pdbqt", ".dat"):
+            shutil.copy(f, tmp_path / f.name)
+
+
+@needs_reference
+def test_oracle_vs_reference_testsuite_golden_maps(tmp_path, built):
+    """Tests/py_hsg1_sm.*.map with the rule of test_autogrid4.py:157-186, bounded
+    by the reference's own deviation from those maps (max 0.003 kcal/mol)."""
+    from autogrid_b200 import Job
+    from oracle.oracle import oracle_points, read_map
+    _copy_tests(tmp_path)
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        prob = Job("hsg1_sm.gpf", "hsg1_sm.glg").problem()
+    finally:
+        os.chdir(cwd)
+    got, _ = oracle_points(prob)
+    for i, name in enumerate(["A", "C", "HD", "N", "NA", "OA", "e", "d"]):
+        py = read_map(REFERENCE / "Tests" / f"py_hsg1_sm.{name}.map")
+        mine = np.round(got[i], 3)
+        assert np.abs(mine - py).max() <= 0.0035, name
+
+
+@needs_reference
+@pytest.mark.parametrize("stem", ["hsg1_sm", "x1hpv_CASE0", "hsg1_sm_nbpreps", "hsg1_sm_nbpcoeffs",
+                                  "hsg1_sm_no_parameter_file", "hsg1_no_receptor_types"])
+def test_oracle_vs_live_reference(stem, tmp_path, built):
+    from autogrid_b200 import Job
+    from oracle.oracle import REF_FULLPREC_BIN, oracle_points, read_map
+    _copy_tests(tmp_path)
+    ref_dir = tmp_path / "ref"
+    ref_dir.mkdir()
+    _copy_tests(ref_dir)
+    r = subprocess.run([str(REF_FULLPREC_BIN), "-p", f"{stem}.gpf", "-l", f"{stem}.glg"], cwd=ref_dir,
+                       capture_output=True, text=True)
+    assert r.returncode == 0
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        job = Job(f"{stem}.gpf", f"{stem}.glg")
+        prob = job.problem()
+    finally:
+        os.chdir(cwd)
+    got, _ = oracle_points(prob)
+    gpf = (tmp_path / f"{stem}.gpf").read_text().splitlines()
+    files = [ln.split()[1] for ln in gpf if ln.split() and ln.split()[0] in ("map", "elecmap", "dsolvmap")]
+    assert len(files) == prob.n_maps
+    for i, f in enumerate(files):
+        ref = read_map(ref_dir / f)
+        ok = full_precision_ok(got[i], ref)
+        assert ok.all(), f"{stem} {f}: max |d| {np.abs(got[i] - ref).max()}"
