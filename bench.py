@@ -47,7 +47,7 @@ METRIC = "grid-pt*type evals/s (plain 127^3 x 16-map AD4 set, 10k-atom receptor)
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
@@ -77,7 +77,7 @@ class ClockSampler:
             return
         self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                      "--format=csv,noheader,nounits", "-lms", "100"],
                                      stdout=self.out, stderr=subprocess.DEVNULL)
 
     def stop(self) -> dict:
