@@ -1,6 +1,7 @@
 // C ABI of the hot path: contexts, plans and the kernel sequence that
 // replaces the reference's grid-point loop (main.cpp:2805-3464).
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -96,12 +97,12 @@ struct ag_plan {
     bool any_cov = false;
     float *maps32 = nullptr;
     double *maps64 = nullptr;
-    int *closest = nullptr;
     double *cov = nullptr;
     float *far_partial = nullptr;
     double *x128 = nullptr, *y128 = nullptr, *z128 = nullptr;
-    float *qw = nullptr, *far_tab = nullptr, *etab = nullptr, *solf = nullptr, *rvf = nullptr, *rv2f = nullptr,
-          *vdwT = nullptr;
+    float *qw = nullptr, *far_tab = nullptr, *etab = nullptr, *solf = nullptr, *vdwT = nullptr;
+    float4 *atomA = nullptr, *atomB = nullptr;
+    int *meta = nullptr;
     size_t h2d_bytes = 0;
     int last_launches = 0;
 };
@@ -198,17 +199,26 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
     pl->h2d_bytes = 0;
     size_t *acc = &pl->h2d_bytes;
 
-    // atoms: SoA doubles, x*A_DIV copies for the far kernel, float bond vectors
+    // atoms: SoA doubles, x*A_DIV copies for the far kernel, and the near
+    // kernel's staged record: bond vectors + vol, lone-pair normal + desolvation
+    // factor, and packed metadata (type, hbond, rexp, flags)
     std::vector<double> x(N), y(N), z(N), x128(N), y128(N), z128(N);
-    std::vector<float> qw(N), rvf(3 * (size_t)N), rv2f(3 * (size_t)N);
+    std::vector<float> qw(N);
+    std::vector<float4> atomA(std::max(N, 1)), atomB(std::max(N, 1));
+    std::vector<int> meta(std::max(N, 1), 0);
     for (int a = 0; a < N; a++) {
         x[a] = p->coord[3 * a]; y[a] = p->coord[3 * a + 1]; z[a] = p->coord[3 * a + 2];
         x128[a] = x[a] * AG_A_DIV; y128[a] = y[a] * AG_A_DIV; z128[a] = z[a] * AG_A_DIV;
         qw[a] = (float)(p->charge[a] * p->coeff_estat * AG_A_DIV);
-        for (int k = 0; k < 3; k++) {
-            rvf[3 * a + k] = (float)p->rvector[3 * a + k];
-            rv2f[3 * a + k] = (float)p->rvector2[3 * a + k];
-        }
+        const double *rv = p->rvector + 3 * a, *rv2 = p->rvector2 + 3 * a;
+        atomA[a] = make_float4((float)rv[0], (float)rv[1], (float)rv[2], (float)p->vol[a]);
+        atomB[a] = make_float4((float)rv2[0], (float)rv2[1], (float)rv2[2],
+                               (float)(p->solpar[a] + p->solpar_q * std::fabs(p->charge[a])));
+        int m = (p->rec_type[a] & 31) | ((p->hbond[a] & 7) << 5) | ((p->rexp[a] & 7) << 8);
+        if (p->disorder[a]) m |= 1 << 11;
+        if (rv[0] == 0.0 && rv[1] == 0.0 && rv[2] == 0.0) m |= 1 << 12;
+        if (p->disorder_h && p->disorder[a] && p->rec_type[a] == p->hydrogen_type) m |= 1 << 13;
+        meta[a] = m;
     }
     std::vector<int> h_index;
     for (int a = 0; a < N; a++)
@@ -248,25 +258,9 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
             if (cell_of[a] >= 0) cell_atoms[fill[cell_of[a]]++] = a;
     }
 
-    // tables
-    pl->mpad = std::max(4, (nAM + 3) / 4 * 4);
-    const int nT = std::max(1, p->n_rec_types);
-    std::vector<float> vdwT((size_t)nT * AG_NEINT * pl->mpad, 0.f);
-    for (int t = 0; t < p->n_rec_types; t++)
-        for (int m = 0; m < nAM; m++)
-            for (int k = 0; k < AG_NEINT; k++)
-                vdwT[((size_t)t * AG_NEINT + k) * pl->mpad + m] = p->e_vdw_hb[((size_t)t * nAM + m) * AG_NEINT + k];
-    std::vector<float> far_tab(AG_NDIEL, 0.f), etab(AG_NDIEL), solf(AG_NDIEL);
-    std::vector<double> reps(AG_NDIEL, 0.0);
-    for (int k = 0; k < AG_NDIEL; k++) {
-        const double f = p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal;
-        if (p->dddiel) reps[k] = p->r_epsilon_fn[k];
-        far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
-        etab[k] = (float)(f * p->coeff_estat);
-        solf[k] = (float)p->sol_fn[k];
-    }
-
-    // map groups (act table after main.cpp:3286-3379)
+    // map groups in kernel order (actions after main.cpp:3286-3379).  Maps that
+    // keep an hbond min/max for some receptor class go first, at most NG_MM per
+    // launch, so their min/max accumulators have fixed register slots.
     std::vector<int> is_partner(std::max(nAM, 1), 0);
     if (p->separate_desolvation_maps) {
         for (int m = 0; m < nAM; m++) {
@@ -275,38 +269,72 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
             m++;
         }
     }
+    std::vector<std::array<uint8_t, 8>> act(std::max(nAM, 1));
+    std::vector<int> mm_maps, plain_maps;
+    for (int m = 0; m < nAM; m++) {
+        const bool aff = !p->map_is_covalent[m] && !is_partner[m];
+        bool mm = false;
+        for (int hb = 0; hb < 8; hb++) {
+            uint8_t a = ACT_PLAIN;
+            if (!aff) a = ACT_SKIP;
+            else if (p->map_is_hbonder[m]) {
+                const int mh = p->map_hbond[m];
+                if ((mh == 3 || mh == 5 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) a = ACT_SUMA;
+                else if ((mh == 4 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) a = ACT_MMA;
+                else if ((mh == 1 || mh == 2 || mh == 6) && (hb > 2 || hb == 6)) a = ACT_MMD;
+            }
+            act[m][hb] = a;
+            if (hb <= 6 && (a == ACT_MMA || a == ACT_MMD)) mm = true;
+        }
+        (mm ? mm_maps : plain_maps).push_back(m);
+    }
     pl->groups.clear();
     pl->any_cov = false;
-    for (int g0 = 0; g0 < nAM || (g0 == 0 && pl->groups.empty()); g0 += NG_MAX) {
+    size_t im = 0, ip = 0;
+    do {
         NearGroup g;
         std::memset(&g, 0, sizeof g);
-        g.g0 = g0;
-        g.ng = std::max(0, std::min(NG_MAX, nAM - g0));
-        g.write_special = (g0 == 0);
+        std::vector<int> order;
+        while (im < mm_maps.size() && (int)order.size() < NG_MM) order.push_back(mm_maps[im++]);
+        while (ip < plain_maps.size() && (int)order.size() < NG_MAX) order.push_back(plain_maps[ip++]);
+        g.ng = (int)order.size();
+        g.write_special = pl->groups.empty() ? 1 : 0;
         g.has_hrow = p->disorder_h ? 1 : 0;
-        for (int j = 0; j < g.ng; j++) {
-            const int m = g0 + j;
-            g.cov[j] = (uint8_t)(p->map_is_covalent[m] ? 1 : 0);
-            if (g.cov[j]) pl->any_cov = true;
-            const bool aff = !g.cov[j] && !is_partner[m];
-            for (int hb = 0; hb < 8; hb++) {
-                uint8_t a = ACT_PLAIN;
-                if (!aff) a = ACT_SKIP;
-                else if (p->map_is_hbonder[m]) {
-                    const int mh = p->map_hbond[m];
-                    if ((mh == 3 || mh == 5 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) a = ACT_SUMA;
-                    else if ((mh == 4 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) a = ACT_MMA;
-                    else if ((mh == 1 || mh == 2 || mh == 6) && (hb > 2 || hb == 6)) a = ACT_MMD;
-                }
-                g.act[j][hb] = a;
-            }
+        g.col0 = (int)pl->groups.size() * NG_MAX;
+        for (int k = 0; k < g.ng; k++) {
+            const int m = order[k];
+            g.out_map[k] = m;
+            g.cov[k] = (uint8_t)(p->map_is_covalent[m] ? 1 : 0);
+            if (g.cov[k]) pl->any_cov = true;
+            for (int hb = 0; hb < 8; hb++) g.actw[hb] |= (unsigned long long)act[m][hb] << (3 * k);
             // desolvation lands on the affinity map, or on its partner when maps are separate
-            const bool gets_desolv = !g.cov[j] && (p->separate_desolvation_maps ? (bool)is_partner[m] : true);
-            g.sp[j] = gets_desolv ? p->map_solpar_probe[m] : 0.0;
-            g.vp[j] = gets_desolv ? p->map_vol_probe[m] : 0.0;
+            const bool gets_desolv = !g.cov[k] && (p->separate_desolvation_maps ? (bool)is_partner[m] : true);
+            g.sp[k] = gets_desolv ? p->map_solpar_probe[m] : 0.0;
+            g.vp[k] = gets_desolv ? p->map_vol_probe[m] : 0.0;
         }
         pl->groups.push_back(g);
-        if (nAM == 0) break;
+    } while (im < mm_maps.size() || ip < plain_maps.size());
+
+    // tables: vdW/H-bond transposed to [type][bin][column], columns in kernel order
+    pl->mpad = (int)pl->groups.size() * NG_MAX;
+    const int nT = std::max(1, p->n_rec_types);
+    std::vector<float> vdwT((size_t)nT * AG_NEINT * pl->mpad, 0.f);
+    for (const NearGroup &g : pl->groups)
+        for (int k = 0; k < g.ng; k++) {
+            const int m = g.out_map[k];
+            for (int t = 0; t < p->n_rec_types; t++)
+                for (int b = 0; b < AG_NEINT; b++)
+                    vdwT[((size_t)t * AG_NEINT + b) * pl->mpad + g.col0 + k] =
+                        p->e_vdw_hb[((size_t)t * nAM + m) * AG_NEINT + b];
+        }
+    std::vector<float> far_tab(AG_NDIEL, 0.f), etab(AG_NDIEL), solf(AG_NDIEL);
+    std::vector<double> reps(AG_NDIEL, 0.0);
+    for (int k = 0; k < AG_NDIEL; k++) {
+        const double f = p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal;
+        if (p->dddiel) reps[k] = p->r_epsilon_fn[k];
+        far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
+        etab[k] = (float)(f * p->coeff_estat);
+        solf[k] = (float)p->sol_fn[k];
     }
 
     // far-field chunking: enough CTAs for ~8 waves
@@ -344,8 +372,9 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
     AGB_CK(upload(B, "rexp", p->rexp, N, &drexp, s, acc));
     AGB_CK(upload(B, "disorder", p->disorder, N, &ddis, s, acc));
     AGB_CK(upload(B, "qw", qw.data(), N, &pl->qw, s, acc));
-    AGB_CK(upload(B, "rvf", rvf.data(), rvf.size(), &pl->rvf, s, acc));
-    AGB_CK(upload(B, "rv2f", rv2f.data(), rv2f.size(), &pl->rv2f, s, acc));
+    AGB_CK(upload(B, "atomA", atomA.data(), atomA.size(), &pl->atomA, s, acc));
+    AGB_CK(upload(B, "atomB", atomB.data(), atomB.size(), &pl->atomB, s, acc));
+    AGB_CK(upload(B, "meta", meta.data(), meta.size(), &pl->meta, s, acc));
     AGB_CK(upload(B, "h_index", h_index.data(), h_index.size(), &dh, s, acc));
     AGB_CK(upload(B, "cell_start", cell_start.data(), cell_start.size(), &dcs, s, acc));
     AGB_CK(upload(B, "cell_atoms", cell_atoms.data(), cell_atoms.size(), &dca, s, acc));
@@ -386,8 +415,6 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
         pl->maps32 = (float *)v;
         pl->maps64 = nullptr;
     }
-    AGB_CK(B->ensure("closest", P * sizeof(int), &v));
-    pl->closest = (int *)v;
     if (pl->any_cov) {
         AGB_CK(B->ensure("cov", P * sizeof(double), &v));
         pl->cov = (double *)v;
@@ -430,14 +457,10 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
         AGB_CK(launch_covalent(d, pl->cov, s));
         launches++;
     }
-    if (d.n_atom_maps > 0) {
-        AGB_CK(launch_closest_h(d, pl->closest, s));
-        launches++;
-    }
     const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || (!exact && d.elec_map >= 0);
     if (need_near) {
         for (const NearGroup &g : pl->groups) {
-            AGB_CK(launch_near(exact, d, g, pl->closest, pl->rvf, pl->rv2f, pl->vdwT, pl->mpad, pl->etab, pl->solf,
+            AGB_CK(launch_near(exact, d, g, pl->atomA, pl->atomB, pl->meta, pl->vdwT, pl->mpad, pl->etab, pl->solf,
                                pl->cov, pl->maps32, pl->maps64, c->d_counters, s));
             launches++;
         }

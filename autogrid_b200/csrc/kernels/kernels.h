@@ -12,10 +12,9 @@ cudaError_t launch_emap_far(const double *ax128, const double *ay128, const doub
                             double spacing_adiv, int n1x, int n1y, int n1z, int nex, int ney, int nez,
                             long long P, float *partial, cudaStream_t s);
 cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s);
-cudaError_t launch_closest_h(const DevProblem &p, int *closest, cudaStream_t s);
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s);
-cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const int *closest,
-                        const float *rvf, const float *rv2f, const float *vdwT, int mpad, const float *etab,
+cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const float4 *atomA,
+                        const float4 *atomB, const int *meta, const float *vdwT, int mpad, const float *etab,
                         const float *solf, const double *cov_map, float *out32, double *out64,
                         unsigned long long *counters, cudaStream_t s);
 int frames_x(int n1x);

@@ -1,10 +1,6 @@
 // Near-field kernels: everything of the reference grid loop except the
 // far-field electrostatics.
 //
-//   k_closest_h  closest DS/D1 hydrogen per point (main.cpp:2986-3015): FP32
-//                prefilter over all DS/D1 atoms, then an FP64 pass in file
-//                order over the candidates within the FP32 error bound, with
-//                the reference's strict '<' so ties keep the first atom.
 //   k_near<EXACT> one thread per grid point, bricks of 8x8x4 points.  Candidate
 //                atoms come from a cell list (cells of AGB_CELL A over the box
 //                grown by 8.05 A) and are staged through shared memory.
@@ -31,7 +27,7 @@
 namespace agb {
 
 constexpr int NB_X = 8, NB_Y = 8, NB_Z = 4, NB_THREADS = 256;
-constexpr int NB_CHUNK = 256;
+constexpr int NB_CHUNK = 384;   // candidates staged at once (most bricks need one chunk)
 constexpr int NB_SEGS = 64;
 constexpr float GUARD_BIN = 2.0e-3f;   // bins: > 3x the FP32 distance error bound
 constexpr float GUARD_COS = 5.0e-5f;
@@ -147,26 +143,31 @@ __device__ __noinline__ void pair_exact(const DevProblem &p, int ia, double cx, 
     }
 }
 
-// FP32 pair quantities from the canonical frame-relative distance.  Returns
-// false when any quantity is within its error bound of a discontinuity; the
-// caller then uses pair_exact().
-__device__ __forceinline__ bool pair_fast(const DevProblem &p, const float *__restrict__ rvf,
-                                          const float *__restrict__ rv2f, int ia, float dX, float dY,
-                                          float dZ, float t, float rs, int ch, float3 rvh,
-                                          PairQ<float> &o)
+// Per-atom metadata packed for shared memory (built by the host, capi.cu).
+constexpr int META_TYPE_MASK = 31;          // bits 0-4   receptor type
+constexpr int META_HB_SHIFT = 5;            // bits 5-7   hbond class
+constexpr int META_REXP_SHIFT = 8;          // bits 8-10  rexp
+constexpr int META_DIS = 1 << 11;           // disorder flag
+constexpr int META_RVZERO = 1 << 12;        // bond vector exactly zero
+constexpr int META_SKIP_AD4 = 1 << 13;      // disordered hydrogen skipped by LOOP 2 (main.cpp:3052)
+
+// FP32 pair quantities from the canonical frame-relative distance and the
+// atom's staged metadata / bond vectors.  Returns false when any quantity is
+// within its error bound of a discontinuity; the caller then uses pair_exact().
+__device__ __forceinline__ bool pair_fast(int meta, float4 rvA, float4 rvB, int ia, float dX, float dY, float dZ,
+                                          float t, float rs, int ch, float3 rvh, PairQ<float> &o)
 {
     const float tf = floorf(t);
     if (t - tf < GUARD_BIN || (tf + 1.f) - t < GUARD_BIN || t < 1.0f) return false;
     o.bin = (int)tf;
     o.bin_e = o.bin;
-    o.ad4_in = t < FAR_T0;  // t not within GUARD_BIN of 1024 here: equals r <= 8
-    const int dis = p.disorder[ia];
-    if (p.disorder_h && dis && p.type[ia] == p.hydrogen_type) o.ad4_in = 0;
+    o.ad4_in = (t < FAR_T0) && !(meta & META_SKIP_AD4);  // t is not within GUARD_BIN of 1024: equals r <= 8
     o.r = t * (1.0f / AG_A_DIV);
     o.inv_rmax = fminf((float)AG_A_DIV * rs, 2.0f);
     o.racc = 1.f; o.rdon = 1.f; o.Hramp = 1.f;
     o.ih = 0;
     if (!o.ad4_in) return true;
+    const bool dis = (meta & META_DIS) != 0;
     if (dis) {
         const float xh = t - 140.8f;  // (r - 1.10) * A_DIV
         if (xh > 0.5f) {
@@ -175,21 +176,21 @@ __device__ __forceinline__ bool pair_fast(const DevProblem &p, const float *__re
             o.ih = min((int)xf, AG_NEINT - 1);
         }
     }
-    const int hb = p.hbond[ia];
+    const int hb = (meta >> META_HB_SHIFT) & 7;
     if (hb != 2 && hb != 4 && hb != 5) return true;
     const float dn0 = dX * rs, dn1 = dY * rs, dn2 = dZ * rs;
-    const float rv0 = rvf[3 * ia], rv1 = rvf[3 * ia + 1], rv2 = rvf[3 * ia + 2];
+    const float rv0 = rvA.x, rv1 = rvA.y, rv2 = rvA.z;
     const float cos_theta = ((0.f - dn0 * rv0) - dn1 * rv1) - dn2 * rv2;
     const float PIH = 1.57079632679489662f;
     // An atom without bonded neighbours keeps a zero bond vector; its cos_theta
     // is exactly 0 in every precision, so the branch at 0 is not ambiguous.
-    const bool rv_zero = (rv0 == 0.f) & (rv1 == 0.f) & (rv2 == 0.f);
+    const bool rv_zero = (meta & META_RVZERO) != 0;
     if (hb == 2) {
         if (fabsf(cos_theta) < GUARD_COS && !rv_zero) return false;
         if (cos_theta <= 0.f) {
             o.racc = 0.f;
         } else {
-            const int e = p.rexp[ia];
+            const int e = (meta >> META_REXP_SHIFT) & 7;
             o.racc = (e == 2) ? cos_theta * cos_theta
                    : (e == 4) ? (cos_theta * cos_theta) * (cos_theta * cos_theta) : cos_theta;
             if (ia != ch && ch >= 0) {
@@ -202,7 +203,7 @@ __device__ __forceinline__ bool pair_fast(const DevProblem &p, const float *__re
         o.rdon = (cos_theta <= 0.f) ? 0.f : cos_theta * cos_theta;
     } else if (!dis) {  // A2 ordered
         if (fabsf(cos_theta) < GUARD_COS && !rv_zero) return false;
-        const float w0 = rv2f[3 * ia], w1 = rv2f[3 * ia + 1], w2 = rv2f[3 * ia + 2];
+        const float w0 = rvB.x, w1 = rvB.y, w2 = rvB.z;
         float t0 = dn0 * w0 + dn1 * w1 + dn2 * w2;
         t0 = fminf(fmaxf(t0, -1.f), 1.f);
         t0 = PIH - acosf(t0);
@@ -233,79 +234,46 @@ __device__ __forceinline__ bool pair_fast(const DevProblem &p, const float *__re
     return true;
 }
 
-// ------------------------------------------------------------ closest H ---
-__global__ void __launch_bounds__(NB_THREADS)
-k_closest_h(DevProblem p, int *__restrict__ closest)
+// Exact distance of the reference's closest-H search (main.cpp:2994-3002).
+__device__ __forceinline__ double h_dist(const DevProblem &p, int a, double cx, double cy, double cz)
 {
-    __shared__ float4 s_h[NB_CHUNK];
-    const int tid = threadIdx.x;
-    const int nbx = (p.n1x + NB_X - 1) / NB_X, nby = (p.n1y + NB_Y - 1) / NB_Y;
-    const int b = blockIdx.x;
-    const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
-    const int ix = bx * NB_X + (tid & 7), iy = by * NB_Y + ((tid >> 3) & 7), iz = bz * NB_Z + (tid >> 6);
-    const bool valid = ix < p.n1x && iy < p.n1y && iz < p.n1z;
-    const double sp128 = p.spacing * AG_A_DIV;
-    const double X0 = frame_origin_bins(bx * NB_X, p.nex, sp128);
-    const double Y0 = frame_origin_bins(by * NB_Y, p.ney, sp128);
-    const double Z0 = frame_origin_bins(bz * NB_Z, p.nez, sp128);
-    const float PX = frame_point_coord(tid & 7, sp128), PY = frame_point_coord((tid >> 3) & 7, sp128),
-                PZ = frame_point_coord(tid >> 6, sp128);
-    const double cx = (double)(ix - p.nex) * p.spacing, cy = (double)(iy - p.ney) * p.spacing,
-                 cz = (double)(iz - p.nez) * p.spacing;
-    float best2 = 3.0e38f;
-    for (int pass = 0; pass < 2; pass++) {
-        const float lim = best2 * (1.0f + 2.0e-5f) + 4.0f;
-        double rmin = 999999.;
-        int best = -1;
-        for (int h0 = 0; h0 < p.n_h; h0 += NB_CHUNK) {
-            const int nh = min(NB_CHUNK, p.n_h - h0);
-            __syncthreads();
-            if (tid < nh) {
-                const int a = p.h_index[h0 + tid];
-                s_h[tid] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0),
-                                       frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
-                                       frame_atom_coord(p.z[a] * AG_A_DIV, Z0), __int_as_float(a));
-            }
-            __syncthreads();
-            if (!valid) continue;
-            if (pass == 0) {
-                for (int j = 0; j < nh; j++) {
-                    const float4 A = s_h[j];
-                    const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
-                    best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
-                }
-            } else {
-                for (int j = 0; j < nh; j++) {
-                    const float4 A = s_h[j];
-                    const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
-                    if (dx * dx + dy * dy + dz * dz > lim) continue;
-                    const int a = __float_as_int(A.w);
-                    const double d0 = __dsub_rn(p.x[a], cx), d1 = __dsub_rn(p.y[a], cy), d2 = __dsub_rn(p.z[a], cz);
-                    const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
-                    if (r < rmin) { rmin = r; best = a; }
-                }
-            }
-        }
-        if (pass == 1 && valid) closest[((long long)iz * p.n1y + iy) * p.n1x + ix] = best;
-    }
+    const double d0 = __dsub_rn(p.x[a], cx), d1 = __dsub_rn(p.y[a], cy), d2 = __dsub_rn(p.z[a], cz);
+    return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
 }
 
 // ----------------------------------------------------------------- near ---
+// One thread per grid point; bricks of 8x8x4 points inside one far-field frame.
+//  stage  candidate atoms of the cells within 8.05 A of the brick, with their
+//         canonical frame-relative FP32 coordinates and packed metadata
+//  A      closest DS/D1 atom per point among the candidates (any DS/D1 atom
+//         within 8.05 A of the point is a candidate, so a best distance
+//         <= 8 A is the global minimum); FP32 prefilter, then FP64 with the
+//         reference's order (strict '<' in file order == lowest index on a tie);
+//         points with no DS/D1 atom within 8 A scan all of them (rare)
+//  B      pair terms of every candidate inside 8 A (+ e-map near pairs)
 template <bool EXACT>
-__global__ void __launch_bounds__(NB_THREADS)
-k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *__restrict__ rvf,
-       const float *__restrict__ rv2f, const float *__restrict__ vdwT, int mpad,
+__global__ void __launch_bounds__(NB_THREADS, 2)
+k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4 *__restrict__ atomB,
+       const int *__restrict__ atom_meta, const float *__restrict__ vdwT, int mpad,
        const float *__restrict__ etab, const float *__restrict__ solf, const double *__restrict__ cov_map,
        float *__restrict__ out32, double *__restrict__ out64, unsigned long long *__restrict__ counters)
 {
     using R = typename std::conditional<EXACT, double, float>::type;
     __shared__ float4 s_pos[NB_CHUNK];
-    __shared__ int s_idx[NB_CHUNK];
+    __shared__ float4 s_a[NB_CHUNK], s_b[NB_CHUNK];
+    __shared__ int s_meta[NB_CHUNK], s_idx[NB_CHUNK];
+    __shared__ float s_etab[NT_SMALL], s_sol[NT_SMALL];
     __shared__ int s_seg_start[NB_SEGS], s_seg_off[NB_SEGS + 1];
+    __shared__ int s_total;
     __shared__ unsigned long long s_cnt[2];
 
     const int tid = threadIdx.x;
     if (tid < 2) s_cnt[tid] = 0ull;
+    for (int i = tid; i < NT_SMALL; i += NB_THREADS) {
+        s_etab[i] = etab[i];
+        s_sol[i] = solf[i];
+    }
+    __syncthreads();
     const int nbx = (p.n1x + NB_X - 1) / NB_X, nby = (p.n1y + NB_Y - 1) / NB_Y;
     const int b = blockIdx.x;
     const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
@@ -323,17 +291,10 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
                 PZ = frame_point_coord(iz - oz, sp128);
     const double cx = (double)(ix - p.nex) * p.spacing, cy = (double)(iy - p.ney) * p.spacing,
                  cz = (double)(iz - p.nez) * p.spacing;
-    const int ch = (valid && p.n_atom_maps > 0) ? closest[lin] : -1;
-    float3 rvh = make_float3(0.f, 0.f, 0.f);
-    if (!EXACT && ch >= 0) rvh = make_float3(rvf[3 * ch], rvf[3 * ch + 1], rvf[3 * ch + 2]);
 
-    R E[NG_MAX], hmin[NG_MAX], hmax[NG_MAX];
-#pragma unroll
-    for (int m = 0; m < NG_MAX; m++) { E[m] = 0; hmin[m] = 999999.; hmax[m] = -999999.; }
-    uint32_t hflag = 0;
-    R D1 = 0, D2 = 0, e_near = 0;
-    unsigned long long n_near = 0, n_fb = 0;
-    const bool need_pairs = g.ng > 0 || (g.write_special && (p.dsolv_map >= 0 || (!EXACT && p.elec_map >= 0)));
+    const bool need_h = p.n_atom_maps > 0;
+    const bool do_e = !EXACT && g.write_special && p.elec_map >= 0;
+    const bool need_pairs = g.ng > 0 || (g.write_special && p.dsolv_map >= 0) || do_e;
 
     // candidate cells: brick bounding box grown by the candidate radius
     const double rc = AGB_NEAR_RADIUS;
@@ -346,11 +307,24 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
     const int cyl = cell_lo(by0, p.cell0[1], p.ncy), cyh = cell_hi(by1, p.cell0[1], p.ncy);
     const int czl = cell_lo(bz0, p.cell0[2], p.ncz), czh = cell_hi(bz1, p.cell0[2], p.ncz);
     const int nrow_y = cyh - cyl + 1;
-    const int nseg_total = need_pairs ? nrow_y * (czh - czl + 1) : 0;
+    const int nseg_total = (need_pairs || need_h) ? nrow_y * (czh - czl + 1) : 0;
 
-    for (int sb = 0; sb < nseg_total; sb += NB_SEGS) {
-        const int nseg = min(NB_SEGS, nseg_total - sb);
-        __syncthreads();
+    // Stage chunk `c0` of segment batch `sb` (the caller has laid out s_seg_*).
+    auto stage = [&](int c0, int nc) {
+        for (int i = tid; i < nc; i += NB_THREADS) {
+            const int c = c0 + i;
+            int s = 0;
+            while (s_seg_off[s + 1] <= c) s++;
+            const int a = p.cell_atoms[s_seg_start[s] + (c - s_seg_off[s])];
+            s_idx[i] = a;
+            s_pos[i] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0), frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
+                                   frame_atom_coord(p.z[a] * AG_A_DIV, Z0), (float)p.q[a]);
+            s_a[i] = atomA[a];
+            s_b[i] = atomB[a];
+            s_meta[i] = atom_meta[a];
+        }
+    };
+    auto layout_segments = [&](int sb, int nseg) {
         if (tid == 0) {
             int off = 0;
             for (int s = 0; s < nseg; s++) {
@@ -363,28 +337,99 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
                 off += en - st;
             }
             s_seg_off[nseg] = off;
+            s_total = off;
+        }
+    };
+    // the candidate list fits one chunk in the common case: stage it once
+    bool resident = false;
+    if (nseg_total > 0 && nseg_total <= NB_SEGS) {
+        __syncthreads();
+        layout_segments(0, nseg_total);
+        __syncthreads();
+        if (s_total <= NB_CHUNK) {
+            stage(0, s_total);
+            resident = true;
         }
         __syncthreads();
-        const int total = s_seg_off[nseg];
-        for (int c0 = 0; c0 < total; c0 += NB_CHUNK) {
-            const int nc = min(NB_CHUNK, total - c0);
+    }
+    // visit every candidate chunk: fn(nc) with the chunk staged in shared memory
+    auto for_each_chunk = [&](auto &&fn) {
+        if (resident) { fn(s_total); return; }
+        for (int sb = 0; sb < nseg_total; sb += NB_SEGS) {
+            const int nseg = min(NB_SEGS, nseg_total - sb);
             __syncthreads();
-            if (tid < nc) {
-                const int c = c0 + tid;
-                int s = 0;
-                while (s_seg_off[s + 1] <= c) s++;
-                const int a = p.cell_atoms[s_seg_start[s] + (c - s_seg_off[s])];
-                s_idx[tid] = a;
-                s_pos[tid] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0),
-                                         frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
-                                         frame_atom_coord(p.z[a] * AG_A_DIV, Z0), 0.f);
+            layout_segments(sb, nseg);
+            __syncthreads();
+            const int total = s_total;
+            for (int c0 = 0; c0 < total; c0 += NB_CHUNK) {
+                const int nc = min(NB_CHUNK, total - c0);
+                __syncthreads();
+                stage(c0, nc);
+                __syncthreads();
+                fn(nc);
             }
-            __syncthreads();
-            if (!valid) continue;
+        }
+    };
+
+    // ---- A: closest DS/D1 hydrogen (main.cpp:2986-3015)
+    int ch = -1;
+    if (need_h) {
+        float best2 = 3.0e38f;
+        for_each_chunk([&](int nc) {
+            if (!valid) return;
+            for (int j = 0; j < nc; j++) {
+                const int hb = (s_meta[j] >> META_HB_SHIFT) & 7;
+                if (hb != 1 && hb != 2) continue;
+                const float4 A = s_pos[j];
+                const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
+                best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
+            }
+        });
+        const float lim = best2 * (1.0f + 2.0e-5f) + 4.0f;
+        double rmin = 999999.;
+        for_each_chunk([&](int nc) {
+            if (!valid) return;
+            for (int j = 0; j < nc; j++) {
+                const int hb = (s_meta[j] >> META_HB_SHIFT) & 7;
+                if (hb != 1 && hb != 2) continue;
+                const float4 A = s_pos[j];
+                const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
+                if (dx * dx + dy * dy + dz * dz > lim) continue;
+                const int a = s_idx[j];
+                const double r = h_dist(p, a, cx, cy, cz);
+                if (r < rmin || (r == rmin && a < ch)) { rmin = r; ch = a; }
+            }
+        });
+        if (valid && !(rmin <= AG_NBC)) {  // nothing within 8 A: scan every DS/D1 atom in file order
+            rmin = 999999.;
+            ch = -1;
+            for (int k = 0; k < p.n_h; k++) {
+                const int a = p.h_index[k];
+                const double r = h_dist(p, a, cx, cy, cz);
+                if (r < rmin) { rmin = r; ch = a; }
+            }
+        }
+    }
+    float3 rvh = make_float3(0.f, 0.f, 0.f);
+    if (!EXACT && ch >= 0) rvh = make_float3(atomA[ch].x, atomA[ch].y, atomA[ch].z);
+
+    // ---- B: pair terms
+    R E[NG_MAX], hmin[NG_MM], hmax[NG_MM];
+#pragma unroll
+    for (int m = 0; m < NG_MAX; m++) E[m] = 0;
+#pragma unroll
+    for (int m = 0; m < NG_MM; m++) { hmin[m] = 999999.; hmax[m] = -999999.; }
+    uint32_t hflag = 0;
+    R D1 = 0, D2 = 0, e_near = 0;
+    unsigned long long n_near = 0, n_fb = 0;
+    if (need_pairs) {
+        for_each_chunk([&](int nc) {
+            if (!valid) return;
             for (int j = 0; j < nc; j++) {
                 const int ia = s_idx[j];
+                const int meta = s_meta[j];
                 PairQ<R> q;
-                bool e_pair;
+                bool e_pair = false;
                 if (EXACT) {
                     const double d0 = __dsub_rn(p.x[ia], cx), d1 = __dsub_rn(p.y[ia], cy), d2 = __dsub_rn(p.z[ia], cz);
                     const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
@@ -394,7 +439,6 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
                     if (!qd.ad4_in) continue;
                     q.ad4_in = 1; q.bin = qd.bin; q.bin_e = qd.bin_e; q.ih = qd.ih;
                     q.r = (R)qd.r; q.inv_rmax = (R)qd.inv_rmax; q.racc = (R)qd.racc; q.rdon = (R)qd.rdon; q.Hramp = (R)qd.Hramp;
-                    e_pair = false;
                 } else {
                     const float4 A = s_pos[j];
                     const float dY = __fsub_rn(A.y, PY), dZ = __fsub_rn(A.z, PZ);
@@ -406,7 +450,7 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
                     if (t >= FAR_T0 + GUARD_BIN) continue;
                     e_pair = t < FAR_T0;  // the far-field kernel skips exactly these pairs
                     PairQ<float> qf;
-                    if (!pair_fast(p, rvf, rv2f, ia, dX, dY, dZ, t, rs, ch, rvh, qf)) {
+                    if (!pair_fast(meta, s_a[j], s_b[j], ia, dX, dY, dZ, t, rs, ch, rvh, qf)) {
                         PairQ<double> qd;
                         pair_exact(p, ia, cx, cy, cz, ch, qd);
                         qf.ad4_in = qd.ad4_in; qf.bin = qd.bin; qf.bin_e = qd.bin_e; qf.ih = qd.ih;
@@ -416,48 +460,50 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
                     }
                     q.ad4_in = qf.ad4_in; q.bin = qf.bin; q.bin_e = qf.bin_e; q.ih = qf.ih;
                     q.r = qf.r; q.inv_rmax = qf.inv_rmax; q.racc = qf.racc; q.rdon = qf.rdon; q.Hramp = qf.Hramp;
-                    if (e_pair && g.write_special && p.elec_map >= 0) {
-                        const int ke = min(q.bin_e, AG_NDIEL - 1);
-                        e_near += (R)(etab[ke] * (float)p.q[ia]) * q.inv_rmax;
-                    }
+                    if (e_pair && do_e) e_near += (R)(s_etab[min(q.bin_e, NT_SMALL - 1)] * A.w) * q.inv_rmax;
                     if (!q.ad4_in) continue;
                 }
                 n_near++;
-                const int kr = min(q.bin, AG_NDIEL - 1);
-                const int kn = min(q.bin, AG_NEINT - 1);
-                const R sol = EXACT ? (R)p.sol_fn[kr] : (R)solf[kr];
-                D1 += (R)p.vol[ia] * sol;
-                D2 += (R)(p.solpar[ia] + p.solpar_q * fabs(p.q[ia])) * sol;
+                const int kr = min(q.bin, NT_SMALL - 1);
+                const R sol = EXACT ? (R)p.sol_fn[kr] : (R)s_sol[kr];
+                const float4 rA = s_a[j], rB = s_b[j];
+                D1 += (R)rA.w * sol;  // vol
+                D2 += (R)rB.w * sol;  // solpar + qasp|q|
                 if (g.ng == 0) continue;
-                const int hb = p.hbond[ia];
-                const int dis = p.disorder[ia];
-                const int ta = p.type[ia];
-                const float *Trow = vdwT + ((size_t)ta * AG_NEINT + kn) * mpad + g.g0;
-                const float *Hrow = (g.has_hrow && dis && p.hydrogen_type >= 0)
-                                        ? vdwT + ((size_t)p.hydrogen_type * AG_NEINT + q.ih) * mpad + g.g0 : Trow;
+                const int hb = (meta >> META_HB_SHIFT) & 7;
+                const bool dis = (meta & META_DIS) != 0;
+                const int ta = meta & META_TYPE_MASK;
+                const int kn = min(q.bin, AG_NEINT - 1);
+                const float4 *Trow = (const float4 *)(vdwT + ((size_t)ta * AG_NEINT + kn) * mpad + g.col0);
+                const float4 *Hrow = (g.has_hrow && dis && p.hydrogen_type >= 0)
+                    ? (const float4 *)(vdwT + ((size_t)p.hydrogen_type * AG_NEINT + q.ih) * mpad + g.col0) : Trow;
+                const unsigned long long aw = g.actw[hb];
 #pragma unroll
-                for (int m = 0; m < NG_MAX; m++) {
-                    if (m >= g.ng) break;
-                    const int act = g.act[m][hb];
-                    if (act == ACT_SKIP) continue;
-                    const R T = (R)__ldg(Trow + m);
-                    if (act == ACT_PLAIN) { E[m] += T; continue; }
-                    R rsph = T / (R)100.;
-                    rsph = rsph > (R)0 ? rsph : (R)0;
-                    rsph = rsph < (R)1 ? rsph : (R)1;
-                    if (act == ACT_SUMA) {
-                        const R Tv = dis ? (R)__ldg(Hrow + m) : T;
-                        E[m] += Tv * q.Hramp * (q.racc + ((R)1 - q.racc) * rsph);
-                    } else if (act == ACT_MMA) {
-                        const R v = T * (q.racc + ((R)1 - q.racc) * rsph);
-                        hmin[m] = hmin[m] < v ? hmin[m] : v;
-                        hmax[m] = hmax[m] > v ? hmax[m] : v;
-                        hflag |= 1u << m;
-                    } else {  // ACT_MMD
-                        if (dis) {
-                            E[m] += (R)__ldg(Hrow + m) * q.Hramp * (q.rdon + ((R)1 - q.rdon) * rsph);
-                        } else {
-                            const R v = T * (q.rdon + ((R)1 - q.rdon) * rsph);
+                for (int m4 = 0; m4 < NG_MAX / 4; m4++) {
+                    if (4 * m4 >= g.ng) break;
+                    const float4 T4 = __ldg(Trow + m4);
+                    float4 H4 = T4;
+                    if (dis) H4 = __ldg(Hrow + m4);
+                    const float Tv[4] = {T4.x, T4.y, T4.z, T4.w};
+                    const float Hv[4] = {H4.x, H4.y, H4.z, H4.w};
+#pragma unroll
+                    for (int u = 0; u < 4; u++) {
+                        const int m = 4 * m4 + u;
+                        const int act = (int)((aw >> (3 * m)) & 7ull);
+                        if (act == ACT_SKIP) continue;
+                        const R T = (R)Tv[u];
+                        if (act == ACT_PLAIN) { E[m] += T; continue; }
+                        R rsph = T / (R)100.;
+                        rsph = rsph > (R)0 ? rsph : (R)0;
+                        rsph = rsph < (R)1 ? rsph : (R)1;
+                        if (act == ACT_SUMA) {
+                            const R Tv2 = dis ? (R)Hv[u] : T;
+                            E[m] += Tv2 * q.Hramp * (q.racc + ((R)1 - q.racc) * rsph);
+                        } else if (act == ACT_MMD && dis) {
+                            E[m] += (R)Hv[u] * q.Hramp * (q.rdon + ((R)1 - q.rdon) * rsph);
+                        } else if (m < NG_MM) {  // min/max maps are placed first by the host
+                            const R f = (act == ACT_MMA) ? q.racc : q.rdon;
+                            const R v = T * (f + ((R)1 - f) * rsph);
                             hmin[m] = hmin[m] < v ? hmin[m] : v;
                             hmax[m] = hmax[m] > v ? hmax[m] : v;
                             hflag |= 1u << m;
@@ -465,7 +511,7 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
                     }
                 }
             }
-        }
+        });
     }
 
     // finalise (main.cpp:3420-3431) and store
@@ -474,9 +520,9 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
         for (int m = 0; m < NG_MAX; m++) {
             if (m >= g.ng) break;
             R v = E[m];
-            if (hflag & (1u << m)) v += hmin[m] + (hmax[m] > (R)0 ? hmax[m] : (R)0);
+            if (m < NG_MM && (hflag & (1u << m))) v += hmin[m] + (hmax[m] > (R)0 ? hmax[m] : (R)0);
             v += (R)g.sp[m] * D1 + (R)g.vp[m] * D2;
-            const size_t o = (size_t)(g.g0 + m) * (size_t)p.P + (size_t)lin;
+            const size_t o = (size_t)g.out_map[m] * (size_t)p.P + (size_t)lin;
             if (g.cov[m]) {
                 if (EXACT) out64[o] = cov_map[lin]; else out32[o] = (float)cov_map[lin];
             } else {
@@ -489,7 +535,7 @@ k_near(DevProblem p, NearGroup g, const int *__restrict__ closest, const float *
                 const R d = (R)p.solpar_q * D1;
                 if (EXACT) out64[o] = (double)d; else out32[o] = (float)d;
             }
-            if (!EXACT && p.elec_map >= 0) {
+            if (do_e) {
                 float e = 0.f;
                 for (int c = 0; c < p.far_chunks; c++) e += p.far_partial[(size_t)c * (size_t)p.P + (size_t)lin];
                 out32[(size_t)p.elec_map * (size_t)p.P + (size_t)lin] = e + (float)e_near;
@@ -531,28 +577,22 @@ static unsigned near_blocks(const DevProblem &p)
     return (unsigned)(((p.n1x + NB_X - 1) / NB_X) * ((p.n1y + NB_Y - 1) / NB_Y) * ((p.n1z + NB_Z - 1) / NB_Z));
 }
 
-cudaError_t launch_closest_h(const DevProblem &p, int *closest, cudaStream_t s)
-{
-    k_closest_h<<<near_blocks(p), NB_THREADS, 0, s>>>(p, closest);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s)
 {
     k_covalent<<<(unsigned)((p.P + 255) / 256), 256, 0, s>>>(p, cov);
     return cudaGetLastError();
 }
 
-cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const int *closest,
-                        const float *rvf, const float *rv2f, const float *vdwT, int mpad, const float *etab,
+cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const float4 *atomA,
+                        const float4 *atomB, const int *meta, const float *vdwT, int mpad, const float *etab,
                         const float *solf, const double *cov_map, float *out32, double *out64,
                         unsigned long long *counters, cudaStream_t s)
 {
     if (exact)
-        k_near<true><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, closest, rvf, rv2f, vdwT, mpad, etab, solf,
-                                                         cov_map, out32, out64, counters);
+        k_near<true><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, atomA, atomB, meta, vdwT, mpad, etab, solf, cov_map,
+                                                         out32, out64, counters);
     else
-        k_near<false><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, closest, rvf, rv2f, vdwT, mpad, etab, solf,
+        k_near<false><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, atomA, atomB, meta, vdwT, mpad, etab, solf,
                                                           cov_map, out32, out64, counters);
     return cudaGetLastError();
 }

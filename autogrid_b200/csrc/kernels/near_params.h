@@ -5,6 +5,8 @@
 namespace agb {
 
 constexpr int NG_MAX = 16;                 // ligand maps per near-kernel launch
+constexpr int NG_MM = 4;                   // of which at most this many keep hbond min/max (placed first)
+constexpr int NT_SMALL = 1040;             // table bins a near pair can reach (r <= 8 A + guard)
 constexpr double AGB_NEAR_RADIUS = 8.05;   // A; > 8 A cutoff + FP32 distance error
 constexpr double AGB_CELL = 4.0;           // A; cell-list edge
 
@@ -19,10 +21,12 @@ enum : uint8_t {
 };
 
 struct NearGroup {
-    int g0, ng;               // ligand maps [g0, g0+ng)
-    int write_special;        // this launch also writes the d and e maps
-    int has_hrow;             // some action reads the hydrogen row (disorder_h)
-    uint8_t act[NG_MAX][8];   // by receptor hbond class 0..6
+    int ng;                    // ligand maps handled by this launch, in kernel order
+    int write_special;         // this launch also writes the d and e maps
+    int has_hrow;              // some action reads the hydrogen row (disorder_h)
+    int col0;                  // first column of this launch's maps in the [type][bin][col] table
+    unsigned long long actw[8];  // per receptor hbond class: 3-bit action of kernel map m at bits 3m..3m+2
+    int out_map[NG_MAX];       // output map index of kernel map m
     uint8_t cov[NG_MAX];
     double sp[NG_MAX], vp[NG_MAX];  // desolvation factors applied to this map's output
 };

@@ -30,7 +30,7 @@ def test_small_box_fp32_all_points(tmp_path, gpu_ctx, seed):
     maps = gpu_ctx.compute(prob, "fp32")
     _check(prob, maps)
     st = gpu_ctx.stats()
-    assert st.near_pairs > 0 and st.gpu_launches >= 3
+    assert st.near_pairs > 0 and st.gpu_launches >= 2
 
 
 @pytest.mark.parametrize("seed", [1, 2])
