@@ -186,6 +186,33 @@ size_t       ag_plan_points(const ag_plan *plan);        /* n1x*n1y*n1z     */
 ag_status    ag_plan_download(ag_plan *plan, float *host_maps);
 ag_status    ag_plan_destroy(ag_plan *plan);
 
+/*
+ * Electrostatic map for callers that cannot allocate device memory.  No
+ * counterpart in the reference (which has no library interface).  Meant for
+ * processes whose device memory is owned by their own pool allocator, or
+ * serving loops that may not call cudaMalloc/cudaFree (cudaFree synchronises
+ * the device) between requests.  Computes the e map of LOOP 1
+ * (main.cpp:2940-2982) from caller-owned DEVICE buffers -- d_coord
+ * [n_atoms*3] centred coordinates, d_charge [n_atoms], d_r_epsilon_fn
+ * [AG_NDIEL] (dddiel only) -- into the caller-owned device map d_emap
+ * [n1z*n1y*n1x] floats, on `stream` (a cudaStream_t; NULL = legacy default
+ * stream), and returns once the work is enqueued.
+ *
+ * Scratch lives in one static device array of AG_NOALLOC_SCRATCH_BYTES that
+ * every GPU which loads this entry point's module keeps until process exit;
+ * grids that do not fit (about 7.5 million points at 10,000 atoms) are
+ * rejected with AG_ERR_TOO_LARGE.  The first call on a device resolves the
+ * array's device address (cudaGetSymbolAddress), so make that first call
+ * before any stream capture.  All calls share the array: calls that overlap on
+ * the GPU (other streams, other host threads) race.  Every scratch word read
+ * is written earlier in the same call, so nothing needs clearing.
+ */
+#define AG_NOALLOC_SCRATCH_BYTES (32u << 20)
+ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, const double *d_coord,
+                                  const double *d_charge, const int32_t n1[3], double spacing,
+                                  int32_t dddiel, const double *d_r_epsilon_fn, double invdielcal,
+                                  double coeff_estat, float *d_emap, void *stream);
+
 /* Front / back end (replaces main.cpp:214-2776 and :3481-3565) ------------- */
 typedef struct ag_job ag_job;
 
