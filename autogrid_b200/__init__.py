@@ -5,8 +5,9 @@ Public API:
     Job(gpf, glg)                front end (GPF, receptor, tables, bond vectors)
     Context(device).compute(p)   hot path on one problem (FP32 or FP64 twin)
     Context(device).plan(p)      device-resident plan for repeated runs
+    Batch(ctx, problems)         many boxes in one persistent, graph-captured launch
 """
 from ._abi import AutoGridError, load_library  # noqa: F401
-from .api import Context, Job, Plan, Problem, Stats, run_gpf  # noqa: F401
+from .api import Batch, Context, Job, Plan, Problem, Stats, run_gpf  # noqa: F401
 
-__all__ = ["AutoGridError", "Context", "Job", "Plan", "Problem", "Stats", "load_library", "run_gpf"]
+__all__ = ["AutoGridError", "Batch", "Context", "Job", "Plan", "Problem", "Stats", "load_library", "run_gpf"]

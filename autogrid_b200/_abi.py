@@ -67,6 +67,12 @@ class ag_stats(C.Structure):
                 ("far_ms", C.c_double)]
 
 
+class ag_tuning(C.Structure):
+    _fields_ = [("far_tile", C.c_int32), ("far_chunked", C.c_int32), ("near_shape", C.c_int32),
+                ("candidates", C.c_int32), ("far_ms", C.c_double), ("near_ms", C.c_double),
+                ("far_ms_default", C.c_double), ("near_ms_default", C.c_double)]
+
+
 # name -> (restype, argtypes); every entry point declared in include/autogrid_b200.h
 SIGNATURES = {
     "ag_last_error": (C.c_char_p, []),
@@ -82,6 +88,15 @@ SIGNATURES = {
     "ag_plan_points": (C.c_size_t, [C.c_void_p]),
     "ag_plan_download": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ag_plan_destroy": (C.c_int, [C.c_void_p]),
+    "ag_batch_create": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(ag_problem)), C.c_int32, C.POINTER(ag_opts),
+                                  C.POINTER(C.c_void_p)]),
+    "ag_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_batch_device_maps": (C.c_void_p, [C.c_void_p, C.c_int32]),
+    "ag_batch_download": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "ag_batch_tuning": (C.c_int, [C.c_void_p, C.POINTER(ag_tuning)]),
+    "ag_batch_destroy": (C.c_int, [C.c_void_p]),
+    "ag_maps_compute_batch": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(ag_problem)), C.c_int32,
+                                        C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),
     "ag_job_load": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(C.c_void_p)]),
     "ag_job_problem": (C.POINTER(ag_problem), [C.c_void_p]),
     "ag_job_write_maps_f32": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -262,6 +262,47 @@ class Plan:
             pass
 
 
+class Batch:
+    """Many independent problems computed by one persistent launch per kernel
+    kind, graph-captured and autotuned at creation (ag_batch)."""
+
+    def __init__(self, ctx: Context, problems: list):
+        self.ctx = ctx
+        self.problems = list(problems)
+        self._lib = ctx._lib
+        self._structs = [p.struct() for p in self.problems]
+        arr = (C.POINTER(ag_problem) * len(self._structs))(*[C.pointer(s) for s in self._structs])
+        opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST)
+        h = C.c_void_p()
+        check(self._lib.ag_batch_create(ctx._h, arr, len(self.problems), C.byref(opts), C.byref(h)))
+        self._h = h
+
+    def run(self, stream: int | None = None) -> None:
+        check(self._lib.ag_batch_run(self._h, C.c_void_p(stream) if stream else None))
+
+    def download(self, i: int, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.empty(self.problems[i].map_shape, dtype=np.float32)
+        check(self._lib.ag_batch_download(self._h, int(i), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def tuning(self) -> dict:
+        t = _abi.ag_tuning()
+        check(self._lib.ag_batch_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in t._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.ag_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def run_gpf(gpf: str, glg: str | None = None, precision: str = "fp32", device: int = 0) -> np.ndarray:
     """Drop-in for `autogrid4 -p gpf -l glg`: parse, compute on the GPU, write the maps."""
     job = Job(gpf, glg)

@@ -432,6 +432,28 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
     return AG_OK;
 }
 
+FarArgs far_args(const ag_plan *pl)
+{
+    const DevProblem &d = pl->dp;
+    FarArgs a;
+    a.ax128 = pl->x128; a.ay128 = pl->y128; a.az128 = pl->z128; a.qw = pl->qw;
+    a.far_tab = pl->far_tab; a.partial = pl->far_partial;
+    a.spacing_adiv = d.spacing * AG_A_DIV; a.P = d.P;
+    a.n_atoms = d.n_atoms; a.chunk_atoms = pl->chunk_atoms;
+    a.n1x = d.n1x; a.n1y = d.n1y; a.n1z = d.n1z; a.nex = d.nex; a.ney = d.ney; a.nez = d.nez;
+    a.nfx = frames_x(d.n1x); a.nfy = frames_y(d.n1y); a.nfz = frames_z(d.n1z);
+    return a;
+}
+
+NearPtrs near_ptrs(const ag_plan *pl, unsigned long long *counters)
+{
+    NearPtrs q;
+    q.atomA = pl->atomA; q.atomB = pl->atomB; q.meta = pl->meta; q.vdwT = pl->vdwT; q.mpad = pl->mpad;
+    q.etab = pl->etab; q.solf = pl->solf; q.cov_map = pl->cov; q.out32 = pl->maps32; q.out64 = pl->maps64;
+    q.counters = counters;
+    return q;
+}
+
 ag_status run_plan(ag_plan *pl, cudaStream_t s)
 {
     ag_context *c = pl->ctx;
@@ -446,9 +468,7 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
             launches++;
         } else if (pl->n_chunks > 0) {
             AGB_CK(cudaEventRecord(c->evf0, s));
-            AGB_CK(launch_emap_far(pl->x128, pl->y128, pl->z128, pl->qw, d.n_atoms, pl->chunk_atoms, pl->n_chunks,
-                                   pl->far_tab, d.spacing * AG_A_DIV, d.n1x, d.n1y, d.n1z, d.nex, d.ney, d.nez,
-                                   d.P, pl->far_partial, s));
+            AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, s));
             AGB_CK(cudaEventRecord(c->evf1, s));
             launches++;
         }
@@ -460,8 +480,7 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
     const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || (!exact && d.elec_map >= 0);
     if (need_near) {
         for (const NearGroup &g : pl->groups) {
-            AGB_CK(launch_near(exact, d, g, pl->atomA, pl->atomB, pl->meta, pl->vdwT, pl->mpad, pl->etab, pl->solf,
-                               pl->cov, pl->maps32, pl->maps64, c->d_counters, s));
+            AGB_CK(launch_near(exact, d, g, near_ptrs(pl, c->d_counters), 0, s));
             launches++;
         }
     }
@@ -494,6 +513,138 @@ ag_status settle_stats(ag_context *c)
 }
 
 ag_status finish_stats(ag_plan *pl) { return settle_stats(pl->ctx); }
+
+ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out);
+
+}  // namespace
+
+struct ag_batch {
+    ag_context *ctx = nullptr;
+    std::vector<std::unique_ptr<ag_plan>> plans;
+    std::vector<FarArgs> far;         // per instance, in work order
+    std::vector<NearInst> near;       // per (instance, group), in work order
+    std::vector<long long> far_begin, near_begin;
+    BufferSet bufs;
+    FarArgs *d_far = nullptr;
+    NearInst *d_near = nullptr;
+    long long *d_far_begin = nullptr, *d_near_begin = nullptr;
+    unsigned long long *d_counters = nullptr;  // [0] far units, [1] near units, [2..3] near statistics
+    ag_tuning tune{};
+    int far_ctas_per_sm = 3, near_ctas_per_sm = 2;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~ag_batch()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+    }
+};
+
+namespace {
+
+// Far-field work units of one instance with the given chunking.
+long long far_units(const FarArgs &a) { return (long long)a.nfx * a.nfy * a.nfz * ((a.n_atoms + a.chunk_atoms - 1) / std::max(1, a.chunk_atoms)); }
+
+ag_status batch_upload_far(ag_batch *b, bool chunked)
+{
+    // chunking: one unit per (frame, all atoms), or per (frame, 2048-atom chunk)
+    b->far_begin.assign(1, 0);
+    for (size_t i = 0; i < b->far.size(); i++) {
+        FarArgs &a = b->far[i];
+        a.chunk_atoms = chunked ? std::min(2048, std::max(a.n_atoms, 1)) : std::max(a.n_atoms, 1);
+        b->far_begin.push_back(b->far_begin.back() + (a.n_atoms > 0 ? far_units(a) : 0));
+    }
+    // the near kernel sums the instance's partial chunks
+    for (NearInst &ni : b->near) {
+        const FarArgs *a = nullptr;
+        for (const FarArgs &f : b->far)
+            if (f.partial == ni.p.far_partial) { a = &f; break; }
+        ni.p.far_chunks = (a && a->n_atoms > 0 && ni.p.elec_map >= 0) ? (a->n_atoms + a->chunk_atoms - 1) / a->chunk_atoms : 0;
+    }
+    AGB_CK(cudaMemcpyAsync(b->d_far, b->far.data(), sizeof(FarArgs) * b->far.size(), cudaMemcpyHostToDevice, b->ctx->stream));
+    AGB_CK(cudaMemcpyAsync(b->d_far_begin, b->far_begin.data(), sizeof(long long) * b->far_begin.size(),
+                           cudaMemcpyHostToDevice, b->ctx->stream));
+    AGB_CK(cudaMemcpyAsync(b->d_near, b->near.data(), sizeof(NearInst) * b->near.size(), cudaMemcpyHostToDevice,
+                           b->ctx->stream));
+    return AG_OK;
+}
+
+ag_status batch_launch(ag_batch *b, cudaStream_t s, int tile, int shape, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2)
+{
+    AGB_CK(cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(unsigned long long), s));
+    if (e0) AGB_CK(cudaEventRecord(e0, s));
+    if (b->far_begin.back() > 0)
+        AGB_CK(launch_emap_far_batch(b->d_far, b->d_far_begin, (int)b->far.size(), b->d_counters, tile,
+                                     b->far_ctas_per_sm, s));
+    if (e1) AGB_CK(cudaEventRecord(e1, s));
+    if (b->near_begin.back() > 0)
+        AGB_CK(launch_near_batch(b->d_near, b->d_near_begin, (int)b->near.size(), b->d_counters + 1, shape,
+                                 b->near_ctas_per_sm, s));
+    if (e2) AGB_CK(cudaEventRecord(e2, s));
+    return AG_OK;
+}
+
+// Time one configuration (best of two runs).
+ag_status batch_time(ag_batch *b, int tile, int shape, double *far_ms, double *near_ms)
+{
+    cudaStream_t s = b->ctx->stream;
+    cudaEvent_t e[3];
+    for (auto &x : e) AGB_CK(cudaEventCreate(&x));
+    double bf = 1e30, bn = 1e30;
+    ag_status st = AG_OK;
+    for (int rep = 0; rep < 2 && st == AG_OK; rep++) {
+        st = batch_launch(b, s, tile, shape, e[0], e[1], e[2]);
+        if (st != AG_OK) break;
+        cudaError_t ce = cudaEventSynchronize(e[2]);
+        if (ce != cudaSuccess) { st = cuda_fail(ce, "cudaEventSynchronize"); break; }
+        float f = 0, n = 0;
+        cudaEventElapsedTime(&f, e[0], e[1]);
+        cudaEventElapsedTime(&n, e[1], e[2]);
+        bf = std::min(bf, (double)f);
+        bn = std::min(bn, (double)n);
+    }
+    for (auto &x : e) cudaEventDestroy(x);
+    *far_ms = bf;
+    *near_ms = bn;
+    return st;
+}
+
+// The autotuner: far tile x chunking, then near brick shape, on this batch.
+ag_status batch_autotune(ag_batch *b)
+{
+    ag_tuning &t = b->tune;
+    t = ag_tuning{};
+    double best_far = 1e30, best_near = 1e30;
+    int best_tile = 512, best_chunked = 0, best_shape = 0;
+    const int tiles[3] = {512, 256, 1024};
+    for (int chunked = 0; chunked < 2; chunked++) {
+        ag_status st = batch_upload_far(b, chunked != 0);
+        if (st != AG_OK) return st;
+        for (int ti = 0; ti < 3; ti++) {
+            double f = 0, n = 0;
+            st = batch_time(b, tiles[ti], 0, &f, &n);
+            if (st != AG_OK) return st;
+            t.candidates++;
+            if (chunked == 0 && ti == 0) { t.far_ms_default = f; t.near_ms_default = n; }
+            if (f < best_far) { best_far = f; best_tile = tiles[ti]; best_chunked = chunked; }
+        }
+    }
+    ag_status st = batch_upload_far(b, best_chunked != 0);
+    if (st != AG_OK) return st;
+    for (int shape = 0; shape < 3; shape++) {
+        double f = 0, n = 0;
+        st = batch_time(b, best_tile, shape, &f, &n);
+        if (st != AG_OK) return st;
+        t.candidates++;
+        if (n < best_near) { best_near = n; best_shape = shape; }
+    }
+    t.far_tile = best_tile;
+    t.far_chunked = best_chunked;
+    t.near_shape = best_shape;
+    t.far_ms = best_far;
+    t.near_ms = best_near;
+    return AG_OK;
+}
 
 ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out)
 {
@@ -642,6 +793,153 @@ ag_status ag_plan_destroy(ag_plan *plan)
     cudaStreamSynchronize(plan->ctx->stream);
     delete plan;
     return AG_OK;
+}
+
+
+ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, int32_t n, const ag_opts *opts,
+                          ag_batch **out)
+{
+    if (!ctx || !problems || !out || n < 1) return invalid("ag_batch_create: bad argument");
+    *out = nullptr;
+    ag_opts o{};
+    if (opts) o = *opts;
+    if (o.precision != AG_PREC_FP32) return invalid("batches run the FP32 path");
+    AGB_CK(cudaSetDevice(ctx->device));
+    std::unique_ptr<ag_batch> b(new ag_batch());
+    b->ctx = ctx;
+    for (int i = 0; i < n; i++) {
+        ag_plan *pl = nullptr;
+        ag_status st = make_plan(ctx, problems[i], &o, true, &pl);
+        if (st != AG_OK) {
+            set_last_error("instance " + std::to_string(i) + ": " + ag_last_error());
+            return st;
+        }
+        b->plans.emplace_back(pl);
+    }
+    // work order: instances by decreasing far work (largest units first)
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const DevProblem &a = b->plans[x]->dp, &c = b->plans[y]->dp;
+        return (double)a.P * (a.n_atoms + 64) > (double)c.P * (c.n_atoms + 64);
+    });
+    b->near_begin.assign(1, 0);
+    for (int i : order) {
+        ag_plan *pl = b->plans[i].get();
+        // each instance's partial buffer must hold the chunked layout (at most ceil(N/2048) chunks)
+        const int max_chunks = std::max(1, (pl->dp.n_atoms + 2047) / 2048);
+        if (pl->dp.elec_map >= 0 && pl->dp.n_atoms > 0) {
+            void *v = nullptr;
+            AGB_CK(pl->bufs->ensure("far_partial", (size_t)max_chunks * (size_t)pl->dp.P * sizeof(float), &v));
+            pl->far_partial = (float *)v;
+            pl->dp.far_partial = pl->far_partial;
+            b->far.push_back(far_args(pl));
+        }
+        const bool need_near = pl->dp.n_atom_maps > 0 || pl->dp.dsolv_map >= 0 || pl->dp.elec_map >= 0;
+        if (need_near)
+            for (const NearGroup &g : pl->groups) {
+                NearInst ni;
+                std::memset(&ni, 0, sizeof ni);
+                ni.p = pl->dp;
+                ni.g = g;
+                ni.ptr = near_ptrs(pl, nullptr);
+                b->near.push_back(ni);
+                b->near_begin.push_back(b->near_begin.back() + near_bricks(pl->dp, 0));
+            }
+        if (pl->any_cov) {
+            AGB_CK(launch_covalent(pl->dp, pl->cov, ctx->stream));  // geometry only: computed once
+        }
+    }
+    void *v = nullptr;
+    AGB_CK(b->bufs.ensure("far", sizeof(FarArgs) * std::max<size_t>(1, b->far.size()), &v));
+    b->d_far = (FarArgs *)v;
+    AGB_CK(b->bufs.ensure("far_begin", sizeof(long long) * (b->far.size() + 1), &v));
+    b->d_far_begin = (long long *)v;
+    AGB_CK(b->bufs.ensure("near", sizeof(NearInst) * std::max<size_t>(1, b->near.size()), &v));
+    b->d_near = (NearInst *)v;
+    AGB_CK(b->bufs.ensure("near_begin", sizeof(long long) * b->near_begin.size(), &v));
+    b->d_near_begin = (long long *)v;
+    AGB_CK(b->bufs.ensure("counters", 4 * sizeof(unsigned long long), &v));
+    b->d_counters = (unsigned long long *)v;
+    if (b->far.empty()) b->far_begin.assign(1, 0);
+    // near units are counted per brick of the tuned shape: refresh after tuning
+    ag_status st = batch_autotune(b.get());
+    if (st != AG_OK) return st;
+    // final near unit table for the chosen shape
+    {
+        b->near_begin.assign(1, 0);
+        for (const NearInst &ni : b->near) b->near_begin.push_back(b->near_begin.back() + near_bricks(ni.p, b->tune.near_shape));
+        AGB_CK(cudaMemcpyAsync(b->d_near_begin, b->near_begin.data(), sizeof(long long) * b->near_begin.size(),
+                               cudaMemcpyHostToDevice, ctx->stream));
+    }
+    // capture the run as a graph on a private stream
+    cudaStream_t cs;
+    AGB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    AGB_CK(cudaStreamSynchronize(ctx->stream));
+    AGB_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    st = batch_launch(b.get(), cs, b->tune.far_tile, b->tune.near_shape, nullptr, nullptr, nullptr);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    if (st != AG_OK) { if (g) cudaGraphDestroy(g); return st; }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    b->graph = g;
+    AGB_CK(cudaGraphInstantiate(&b->exec, g, 0));
+    *out = b.release();
+    return AG_OK;
+}
+
+ag_status ag_batch_run(ag_batch *b, void *stream)
+{
+    if (!b) return invalid("null batch");
+    cudaStream_t s = stream ? (cudaStream_t)stream : b->ctx->stream;
+    AGB_CK(cudaGraphLaunch(b->exec, s));
+    return AG_OK;
+}
+
+const float *ag_batch_device_maps(const ag_batch *b, int32_t i)
+{
+    if (!b || i < 0 || i >= (int32_t)b->plans.size()) return nullptr;
+    return b->plans[i]->maps32;
+}
+
+ag_status ag_batch_download(ag_batch *b, int32_t i, float *host_maps)
+{
+    if (!b || !host_maps || i < 0 || i >= (int32_t)b->plans.size()) return invalid("ag_batch_download: bad argument");
+    const ag_plan *pl = b->plans[i].get();
+    AGB_CK(cudaMemcpyAsync(host_maps, pl->maps32, (size_t)pl->dp.n_maps * (size_t)pl->dp.P * sizeof(float),
+                           cudaMemcpyDefault, b->ctx->stream));
+    AGB_CK(cudaStreamSynchronize(b->ctx->stream));
+    return AG_OK;
+}
+
+ag_status ag_batch_tuning(const ag_batch *b, ag_tuning *out)
+{
+    if (!b || !out) return invalid("null argument");
+    *out = b->tune;
+    return AG_OK;
+}
+
+ag_status ag_batch_destroy(ag_batch *b)
+{
+    if (!b) return AG_OK;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    delete b;
+    return AG_OK;
+}
+
+ag_status ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *problems, int32_t n, const ag_opts *opts,
+                                float *const *maps)
+{
+    if (!maps) return invalid("null maps");
+    ag_batch *b = nullptr;
+    ag_status st = ag_batch_create(ctx, problems, n, opts, &b);
+    if (st != AG_OK) return st;
+    std::unique_ptr<ag_batch, ag_status (*)(ag_batch *)> guard(b, ag_batch_destroy);
+    st = ag_batch_run(b, nullptr);
+    for (int i = 0; st == AG_OK && i < n; i++) st = ag_batch_download(b, i, maps[i]);
+    return st;
 }
 
 }  // extern "C"

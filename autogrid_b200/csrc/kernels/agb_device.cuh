@@ -66,6 +66,18 @@ __device__ __forceinline__ float far_pair_t(float ax, float px, float s)
     return __fmul_rn(t2, rsqrt_approx(t2));
 }
 
+// Far-field e-map kernel arguments for one instance.
+struct FarArgs {
+    const double *ax128, *ay128, *az128;  // x*A_DIV (exact in FP64)
+    const float *qw;                      // q*coeff_estat*A_DIV
+    const float *far_tab;                 // [NDIEL], zero below FAR_BIN0
+    float *partial;                       // [chunks][P]
+    double spacing_adiv;
+    long long P;
+    int n_atoms, chunk_atoms;
+    int n1x, n1y, n1z, nex, ney, nez, nfx, nfy, nfz;
+};
+
 // Device image of one problem instance.
 struct DevProblem {
     int n_atoms, n_maps, n_atom_maps, n_rec_types;

@@ -13,12 +13,13 @@
 //                in fixed chunk order by the near-field kernel (deterministic).
 // k_emap_exact -- FP64 twin: every pair, exactly the reference expression
 //                (nested hypot, double table), file order summation.
+#include <algorithm>
+
 #include "agb_device.cuh"
 
 namespace agb {
 
 constexpr int EF_THREADS = 256;
-constexpr int EF_TILE = 512;      // atoms per shared-memory tile
 constexpr int EF_PAIRS = 4;       // float2 pairs of points per thread (8 points)
 
 __device__ __forceinline__ float lds_f32(uint32_t addr)
@@ -28,65 +29,62 @@ __device__ __forceinline__ float lds_f32(uint32_t addr)
     return v;
 }
 
-// Atom tile entry: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
-__global__ void __launch_bounds__(EF_THREADS, 3)
-k_emap_far(const double *__restrict__ ax128, const double *__restrict__ ay128,
-           const double *__restrict__ az128, const float *__restrict__ qw, int n_atoms,
-           int chunk_atoms, const float *__restrict__ far_tab, double spacing_adiv,
-           int n1x, int n1y, int n1z, int nex, int ney, int nez, int nfx, int nfy,
-           long long P, float *__restrict__ partial)
+__device__ __forceinline__ void load_far_table(float4 *s_tab4, const float *far_tab)
 {
-    extern __shared__ float4 ef_smem[];
-    float4 *s_tab4 = ef_smem;                         // AG_NDIEL floats
-    float4 *s_atom = ef_smem + AG_NDIEL / 4;          // EF_TILE entries
-    const int tid = threadIdx.x;
-    for (int i = tid; i < AG_NDIEL / 4; i += EF_THREADS) s_tab4[i] = __ldg(((const float4 *)far_tab) + i);
+    for (int i = threadIdx.x; i < AG_NDIEL / 4; i += EF_THREADS) s_tab4[i] = __ldg(((const float4 *)far_tab) + i);
+}
 
-    const int f = blockIdx.x;
-    const int fx = f % nfx, fy = (f / nfx) % nfy, fz = f / (nfx * nfy);
+// One work unit: frame `f` of one instance against atom chunk `chunk`.
+// The caller has loaded the instance's table into s_tab4 and synchronised.
+// Atom tile entries: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
+template <int TILE>
+__device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
+{
+    const int tid = threadIdx.x;
+    const int fx = f % a.nfx, fy = (f / a.nfx) % a.nfy, fz = f / (a.nfx * a.nfy);
     const int ox = fx * FRAME_X, oy = fy * FRAME_Y, oz = fz * FRAME_Z;
     // frame origin in bins, exactly (ox-nex)*spacing*A_DIV as the reference forms c (main.cpp:2859)
-    const double X0 = frame_origin_bins(ox, nex, spacing_adiv);
-    const double Y0 = frame_origin_bins(oy, ney, spacing_adiv);
-    const double Z0 = frame_origin_bins(oz, nez, spacing_adiv);
+    const double X0 = frame_origin_bins(ox, a.nex, a.spacing_adiv);
+    const double Y0 = frame_origin_bins(oy, a.ney, a.spacing_adiv);
+    const double Z0 = frame_origin_bins(oz, a.nez, a.spacing_adiv);
 
     // compact 4x4x2 lane footprint per warp (fewest table bank conflicts)
     const int lane = tid & 31, w = tid >> 5;
     const int tx = lane & 3;
     const int ty = ((lane >> 2) & 3) + 4 * (w & 1);
     const int tz = (lane >> 4) + 2 * (w >> 1);
-    const float py = frame_point_coord(ty, spacing_adiv);
-    const float pz = frame_point_coord(tz, spacing_adiv);
+    const float py = frame_point_coord(ty, a.spacing_adiv);
+    const float pz = frame_point_coord(tz, a.spacing_adiv);
     float2 npx[EF_PAIRS];
 #pragma unroll
     for (int j = 0; j < EF_PAIRS; j++)
-        npx[j] = make_float2(-frame_point_coord(tx + 8 * j, spacing_adiv),
-                             -frame_point_coord(tx + 8 * j + 4, spacing_adiv));
+        npx[j] = make_float2(-frame_point_coord(tx + 8 * j, a.spacing_adiv),
+                             -frame_point_coord(tx + 8 * j + 4, a.spacing_adiv));
     const float2 npyz = make_float2(-py, -pz);
     float2 tot[EF_PAIRS];
 #pragma unroll
     for (int j = 0; j < EF_PAIRS; j++) tot[j] = make_float2(0.f, 0.f);
 
-    // 32-bit shared address of s_tab, pre-biased so that the bit pattern of
-    // (t + 2^23) rounded toward zero indexes the table directly:
+    // 32-bit shared address of the table, pre-biased so that the bit pattern of
+    // (t + 2^23) rounded toward zero indexes it directly:
     // bits(t + 2^23) = 0x4B000000 + floor(t) for 0 <= t < 2^23.
     const uint32_t tab_base = (uint32_t)__cvta_generic_to_shared(s_tab4) - (0x4B000000u << 2);
     const float2 magic = make_float2(8388608.f, 8388608.f);
     const float2 tmax = make_float2(FAR_MAX_T, FAR_MAX_T);
 
-    const int a_begin = blockIdx.y * chunk_atoms;
-    const int a_end = min(n_atoms, a_begin + chunk_atoms);
-    for (int a0 = a_begin; a0 < a_end; a0 += EF_TILE) {
-        const int na = min(EF_TILE, a_end - a0);
+    const int a_begin = chunk * a.chunk_atoms;
+    const int a_end = min(a.n_atoms, a_begin + a.chunk_atoms);
+    for (int a0 = a_begin; a0 < a_end; a0 += TILE) {
+        const int na = min(TILE, a_end - a0);
         __syncthreads();
-        for (int i = tid; i < EF_TILE; i += EF_THREADS) {
+        for (int i = tid; i < TILE; i += EF_THREADS) {
             float4 v;
             if (i < na) {
-                const int a = a0 + i;
-                v.x = frame_atom_coord(__ldg(ax128 + a), X0);
-                v.y = frame_atom_coord(__ldg(ay128 + a), Y0);
-                v.z = frame_atom_coord(__ldg(az128 + a), Z0);
-                v.w = __ldg(qw + a);
+                const int at = a0 + i;
+                v.x = frame_atom_coord(__ldg(a.ax128 + at), X0);
+                v.y = frame_atom_coord(__ldg(a.ay128 + at), Y0);
+                v.z = frame_atom_coord(__ldg(a.az128 + at), Z0);
+                v.w = __ldg(a.qw + at);
             } else {
                 v = make_float4(1.0e6f, 1.0e6f, 1.0e6f, 0.f);  // far, zero weight
             }
@@ -123,14 +121,64 @@ k_emap_far(const double *__restrict__ ax128, const double *__restrict__ ay128,
     }
 
     const int iy = oy + ty, iz = oz + tz;
-    if (iy < n1y && iz < n1z) {
-        float *out = partial + (size_t)blockIdx.y * (size_t)P + ((size_t)iz * n1y + iy) * (size_t)n1x;
+    if (iy < a.n1y && iz < a.n1z) {
+        float *out = a.partial + (size_t)chunk * (size_t)a.P + ((size_t)iz * a.n1y + iy) * (size_t)a.n1x;
 #pragma unroll
         for (int j = 0; j < EF_PAIRS; j++) {
             const int ix0 = ox + tx + 8 * j, ix1 = ix0 + 4;
-            if (ix0 < n1x) out[ix0] = tot[j].x;
-            if (ix1 < n1x) out[ix1] = tot[j].y;
+            if (ix0 < a.n1x) out[ix0] = tot[j].x;
+            if (ix1 < a.n1x) out[ix1] = tot[j].y;
         }
+    }
+}
+
+// Single instance: one CTA per (frame, chunk) = (blockIdx.x, blockIdx.y).
+template <int TILE>
+__global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
+{
+    extern __shared__ float4 ef_smem[];
+    float4 *s_tab4 = ef_smem;                 // AG_NDIEL floats
+    float4 *s_atom = ef_smem + AG_NDIEL / 4;  // TILE entries
+    load_far_table(s_tab4, a.far_tab);
+    far_unit<TILE>(a, blockIdx.x, blockIdx.y, s_tab4, s_atom);
+}
+
+// Many instances, persistent: each CTA takes (instance, frame, chunk) units
+// from an atomic counter until none is left; units are numbered instance by
+// instance (instances ordered by decreasing work) and never wait on each other.
+template <int TILE>
+__global__ void __launch_bounds__(EF_THREADS, 3)
+k_emap_far_batch(const FarArgs *__restrict__ insts, const long long *__restrict__ unit_begin, int n_inst,
+                 unsigned long long *__restrict__ counter)
+{
+    extern __shared__ float4 ef_smem[];
+    float4 *s_tab4 = ef_smem;
+    float4 *s_atom = ef_smem + AG_NDIEL / 4;
+    __shared__ long long s_unit;
+    __shared__ FarArgs s_a;
+    int cur = -1;
+    const long long total = unit_begin[n_inst];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const long long u = s_unit;
+        if (u >= total) break;
+        int lo = 0, hi = n_inst - 1;  // instance holding unit u
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (unit_begin[mid] <= u) lo = mid; else hi = mid - 1;
+        }
+        if (lo != cur) {
+            __syncthreads();
+            if (threadIdx.x == 0) s_a = insts[lo];
+            __syncthreads();
+            load_far_table(s_tab4, s_a.far_tab);
+            cur = lo;
+        }
+        const long long lu = u - unit_begin[lo];
+        const int frames = s_a.nfx * s_a.nfy * s_a.nfz;
+        far_unit<TILE>(s_a, (int)(lu % frames), (int)(lu / frames), s_tab4, s_atom);
     }
 }
 
@@ -177,17 +225,47 @@ int frames_x(int n1x) { return (n1x + FRAME_X - 1) / FRAME_X; }
 int frames_y(int n1y) { return (n1y + FRAME_Y - 1) / FRAME_Y; }
 int frames_z(int n1z) { return (n1z + FRAME_Z - 1) / FRAME_Z; }
 
-cudaError_t launch_emap_far(const double *ax128, const double *ay128, const double *az128, const float *qw,
-                            int n_atoms, int chunk_atoms, int n_chunks, const float *far_tab,
-                            double spacing_adiv, int n1x, int n1y, int n1z, int nex, int ney, int nez,
-                            long long P, float *partial, cudaStream_t s)
+size_t far_smem_bytes(int tile) { return AG_NDIEL * sizeof(float) + (size_t)tile * sizeof(float4); }
+
+cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s)
 {
-    const int nfx = frames_x(n1x), nfy = frames_y(n1y), nfz = frames_z(n1z);
-    const size_t smem = AG_NDIEL * sizeof(float) + EF_TILE * sizeof(float4);
-    dim3 grid((unsigned)(nfx * nfy * nfz), (unsigned)n_chunks);
-    k_emap_far<<<grid, EF_THREADS, smem, s>>>(ax128, ay128, az128, qw, n_atoms, chunk_atoms, far_tab,
-                                              spacing_adiv, n1x, n1y, n1z, nex, ney, nez, nfx, nfy, P, partial);
+    const int frames = a.nfx * a.nfy * a.nfz;
+    dim3 grid((unsigned)frames, (unsigned)n_chunks);
+    const size_t smem = far_smem_bytes(tile);
+    if (tile == 256) k_emap_far<256><<<grid, EF_THREADS, smem, s>>>(a);
+    else if (tile == 1024) k_emap_far<1024><<<grid, EF_THREADS, smem, s>>>(a);
+    else k_emap_far<512><<<grid, EF_THREADS, smem, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int TILE>
+static cudaError_t far_batch_t(const FarArgs *insts, const long long *unit_begin, int n_inst,
+                               unsigned long long *counter, int ctas_per_sm, cudaStream_t s)
+{
+    const size_t smem = far_smem_bytes(TILE);
+    static bool attr_set = false;  // set once, outside any stream capture (the first call is the autotuner's)
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(k_emap_far_batch<TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_emap_far_batch<TILE>, EF_THREADS, smem);
+    const int per_sm = std::max(1, std::min(ctas_per_sm, occ));
+    k_emap_far_batch<TILE><<<sms * per_sm, EF_THREADS, smem, s>>>(insts, unit_begin, n_inst, counter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_begin, int n_inst,
+                                  unsigned long long *counter, int tile, int ctas_per_sm, cudaStream_t s)
+{
+    if (tile == 256) return far_batch_t<256>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+    if (tile == 1024) return far_batch_t<1024>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+    return far_batch_t<512>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
 }
 
 cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s)

@@ -7,16 +7,45 @@
 
 namespace agb {
 
-cudaError_t launch_emap_far(const double *ax128, const double *ay128, const double *az128, const float *qw,
-                            int n_atoms, int chunk_atoms, int n_chunks, const float *far_tab,
-                            double spacing_adiv, int n1x, int n1y, int n1z, int nex, int ney, int nez,
-                            long long P, float *partial, cudaStream_t s);
+struct NearPtrs {
+    const float4 *atomA, *atomB;
+    const int *meta;
+    const float *vdwT;
+    int mpad;
+    const float *etab, *solf;
+    const double *cov_map;
+    float *out32;
+    double *out64;
+    unsigned long long *counters;
+};
+
+struct NearSmem {
+    float4 pos[NB_CHUNK_MAX], a[NB_CHUNK_MAX], b[NB_CHUNK_MAX];
+    int meta[NB_CHUNK_MAX], idx[NB_CHUNK_MAX];
+    float etab[NT_SMALL], sol[NT_SMALL];
+    int seg_start[NB_SEGS_MAX], seg_off[NB_SEGS_MAX + 1];
+    int total;
+    unsigned long long cnt[2];
+};
+
+struct NearInst {
+    DevProblem p;
+    NearGroup g;
+    NearPtrs ptr;
+};
+
+
+size_t far_smem_bytes(int tile);
+cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s);
+cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_begin, int n_inst,
+                                  unsigned long long *counter, int tile, int ctas_per_sm, cudaStream_t s);
 cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s);
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s);
-cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const float4 *atomA,
-                        const float4 *atomB, const int *meta, const float *vdwT, int mpad, const float *etab,
-                        const float *solf, const double *cov_map, float *out32, double *out64,
-                        unsigned long long *counters, cudaStream_t s);
+int near_bricks(const DevProblem &p, int shape);
+cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int shape,
+                        cudaStream_t s);
+cudaError_t launch_near_batch(const NearInst *insts, const long long *unit_begin, int n_inst,
+                              unsigned long long *counter, int shape, int ctas_per_sm, cudaStream_t s);
 int frames_x(int n1x);
 int frames_y(int n1y);
 int frames_z(int n1z);

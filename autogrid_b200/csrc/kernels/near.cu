@@ -19,16 +19,16 @@
 //   Desolvation is factored: sum_a sol(r)(sp_m vol_a + (solpar_a+qasp|q_a|) vp_m)
 //   = sp_m*D1 + vp_m*D2 with D1 = sum vol_a sol, D2 = sum (solpar_a+qasp|q_a|) sol,
 //   and the d map is qasp*D1 (main.cpp:3381-3404).
+#include <algorithm>
 #include <type_traits>
 
-#include "agb_device.cuh"
-#include "near_params.h"
+#include "kernels.h"
 
 namespace agb {
 
-constexpr int NB_X = 8, NB_Y = 8, NB_Z = 4, NB_THREADS = 256;
-constexpr int NB_CHUNK = 384;   // candidates staged at once (most bricks need one chunk)
-constexpr int NB_SEGS = 64;
+constexpr int NB_THREADS = 256;   // one thread per brick point (brick shape is a template parameter)
+constexpr int NB_CHUNK = NB_CHUNK_MAX;   // candidates staged at once (most bricks need one chunk)
+constexpr int NB_SEGS = NB_SEGS_MAX;
 constexpr float GUARD_BIN = 2.0e-3f;   // bins: > 3x the FP32 distance error bound
 constexpr float GUARD_COS = 5.0e-5f;
 constexpr double APPROX_ZERO_D = 1.0e-6;
@@ -201,12 +201,13 @@ __device__ __forceinline__ bool pair_fast(int meta, float4 rvA, float4 rvB, int 
         }
     } else if (hb == 4) {
         o.rdon = (cos_theta <= 0.f) ? 0.f : cos_theta * cos_theta;
-    } else if (!dis) {  // A2 ordered
+    } else if (!dis) {  // A2 ordered (main.cpp:3163-3246)
         if (fabsf(cos_theta) < GUARD_COS && !rv_zero) return false;
         const float w0 = rvB.x, w1 = rvB.y, w2 = rvB.z;
         float t0 = dn0 * w0 + dn1 * w1 + dn2 * w2;
         t0 = fminf(fmaxf(t0, -1.f), 1.f);
-        t0 = PIH - acosf(t0);
+        // cos(pi/2 - acos(t0)) = sqrt(1 - t0^2)
+        const float cos_t0 = sqrtf(fmaxf(1.f - t0 * t0, 0.f));
         const float c0 = dn1 * w2 - dn2 * w1, c1 = dn2 * w0 - dn0 * w2, c2 = dn0 * w1 - dn1 * w0;
         float rd2 = c0 * c0 + c1 * c1 + c2 * c2;
         rd2 = fmaxf(rd2, 1.0e-6f);
@@ -215,18 +216,20 @@ __device__ __forceinline__ bool pair_fast(int meta, float4 rvA, float4 rvB, int 
         o.rdon = 0.f;
         if (cos_theta >= 0.f) {
             ti = fminf(fmaxf(ti, -1.f), 1.f);
-            ti = fabsf(acosf(ti) - PIH);
-            o.rdon = (0.9f + 0.1f * sinf(ti + ti)) * cosf(t0);
+            // sin(2|acos(ti) - pi/2|) = |sin(2 acos(ti))| = 2|ti|sqrt(1 - ti^2)
+            const float s2 = 2.f * fabsf(ti) * sqrtf(fmaxf(1.f - ti * ti, 0.f));
+            o.rdon = (0.9f + 0.1f * s2) * cos_t0;
         } else if (cos_theta >= -0.34202f) {
             const float b = 0.116978f - cos_theta * cos_theta;
-            o.rdon = 562.25f * (b * b * b) * cosf(t0);
+            o.rdon = 562.25f * (b * b * b) * cos_t0;
         }
-    } else {  // A2 disordered (cylindrical hydroxyl)
+    } else {  // A2 disordered, cylindrical hydroxyl (main.cpp:3247-3272)
         const float ct = fminf(fmaxf(cos_theta, -1.f), 1.f);
-        const float theta = acosf(ct);
         o.racc = 0.f; o.rdon = 0.f;
-        if (theta <= 1.24791f + PIH) {
-            const float c = cosf(theta - 1.24791f);
+        // theta = acos(ct) <= 1.24791 + pi/2  <=>  ct >= -sin(1.24791); the value is 0 at the edge
+        if (ct >= -0.94832352f) {
+            // cos(theta - a) = ct cos(a) + sin(theta) sin(a), a = 1.24791
+            const float c = ct * 0.31730505f + sqrtf(fmaxf(1.f - ct * ct, 0.f)) * 0.94832352f;
             o.rdon = (c * c) * (c * c);
             o.racc = o.rdon;
         }
@@ -251,40 +254,31 @@ __device__ __forceinline__ double h_dist(const DevProblem &p, int a, double cx, 
 //         reference's order (strict '<' in file order == lowest index on a tie);
 //         points with no DS/D1 atom within 8 A scan all of them (rare)
 //  B      pair terms of every candidate inside 8 A (+ e-map near pairs)
-template <bool EXACT>
-__global__ void __launch_bounds__(NB_THREADS, 2)
-k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4 *__restrict__ atomB,
-       const int *__restrict__ atom_meta, const float *__restrict__ vdwT, int mpad,
-       const float *__restrict__ etab, const float *__restrict__ solf, const double *__restrict__ cov_map,
-       float *__restrict__ out32, double *__restrict__ out64, unsigned long long *__restrict__ counters)
+// One brick `b` of one instance (p, g).
+template <bool EXACT, int BX, int BY, int BZ>
+__device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int b,
+                                          NearSmem &S)
 {
+    static_assert(BX * BY * BZ == NB_THREADS, "one thread per brick point");
+    static_assert(FRAME_X % BX == 0 && FRAME_Y % BY == 0 && FRAME_Z % BZ == 0, "bricks tile far frames");
     using R = typename std::conditional<EXACT, double, float>::type;
-    __shared__ float4 s_pos[NB_CHUNK];
-    __shared__ float4 s_a[NB_CHUNK], s_b[NB_CHUNK];
-    __shared__ int s_meta[NB_CHUNK], s_idx[NB_CHUNK];
-    __shared__ float s_etab[NT_SMALL], s_sol[NT_SMALL];
-    __shared__ int s_seg_start[NB_SEGS], s_seg_off[NB_SEGS + 1];
-    __shared__ int s_total;
-    __shared__ unsigned long long s_cnt[2];
-
     const int tid = threadIdx.x;
-    if (tid < 2) s_cnt[tid] = 0ull;
+    if (tid < 2) S.cnt[tid] = 0ull;
     for (int i = tid; i < NT_SMALL; i += NB_THREADS) {
-        s_etab[i] = etab[i];
-        s_sol[i] = solf[i];
+        S.etab[i] = ptr.etab[i];
+        S.sol[i] = ptr.solf[i];
     }
     __syncthreads();
-    const int nbx = (p.n1x + NB_X - 1) / NB_X, nby = (p.n1y + NB_Y - 1) / NB_Y;
-    const int b = blockIdx.x;
+    const int nbx = (p.n1x + BX - 1) / BX, nby = (p.n1y + BY - 1) / BY;
     const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
-    const int ix = bx * NB_X + (tid & 7), iy = by * NB_Y + ((tid >> 3) & 7), iz = bz * NB_Z + (tid >> 6);
+    const int ix = bx * BX + tid % BX, iy = by * BY + (tid / BX) % BY, iz = bz * BZ + tid / (BX * BY);
     const bool valid = ix < p.n1x && iy < p.n1y && iz < p.n1z;
     const long long lin = ((long long)iz * p.n1y + iy) * p.n1x + ix;
 
     // far-kernel frame of this brick and the point's canonical coordinates
     const double sp128 = p.spacing * AG_A_DIV;
-    const int ox = ((bx * NB_X) / FRAME_X) * FRAME_X, oy = ((by * NB_Y) / FRAME_Y) * FRAME_Y,
-              oz = ((bz * NB_Z) / FRAME_Z) * FRAME_Z;
+    const int ox = ((bx * BX) / FRAME_X) * FRAME_X, oy = ((by * BY) / FRAME_Y) * FRAME_Y,
+              oz = ((bz * BZ) / FRAME_Z) * FRAME_Z;
     const double X0 = frame_origin_bins(ox, p.nex, sp128), Y0 = frame_origin_bins(oy, p.ney, sp128),
                  Z0 = frame_origin_bins(oz, p.nez, sp128);
     const float PX = frame_point_coord(ix - ox, sp128), PY = frame_point_coord(iy - oy, sp128),
@@ -298,9 +292,9 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
 
     // candidate cells: brick bounding box grown by the candidate radius
     const double rc = AGB_NEAR_RADIUS;
-    const double bx0 = (double)(bx * NB_X - p.nex) * p.spacing, bx1 = (double)(min(bx * NB_X + NB_X - 1, p.n1x - 1) - p.nex) * p.spacing;
-    const double by0 = (double)(by * NB_Y - p.ney) * p.spacing, by1 = (double)(min(by * NB_Y + NB_Y - 1, p.n1y - 1) - p.ney) * p.spacing;
-    const double bz0 = (double)(bz * NB_Z - p.nez) * p.spacing, bz1 = (double)(min(bz * NB_Z + NB_Z - 1, p.n1z - 1) - p.nez) * p.spacing;
+    const double bx0 = (double)(bx * BX - p.nex) * p.spacing, bx1 = (double)(min(bx * BX + BX - 1, p.n1x - 1) - p.nex) * p.spacing;
+    const double by0 = (double)(by * BY - p.ney) * p.spacing, by1 = (double)(min(by * BY + BY - 1, p.n1y - 1) - p.ney) * p.spacing;
+    const double bz0 = (double)(bz * BZ - p.nez) * p.spacing, bz1 = (double)(min(bz * BZ + BZ - 1, p.n1z - 1) - p.nez) * p.spacing;
     auto cell_lo = [&](double v, double o, int n) { int c = (int)floor((v - rc - o) / p.cell_size); return max(0, min(n - 1, c)); };
     auto cell_hi = [&](double v, double o, int n) { int c = (int)floor((v + rc - o) / p.cell_size); return max(0, min(n - 1, c)); };
     const int cxl = cell_lo(bx0, p.cell0[0], p.ncx), cxh = cell_hi(bx1, p.cell0[0], p.ncx);
@@ -314,14 +308,14 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
         for (int i = tid; i < nc; i += NB_THREADS) {
             const int c = c0 + i;
             int s = 0;
-            while (s_seg_off[s + 1] <= c) s++;
-            const int a = p.cell_atoms[s_seg_start[s] + (c - s_seg_off[s])];
-            s_idx[i] = a;
-            s_pos[i] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0), frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
+            while (S.seg_off[s + 1] <= c) s++;
+            const int a = p.cell_atoms[S.seg_start[s] + (c - S.seg_off[s])];
+            S.idx[i] = a;
+            S.pos[i] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0), frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
                                    frame_atom_coord(p.z[a] * AG_A_DIV, Z0), (float)p.q[a]);
-            s_a[i] = atomA[a];
-            s_b[i] = atomB[a];
-            s_meta[i] = atom_meta[a];
+            S.a[i] = ptr.atomA[a];
+            S.b[i] = ptr.atomB[a];
+            S.meta[i] = ptr.meta[a];
         }
     };
     auto layout_segments = [&](int sb, int nseg) {
@@ -332,12 +326,12 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
                 const int cyy = cyl + k % nrow_y, czz = czl + k / nrow_y;
                 const int c0 = (czz * p.ncy + cyy) * p.ncx + cxl, c1 = (czz * p.ncy + cyy) * p.ncx + cxh;
                 const int st = p.cell_start[c0], en = p.cell_start[c1 + 1];
-                s_seg_start[s] = st;
-                s_seg_off[s] = off;
+                S.seg_start[s] = st;
+                S.seg_off[s] = off;
                 off += en - st;
             }
-            s_seg_off[nseg] = off;
-            s_total = off;
+            S.seg_off[nseg] = off;
+            S.total = off;
         }
     };
     // the candidate list fits one chunk in the common case: stage it once
@@ -346,31 +340,36 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
         __syncthreads();
         layout_segments(0, nseg_total);
         __syncthreads();
-        if (s_total <= NB_CHUNK) {
-            stage(0, s_total);
+        if (S.total <= NB_CHUNK) {
+            stage(0, S.total);
             resident = true;
         }
         __syncthreads();
     }
-    // visit every candidate chunk: fn(nc) with the chunk staged in shared memory
+    // visit every candidate chunk: fn(nc) with the chunk staged in shared memory.
+    // One call site for fn, so its body is instantiated once.
     auto for_each_chunk = [&](auto &&fn) {
-        if (resident) { fn(s_total); return; }
-        for (int sb = 0; sb < nseg_total; sb += NB_SEGS) {
-            const int nseg = min(NB_SEGS, nseg_total - sb);
-            __syncthreads();
-            layout_segments(sb, nseg);
-            __syncthreads();
-            const int total = s_total;
+        const int nsb = resident ? 1 : (nseg_total + NB_SEGS - 1) / NB_SEGS;
+        for (int sbi = 0; sbi < nsb; sbi++) {
+            int total = S.total;
+            if (!resident) {
+                const int sb = sbi * NB_SEGS;
+                __syncthreads();
+                layout_segments(sb, min(NB_SEGS, nseg_total - sb));
+                __syncthreads();
+                total = S.total;
+            }
             for (int c0 = 0; c0 < total; c0 += NB_CHUNK) {
                 const int nc = min(NB_CHUNK, total - c0);
-                __syncthreads();
-                stage(c0, nc);
-                __syncthreads();
+                if (!resident) {
+                    __syncthreads();
+                    stage(c0, nc);
+                    __syncthreads();
+                }
                 fn(nc);
             }
         }
     };
-
     // ---- A: closest DS/D1 hydrogen (main.cpp:2986-3015)
     int ch = -1;
     if (need_h) {
@@ -378,9 +377,9 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
         for_each_chunk([&](int nc) {
             if (!valid) return;
             for (int j = 0; j < nc; j++) {
-                const int hb = (s_meta[j] >> META_HB_SHIFT) & 7;
+                const int hb = (S.meta[j] >> META_HB_SHIFT) & 7;
                 if (hb != 1 && hb != 2) continue;
-                const float4 A = s_pos[j];
+                const float4 A = S.pos[j];
                 const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
                 best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
             }
@@ -390,12 +389,12 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
         for_each_chunk([&](int nc) {
             if (!valid) return;
             for (int j = 0; j < nc; j++) {
-                const int hb = (s_meta[j] >> META_HB_SHIFT) & 7;
+                const int hb = (S.meta[j] >> META_HB_SHIFT) & 7;
                 if (hb != 1 && hb != 2) continue;
-                const float4 A = s_pos[j];
+                const float4 A = S.pos[j];
                 const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
                 if (dx * dx + dy * dy + dz * dz > lim) continue;
-                const int a = s_idx[j];
+                const int a = S.idx[j];
                 const double r = h_dist(p, a, cx, cy, cz);
                 if (r < rmin || (r == rmin && a < ch)) { rmin = r; ch = a; }
             }
@@ -411,7 +410,7 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
         }
     }
     float3 rvh = make_float3(0.f, 0.f, 0.f);
-    if (!EXACT && ch >= 0) rvh = make_float3(atomA[ch].x, atomA[ch].y, atomA[ch].z);
+    if (!EXACT && ch >= 0) rvh = make_float3(ptr.atomA[ch].x, ptr.atomA[ch].y, ptr.atomA[ch].z);
 
     // ---- B: pair terms
     R E[NG_MAX], hmin[NG_MM], hmax[NG_MM];
@@ -426,8 +425,8 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
         for_each_chunk([&](int nc) {
             if (!valid) return;
             for (int j = 0; j < nc; j++) {
-                const int ia = s_idx[j];
-                const int meta = s_meta[j];
+                const int ia = S.idx[j];
+                const int meta = S.meta[j];
                 PairQ<R> q;
                 bool e_pair = false;
                 if (EXACT) {
@@ -440,7 +439,7 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
                     q.ad4_in = 1; q.bin = qd.bin; q.bin_e = qd.bin_e; q.ih = qd.ih;
                     q.r = (R)qd.r; q.inv_rmax = (R)qd.inv_rmax; q.racc = (R)qd.racc; q.rdon = (R)qd.rdon; q.Hramp = (R)qd.Hramp;
                 } else {
-                    const float4 A = s_pos[j];
+                    const float4 A = S.pos[j];
                     const float dY = __fsub_rn(A.y, PY), dZ = __fsub_rn(A.z, PZ);
                     const float s = __fmaf_rn(dY, dY, __fmaf_rn(dZ, dZ, TINY_T2));
                     const float dX = __fsub_rn(A.x, PX);
@@ -450,7 +449,7 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
                     if (t >= FAR_T0 + GUARD_BIN) continue;
                     e_pair = t < FAR_T0;  // the far-field kernel skips exactly these pairs
                     PairQ<float> qf;
-                    if (!pair_fast(meta, s_a[j], s_b[j], ia, dX, dY, dZ, t, rs, ch, rvh, qf)) {
+                    if (!pair_fast(meta, S.a[j], S.b[j], ia, dX, dY, dZ, t, rs, ch, rvh, qf)) {
                         PairQ<double> qd;
                         pair_exact(p, ia, cx, cy, cz, ch, qd);
                         qf.ad4_in = qd.ad4_in; qf.bin = qd.bin; qf.bin_e = qd.bin_e; qf.ih = qd.ih;
@@ -460,23 +459,27 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
                     }
                     q.ad4_in = qf.ad4_in; q.bin = qf.bin; q.bin_e = qf.bin_e; q.ih = qf.ih;
                     q.r = qf.r; q.inv_rmax = qf.inv_rmax; q.racc = qf.racc; q.rdon = qf.rdon; q.Hramp = qf.Hramp;
-                    if (e_pair && do_e) e_near += (R)(s_etab[min(q.bin_e, NT_SMALL - 1)] * A.w) * q.inv_rmax;
+                    if (e_pair && do_e) e_near += (R)(S.etab[min(q.bin_e, NT_SMALL - 1)] * A.w) * q.inv_rmax;
                     if (!q.ad4_in) continue;
                 }
                 n_near++;
                 const int kr = min(q.bin, NT_SMALL - 1);
-                const R sol = EXACT ? (R)p.sol_fn[kr] : (R)s_sol[kr];
-                const float4 rA = s_a[j], rB = s_b[j];
-                D1 += (R)rA.w * sol;  // vol
-                D2 += (R)rB.w * sol;  // solpar + qasp|q|
+                const R sol = EXACT ? (R)p.sol_fn[kr] : (R)S.sol[kr];
+                if (EXACT) {
+                    D1 += (R)p.vol[ia] * sol;
+                    D2 += (R)(p.solpar[ia] + p.solpar_q * fabs(p.q[ia])) * sol;
+                } else {
+                    D1 += (R)S.a[j].w * sol;  // vol
+                    D2 += (R)S.b[j].w * sol;  // solpar + qasp|q|
+                }
                 if (g.ng == 0) continue;
                 const int hb = (meta >> META_HB_SHIFT) & 7;
                 const bool dis = (meta & META_DIS) != 0;
                 const int ta = meta & META_TYPE_MASK;
                 const int kn = min(q.bin, AG_NEINT - 1);
-                const float4 *Trow = (const float4 *)(vdwT + ((size_t)ta * AG_NEINT + kn) * mpad + g.col0);
+                const float4 *Trow = (const float4 *)(ptr.vdwT + ((size_t)ta * AG_NEINT + kn) * ptr.mpad + g.col0);
                 const float4 *Hrow = (g.has_hrow && dis && p.hydrogen_type >= 0)
-                    ? (const float4 *)(vdwT + ((size_t)p.hydrogen_type * AG_NEINT + q.ih) * mpad + g.col0) : Trow;
+                    ? (const float4 *)(ptr.vdwT + ((size_t)p.hydrogen_type * AG_NEINT + q.ih) * ptr.mpad + g.col0) : Trow;
                 const unsigned long long aw = g.actw[hb];
 #pragma unroll
                 for (int m4 = 0; m4 < NG_MAX / 4; m4++) {
@@ -524,32 +527,74 @@ k_near(DevProblem p, NearGroup g, const float4 *__restrict__ atomA, const float4
             v += (R)g.sp[m] * D1 + (R)g.vp[m] * D2;
             const size_t o = (size_t)g.out_map[m] * (size_t)p.P + (size_t)lin;
             if (g.cov[m]) {
-                if (EXACT) out64[o] = cov_map[lin]; else out32[o] = (float)cov_map[lin];
+                if (EXACT) ptr.out64[o] = ptr.cov_map[lin]; else ptr.out32[o] = (float)ptr.cov_map[lin];
             } else {
-                if (EXACT) out64[o] = (double)v; else out32[o] = (float)v;
+                if (EXACT) ptr.out64[o] = (double)v; else ptr.out32[o] = (float)v;
             }
         }
         if (g.write_special) {
             if (p.dsolv_map >= 0) {
                 const size_t o = (size_t)p.dsolv_map * (size_t)p.P + (size_t)lin;
                 const R d = (R)p.solpar_q * D1;
-                if (EXACT) out64[o] = (double)d; else out32[o] = (float)d;
+                if (EXACT) ptr.out64[o] = (double)d; else ptr.out32[o] = (float)d;
             }
             if (do_e) {
                 float e = 0.f;
                 for (int c = 0; c < p.far_chunks; c++) e += p.far_partial[(size_t)c * (size_t)p.P + (size_t)lin];
-                out32[(size_t)p.elec_map * (size_t)p.P + (size_t)lin] = e + (float)e_near;
+                ptr.out32[(size_t)p.elec_map * (size_t)p.P + (size_t)lin] = e + (float)e_near;
             }
         }
     }
-    if (counters) {
-        atomicAdd(&s_cnt[0], n_near);
-        atomicAdd(&s_cnt[1], n_fb);
+    if (ptr.counters) {
+        atomicAdd(&S.cnt[0], n_near);
+        atomicAdd(&S.cnt[1], n_fb);
         __syncthreads();
         if (tid == 0) {
-            atomicAdd(counters + 0, s_cnt[0]);
-            atomicAdd(counters + 1, s_cnt[1]);
+            atomicAdd(ptr.counters + 0, S.cnt[0]);
+            atomicAdd(ptr.counters + 1, S.cnt[1]);
         }
+    }
+}
+
+// Single instance: one CTA per brick.
+template <bool EXACT, int BX, int BY, int BZ>
+__global__ void __launch_bounds__(NB_THREADS, 2) k_near(DevProblem p, NearGroup g, NearPtrs ptr)
+{
+    __shared__ NearSmem S;
+    near_unit<EXACT, BX, BY, BZ>(p, g, ptr, blockIdx.x, S);
+}
+
+// Many instances, persistent: (instance-group, brick) units from an atomic
+// counter; units never wait on each other.
+template <int BX, int BY, int BZ>
+__global__ void __launch_bounds__(NB_THREADS, 2)
+k_near_batch(const NearInst *__restrict__ insts, const long long *__restrict__ unit_begin, int n_inst,
+             unsigned long long *__restrict__ counter)
+{
+    __shared__ NearSmem S;
+    __shared__ NearInst s_i;
+    __shared__ long long s_unit;
+    int cur = -1;
+    const long long total = unit_begin[n_inst];
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_unit = (long long)atomicAdd(counter, 1ull);
+        __syncthreads();
+        const long long u = s_unit;
+        if (u >= total) break;
+        int lo = 0, hi = n_inst - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (unit_begin[mid] <= u) lo = mid; else hi = mid - 1;
+        }
+        if (lo != cur) {
+            __syncthreads();
+            for (int i = threadIdx.x; i < (int)(sizeof(NearInst) / 4); i += NB_THREADS)
+                ((int *)&s_i)[i] = ((const int *)&insts[lo])[i];
+            __syncthreads();
+            cur = lo;
+        }
+        near_unit<false, BX, BY, BZ>(s_i.p, s_i.g, s_i.ptr, (int)(u - unit_begin[lo]), S);
     }
 }
 
@@ -572,9 +617,12 @@ __global__ void k_covalent(DevProblem p, double *__restrict__ cov)
 
 namespace agb {
 
-static unsigned near_blocks(const DevProblem &p)
+int near_bricks(const DevProblem &p, int shape)
 {
-    return (unsigned)(((p.n1x + NB_X - 1) / NB_X) * ((p.n1y + NB_Y - 1) / NB_Y) * ((p.n1z + NB_Z - 1) / NB_Z));
+    int bx = 8, by = 8, bz = 4;
+    if (shape == 1) { by = 4; bz = 8; }
+    else if (shape == 2) { bx = 4; bz = 8; }
+    return ((p.n1x + bx - 1) / bx) * ((p.n1y + by - 1) / by) * ((p.n1z + bz - 1) / bz);
 }
 
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s)
@@ -583,18 +631,41 @@ cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s)
     return cudaGetLastError();
 }
 
-cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const float4 *atomA,
-                        const float4 *atomB, const int *meta, const float *vdwT, int mpad, const float *etab,
-                        const float *solf, const double *cov_map, float *out32, double *out64,
-                        unsigned long long *counters, cudaStream_t s)
+cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int shape,
+                        cudaStream_t s)
 {
-    if (exact)
-        k_near<true><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, atomA, atomB, meta, vdwT, mpad, etab, solf, cov_map,
-                                                         out32, out64, counters);
-    else
-        k_near<false><<<near_blocks(p), NB_THREADS, 0, s>>>(p, g, atomA, atomB, meta, vdwT, mpad, etab, solf,
-                                                          cov_map, out32, out64, counters);
+    const unsigned nb = (unsigned)near_bricks(p, shape);
+    if (exact) {
+        k_near<true, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+    } else if (shape == 1) {
+        k_near<false, 8, 4, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+    } else if (shape == 2) {
+        k_near<false, 4, 8, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+    } else {
+        k_near<false, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+    }
     return cudaGetLastError();
+}
+
+template <int BX, int BY, int BZ>
+static cudaError_t near_batch_t(const NearInst *insts, const long long *unit_begin, int n_inst,
+                                unsigned long long *counter, int ctas_per_sm, cudaStream_t s)
+{
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_near_batch<BX, BY, BZ>, NB_THREADS, 0);
+    const int per_sm = std::max(1, std::min(ctas_per_sm, occ));
+    k_near_batch<BX, BY, BZ><<<sms * per_sm, NB_THREADS, 0, s>>>(insts, unit_begin, n_inst, counter);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_near_batch(const NearInst *insts, const long long *unit_begin, int n_inst,
+                              unsigned long long *counter, int shape, int ctas_per_sm, cudaStream_t s)
+{
+    if (shape == 1) return near_batch_t<8, 4, 8>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+    if (shape == 2) return near_batch_t<4, 8, 8>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+    return near_batch_t<8, 8, 4>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
 }
 
 }  // namespace agb

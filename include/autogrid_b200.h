@@ -213,6 +213,36 @@ ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, const double 
                                   int32_t dddiel, const double *d_r_epsilon_fn, double invdielcal,
                                   double coeff_estat, float *d_emap, void *stream);
 
+/*
+ * Batched ensemble: many independent receptor/box instances (uneven atom
+ * counts and grids) computed by one persistent launch per kernel kind, each
+ * CTA taking (instance, tile) work units from an atomic counter.  The kernel
+ * sequence is captured once in a CUDA graph.  ag_batch_create() also runs the
+ * autotuner: it times the far-field atom-tile size and chunking and the
+ * near-field brick shape on this batch and keeps the fastest.  No counterpart
+ * in the reference, which computes one box per process.  FP32 path only.
+ */
+typedef struct ag_batch ag_batch;
+typedef struct ag_tuning {
+    int32_t far_tile;         /* atoms per shared-memory tile (256, 512, 1024)     */
+    int32_t far_chunked;      /* 1: atoms split in 2048-atom chunks per unit       */
+    int32_t near_shape;       /* 0: 8x8x4, 1: 8x4x8, 2: 4x8x8 points per brick     */
+    int32_t candidates;       /* configurations timed                             */
+    double  far_ms, near_ms;  /* device time of the chosen far / near launches    */
+    double  far_ms_default, near_ms_default;  /* same with the untuned defaults   */
+} ag_tuning;
+ag_status    ag_batch_create(ag_context *ctx, const ag_problem *const *problems, int32_t n,
+                             const ag_opts *opts, ag_batch **out);
+ag_status    ag_batch_run(ag_batch *batch, void *stream);
+const float *ag_batch_device_maps(const ag_batch *batch, int32_t i);
+ag_status    ag_batch_download(ag_batch *batch, int32_t i, float *host_maps);
+ag_status    ag_batch_tuning(const ag_batch *batch, ag_tuning *out);
+ag_status    ag_batch_destroy(ag_batch *batch);
+/* One-shot: create, run, download every instance's maps (maps[i] host or
+ * device, [n_maps_i][P_i] each), destroy. */
+ag_status    ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *problems, int32_t n,
+                                   const ag_opts *opts, float *const *maps);
+
 /* Front / back end (replaces main.cpp:214-2776 and :3481-3565) ------------- */
 typedef struct ag_job ag_job;
 
