@@ -184,3 +184,42 @@ def workload(name: str, seed: int = 0) -> tuple:
     w = WORKLOADS[name]
     rec = make_receptor(w["n_atoms"], seed=seed, radius=w["radius"], center=(11.125, -4.5, 7.25))
     return rec, w["spec"]
+
+
+# ----------------------------------------------------------------- ensembles --
+ENSEMBLE_LIGANDS = list(LIGAND_TYPES_8)
+
+
+def ensemble_specs(n: int, seed: int, atoms_range=(1000, 12000), npts_range=(20, 100)) -> list:
+    """(n_atoms, npts) of each instance of a batched ensemble: atom counts
+    log-uniform over atoms_range, per-axis npts uniform over npts_range
+    (independently per axis; odd values are truncated to even by the GPF
+    reader, as check_size.cpp:79-83 does)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(atoms_range[0]), np.log(atoms_range[1])
+    out = []
+    for _ in range(n):
+        na = int(round(float(np.exp(rng.uniform(lo, hi)))))
+        npts = tuple(int(v) for v in rng.integers(npts_range[0], npts_range[1] + 1, 3))
+        out.append((na, npts))
+    return out
+
+
+def _write_instance(args):
+    directory, i, na, npts, seed = args
+    rec = make_receptor(na, seed=seed, center=(0.0, 0.0, 0.0))
+    spec = GridSpec(npts=npts, ligand_types=list(ENSEMBLE_LIGANDS))
+    return str(write_case(directory, f"inst{i:04d}", rec, spec))
+
+
+def write_ensemble(directory, n: int, seed: int = 0, workers: int | None = None, **kw) -> list:
+    """Write n instances (PDBQT + GPF) in parallel; returns the GPF paths."""
+    import multiprocessing as mp
+    import os
+    specs = ensemble_specs(n, seed, **kw)
+    jobs = [(str(directory), i, na, npts, seed * 100003 + i) for i, (na, npts) in enumerate(specs)]
+    workers = workers or min(16, os.cpu_count() or 1)
+    if workers <= 1 or n < 4:
+        return [_write_instance(j) for j in jobs]
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(_write_instance, jobs)

@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble comparison")
+    ap.add_argument("--batch-instances", type=int, default=256)
     return ap.parse_args()
 
 
@@ -249,6 +251,8 @@ def main():
             "clocks": clk,
             "diagnostics": {"near_pairs_per_step": st.near_pairs, "fp64_fallbacks_per_step": st.fp64_fallbacks},
         }
+        if not args.no_batch and world == 1:
+            line["batched"] = batched_ensemble(ctx, args.batch_instances, work, stream)
         if not args.no_cpu_baseline and world == 1:
             threads = min(32, os.cpu_count() or 1)
             res = reference_sample(rec, spec, work, threads)
@@ -262,6 +266,65 @@ def main():
     if world > 1:
         dist.destroy_process_group()
     shutil.rmtree(work, ignore_errors=True)
+
+
+def batched_ensemble(ctx, n, work: Path, stream):
+    """The batched form: n uneven instances (atoms log-uniform 1,000-12,000,
+    per-axis npts uniform 20-100, spacing 0.375 A, 8 maps) in one persistent,
+    graph-captured launch per kernel kind, against the plain per-box path
+    (one device-resident plan per instance, run one after another)."""
+    import torch
+    from autogrid_b200 import Batch, Job, synth
+    d = work / "ensemble"
+    gpfs = synth.write_ensemble(d, n, seed=2024)
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        probs = [Job(os.path.basename(g), None).problem() for g in gpfs]
+    finally:
+        os.chdir(cwd)
+    evals = sum(p.points * p.n_maps for p in probs)
+    pairs = sum(p.points * p.n_atoms for p in probs)
+    t0 = time.perf_counter()
+    b = Batch(ctx, probs)
+    create_s = time.perf_counter() - t0
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn, reps):
+        out = []
+        for _ in range(reps):
+            flush.zero_()
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            fn()
+            e_.record(stream)
+            torch.cuda.synchronize()
+            out.append(s_.elapsed_time(e_))
+        return float(np.mean(out))
+
+    b.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    batch_ms = timed(lambda: b.run(stream.cuda_stream), 5)
+    plans = [ctx.plan(p) for p in probs]
+    for pl in plans:
+        pl.run(stream.cuda_stream)
+    torch.cuda.synchronize()
+    plain_ms = timed(lambda: [pl.run(stream.cuda_stream) for pl in plans], 3)
+    # same maps from both paths
+    worst = 0.0
+    for i in range(0, n, max(1, n // 16)):
+        a = b.download(i)
+        c = plans[i].download()
+        worst = max(worst, float(np.max(np.abs(a - c) / np.maximum(1e-3, 1e-4 * np.abs(c)))))
+    for pl in plans:
+        pl.close()
+    tune = b.tuning()
+    b.close()
+    return {"instances": n, "points": int(sum(p.points for p in probs)), "pair_terms": int(pairs),
+            "evals_per_s": evals / (batch_ms * 1e-3), "ms_per_ensemble": batch_ms,
+            "plain_per_box_ms": plain_ms, "plain_per_box_evals_per_s": evals / (plain_ms * 1e-3),
+            "speedup_vs_plain_per_box": plain_ms / batch_ms, "max_diff_over_tolerance": worst,
+            "create_s": create_s, "tuning": tune}
 
 
 def far_kernel_ms(ctx, plan, stream, steps):
