@@ -584,6 +584,16 @@ ag_status batch_launch(ag_batch *b, cudaStream_t s, int tile, int shape, cudaEve
     return AG_OK;
 }
 
+// Near work units (bricks) of every instance-group for one brick shape.
+ag_status batch_set_near_shape(ag_batch *b, int shape)
+{
+    b->near_begin.assign(1, 0);
+    for (const NearInst &ni : b->near) b->near_begin.push_back(b->near_begin.back() + near_bricks(ni.p, shape));
+    AGB_CK(cudaMemcpyAsync(b->d_near_begin, b->near_begin.data(), sizeof(long long) * b->near_begin.size(),
+                           cudaMemcpyHostToDevice, b->ctx->stream));
+    return AG_OK;
+}
+
 // Time one configuration (best of two runs).
 ag_status batch_time(ag_batch *b, int tile, int shape, double *far_ms, double *near_ms)
 {
@@ -633,6 +643,8 @@ ag_status batch_autotune(ag_batch *b)
     if (st != AG_OK) return st;
     for (int shape = 0; shape < 3; shape++) {
         double f = 0, n = 0;
+        st = batch_set_near_shape(b, shape);
+        if (st != AG_OK) return st;
         st = batch_time(b, best_tile, shape, &f, &n);
         if (st != AG_OK) return st;
         t.candidates++;
@@ -862,16 +874,13 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     AGB_CK(b->bufs.ensure("counters", 4 * sizeof(unsigned long long), &v));
     b->d_counters = (unsigned long long *)v;
     if (b->far.empty()) b->far_begin.assign(1, 0);
-    // near units are counted per brick of the tuned shape: refresh after tuning
-    ag_status st = batch_autotune(b.get());
+    ag_status st = batch_set_near_shape(b.get(), 0);
+    if (st != AG_OK) return st;
+    st = batch_autotune(b.get());
     if (st != AG_OK) return st;
     // final near unit table for the chosen shape
-    {
-        b->near_begin.assign(1, 0);
-        for (const NearInst &ni : b->near) b->near_begin.push_back(b->near_begin.back() + near_bricks(ni.p, b->tune.near_shape));
-        AGB_CK(cudaMemcpyAsync(b->d_near_begin, b->near_begin.data(), sizeof(long long) * b->near_begin.size(),
-                               cudaMemcpyHostToDevice, ctx->stream));
-    }
+    st = batch_set_near_shape(b.get(), b->tune.near_shape);
+    if (st != AG_OK) return st;
     // capture the run as a graph on a private stream
     cudaStream_t cs;
     AGB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
