@@ -58,7 +58,8 @@ class ag_problem(C.Structure):
 
 
 class ag_opts(C.Structure):
-    _fields_ = [("precision", C.c_int32), ("table_mode", C.c_int32), ("reserved", C.c_int32 * 6)]
+    _fields_ = [("precision", C.c_int32), ("table_mode", C.c_int32), ("autotune", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
 
 
 class ag_stats(C.Structure):

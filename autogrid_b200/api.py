@@ -264,15 +264,15 @@ class Plan:
 
 class Batch:
     """Many independent problems computed by one persistent launch per kernel
-    kind, graph-captured and autotuned at creation (ag_batch)."""
+    kind, graph-captured, and (by default) autotuned at creation (ag_batch)."""
 
-    def __init__(self, ctx: Context, problems: list):
+    def __init__(self, ctx: Context, problems: list, autotune: bool = True):
         self.ctx = ctx
         self.problems = list(problems)
         self._lib = ctx._lib
         self._structs = [p.struct() for p in self.problems]
         arr = (C.POINTER(ag_problem) * len(self._structs))(*[C.pointer(s) for s in self._structs])
-        opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST)
+        opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST, autotune=int(autotune))
         h = C.c_void_p()
         check(self._lib.ag_batch_create(ctx._h, arr, len(self.problems), C.byref(opts), C.byref(h)))
         self._h = h
@@ -301,6 +301,18 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def compute_batch(ctx: Context, problems: list) -> list:
+    """One-shot batched computation (ag_maps_compute_batch): host inputs in,
+    host maps out, no autotuning."""
+    structs = [p.struct() for p in problems]
+    arr = (C.POINTER(ag_problem) * len(structs))(*[C.pointer(s) for s in structs])
+    outs = [np.empty(p.map_shape, dtype=np.float32) for p in problems]
+    ptrs = (C.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+    opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST)
+    check(ctx._lib.ag_maps_compute_batch(ctx._h, arr, len(problems), C.byref(opts), ptrs))
+    return outs
 
 
 def run_gpf(gpf: str, glg: str | None = None, precision: str = "fp32", device: int = 0) -> np.ndarray:

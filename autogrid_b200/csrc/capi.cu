@@ -876,8 +876,16 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     if (b->far.empty()) b->far_begin.assign(1, 0);
     ag_status st = batch_set_near_shape(b.get(), 0);
     if (st != AG_OK) return st;
-    st = batch_autotune(b.get());
-    if (st != AG_OK) return st;
+    if (o.autotune) {
+        st = batch_autotune(b.get());
+        if (st != AG_OK) return st;
+    } else {
+        st = batch_upload_far(b.get(), false);
+        if (st != AG_OK) return st;
+        b->tune = ag_tuning{};
+        b->tune.far_tile = 512;
+        b->tune.near_shape = 0;
+    }
     // final near unit table for the chosen shape
     st = batch_set_near_shape(b.get(), b->tune.near_shape);
     if (st != AG_OK) return st;

@@ -320,7 +320,22 @@ def batched_ensemble(ctx, n, work: Path, stream):
         pl.close()
     tune = b.tuning()
     b.close()
+    # end to end through the public calls, host inputs and host maps: the
+    # drop-in ag_maps_compute per box vs one ag_maps_compute_batch call
+    from autogrid_b200.api import compute_batch
+    outs = [np.empty(p.map_shape, dtype=np.float32) for p in probs]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for p, o in zip(probs, outs):
+        ctx.compute(p, "fp32", out=o)
+    e2e_plain_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    compute_batch(ctx, probs)
+    e2e_batch_s = time.perf_counter() - t0
     return {"instances": n, "points": int(sum(p.points for p in probs)), "pair_terms": int(pairs),
+            "e2e_plain_per_box_s": e2e_plain_s, "e2e_batch_s": e2e_batch_s,
+            "e2e_speedup_vs_plain_per_box": e2e_plain_s / e2e_batch_s,
             "evals_per_s": evals / (batch_ms * 1e-3), "ms_per_ensemble": batch_ms,
             "plain_per_box_ms": plain_ms, "plain_per_box_evals_per_s": evals / (plain_ms * 1e-3),
             "speedup_vs_plain_per_box": plain_ms / batch_ms, "max_diff_over_tolerance": worst,

@@ -129,7 +129,9 @@ enum { AG_TABLE_NEAREST = 0 }; /* reference nearest-bin tables (drop-in)       *
 typedef struct ag_opts {
     int32_t precision;   /* AG_PREC_*                                          */
     int32_t table_mode;  /* AG_TABLE_*                                         */
-    int32_t reserved[6]; /* zero                                               */
+    int32_t autotune;    /* batches: 1 = time tile/brick shapes at creation,   */
+                         /* 0 = use the defaults                               */
+    int32_t reserved[5]; /* zero                                               */
 } ag_opts;
 
 /* Diagnostics of the last compute or plan run on a context (FP32 path);
@@ -217,9 +219,10 @@ ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, const double 
  * Batched ensemble: many independent receptor/box instances (uneven atom
  * counts and grids) computed by one persistent launch per kernel kind, each
  * CTA taking (instance, tile) work units from an atomic counter.  The kernel
- * sequence is captured once in a CUDA graph.  ag_batch_create() also runs the
- * autotuner: it times the far-field atom-tile size and chunking and the
- * near-field brick shape on this batch and keeps the fastest.  No counterpart
+ * sequence is captured once in a CUDA graph.  With opts->autotune set,
+ * ag_batch_create() also runs the autotuner: it times the far-field atom-tile
+ * size and chunking and the near-field brick shape on this batch and keeps
+ * the fastest.  No counterpart
  * in the reference, which computes one box per process.  FP32 path only.
  */
 typedef struct ag_batch ag_batch;
