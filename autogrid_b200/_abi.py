@@ -104,6 +104,8 @@ SIGNATURES = {
     "ag_job_write_maps_f64": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ag_job_fail": (None, [C.c_void_p, C.c_char_p]),
     "ag_job_free": (None, [C.c_void_p]),
+    "ag_job_bond_vectors": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_job_bond_vectors_backward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_emap_compute_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
                                           C.c_double, C.c_int32, C.c_void_p, C.c_double, C.c_double,
                                           C.c_void_p, C.c_void_p]),

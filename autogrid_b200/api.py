@@ -157,6 +157,28 @@ class Job:
             m = np.ascontiguousarray(m, dtype=np.float32)
             check(self._lib.ag_job_write_maps_f32(self._h, m.ctypes.data_as(C.c_void_p)))
 
+    def bond_vectors(self, coord: np.ndarray | None = None) -> tuple:
+        """(rvector, rvector2) [N,3] at coord [N,3] (centred frame), with the
+        bonded neighbours found at load time (ag_job_bond_vectors)."""
+        n = self.problem().n_atoms
+        rv = np.zeros((n, 3)); rv2 = np.zeros((n, 3))
+        c = None if coord is None else np.ascontiguousarray(coord, dtype=np.float64).reshape(n, 3)
+        check(self._lib.ag_job_bond_vectors(self._h, None if c is None else c.ctypes.data_as(C.c_void_p),
+                                            rv.ctypes.data_as(C.c_void_p), rv2.ctypes.data_as(C.c_void_p)))
+        return rv, rv2
+
+    def bond_vectors_backward(self, coord, g_rvector, g_rvector2) -> np.ndarray:
+        """d(rvector, rvector2)/d(coord)^T (g_rvector, g_rvector2), [N,3] FP64."""
+        n = self.problem().n_atoms
+        c = np.ascontiguousarray(coord, dtype=np.float64).reshape(n, 3)
+        g1 = np.ascontiguousarray(g_rvector, dtype=np.float64).reshape(n, 3)
+        g2 = np.ascontiguousarray(g_rvector2, dtype=np.float64).reshape(n, 3)
+        out = np.zeros((n, 3))
+        check(self._lib.ag_job_bond_vectors_backward(self._h, c.ctypes.data_as(C.c_void_p),
+                                                     g1.ctypes.data_as(C.c_void_p), g2.ctypes.data_as(C.c_void_p),
+                                                     out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def fail(self, message: str) -> None:
         self._lib.ag_job_fail(self._h, message.encode())
 

@@ -137,6 +137,14 @@ bool distance_le(const double a[3], const double b[3], double limit, double dc[3
     return d <= limit;
 }
 
+// Which neighbours define a directional atom's bond vectors (main.cpp:2320-2656).
+struct BondRec {
+    enum Kind { NONE = 0, D1, A2_ONE, A2_DIS, A2_TWO, A1 };
+    int kind = NONE;
+    int i1 = -1, i2 = -1;  // D1: parent; A2_ONE: bonded atom, its last neighbour; A2_DIS: carbon; A2_TWO: both
+    int nb = 0, nbr[3] = {-1, -1, -1};  // A1: bonded atoms
+};
+
 struct MapObj {  // main.cpp:289-315
     int atom_type = 0, map_index = 0, is_covalent = 0, is_hbonder = 0;
     std::string filename, type;
@@ -180,6 +188,7 @@ struct Job {
     std::vector<uint8_t> disorder;
     std::vector<int> nbonds;
     std::vector<std::array<int, kMaxNBonds>> bonded;
+    std::vector<BondRec> bondrec;
     std::vector<std::string> receptor_types;  // by rec index
     int receptor_types_ct = 0, receptor_types_gpf_ct = 0;
     bool has_receptor_types_in_gpf = false;
@@ -277,6 +286,8 @@ struct Job {
     void finish_setup();
     void build_tables();
     void build_bond_vectors();
+    void eval_bond_vectors(const double *xyz, double *rv, double *rv2) const;
+    void bond_vectors_backward(const double *xyz, const double *g_rv, const double *g_rv2, double *g_xyz) const;
     void build_disorder();
     void make_problem();
     void write_maps(const double *maps64, const float *maps32);
@@ -825,7 +836,10 @@ void Job::build_tables()
 }
 
 // ----------------------------------------------------------- bond vectors --
-// main.cpp:2297-2659
+// main.cpp:2297-2659.  Detection (which neighbours define each directional
+// atom's bond vectors) is recorded as a BondRec; eval_bond_vectors() then
+// computes rvector/rvector2 from coordinates, so the same topology can be
+// re-evaluated and differentiated at other coordinates.
 void Job::build_bond_vectors()
 {
     rvector.assign((size_t)3 * n_atoms, 0.0);
@@ -833,6 +847,7 @@ void Job::build_bond_vectors()
     disorder.assign(n_atoms, 0);
     nbonds.assign(n_atoms, 0);
     bonded.assign(n_atoms, std::array<int, kMaxNBonds>{{0, 0, 0, 0}});
+    bondrec.assign(n_atoms, BondRec{});
     auto C = [&](int a) { return &coord[3 * (size_t)a]; };
     auto add_bond = [&](int i, int j) {  // bondmanager.cpp:44-88
         if (nbonds[i] >= kMaxNBonds || nbonds[j] >= kMaxNBonds)
@@ -842,14 +857,15 @@ void Job::build_bond_vectors()
     };
     for (int ia = 0; ia < n_atoms; ia++) {
         const int from = std::max(ia - 20, 0), to = std::min(ia + 20, n_atoms - 1);
-        double *rv = &rvector[3 * (size_t)ia], *rv2 = &rvector2[3 * (size_t)ia];
+        BondRec &br = bondrec[ia];
         if (hbond[ia] == 2) {  // D1 donor hydrogen, main.cpp:2320-2414
             for (int ib = from; ib <= to; ib++) {
                 if (ib == ia) continue;
                 double d[3], rd;
                 if (!distance_le(C(ia), C(ib), 1.378, d, rd)) continue;
-                for (int i = 0; i < 3; i++) rv[i] = d[i];
-                if (vect_normalize(rv) == 0.)
+                br.kind = BondRec::D1;  // the last bonded atom in the scan wins
+                br.i1 = ib;
+                if (vect_normalize(d) == 0.)
                     warn(fmt("While calculating an H-O or H-N bond vector...\nAttempt to divide by zero was just "
                              "prevented.\nAre the coordinates of atoms %d and %d the same?", ia + 1, ib + 1));
                 if (atom_type[ib] == nitrogen) rexp[ia] = 2;
@@ -871,16 +887,13 @@ void Job::build_bond_vectors()
             if (nbond == 0)
                 warn(fmt("Oxygen atom found with no bonded atoms, atom serial number %d, atom_type %d", ia + 1, atom_type[ia]));
             if (nbond == 1) {
-                vect_sub_normalize(rv, C(ia), C(i1));
+                br.kind = BondRec::A2_ONE;
+                br.i1 = i1;
                 for (int j2 = from; j2 <= to; j2++) {
                     if (j2 == i1 || j2 == ia) continue;
                     double d[3], rdcx;
                     if (!distance_le(C(i1), C(j2), atom_type[j2] == hydrogen ? 1.3 : 1.7, d, rdcx)) continue;
-                    vect_normalize(d);
-                    rv2[0] = rv[1] * d[2] - rv[2] * d[1];
-                    rv2[1] = rv[2] * d[0] - rv[0] * d[2];
-                    rv2[2] = rv[0] * d[1] - rv[1] * d[0];
-                    vect_normalize(rv2);
+                    br.i2 = j2;  // the last neighbour of i1 in the scan wins
                 }
             } else if (nbond == 2) {
                 if (disorder_h && (atom_type[i1] == hydrogen || atom_type[i2] == hydrogen) &&
@@ -890,30 +903,191 @@ void Job::build_bond_vectors()
                     else if (atom_type[i2] == carbon || atom_type[i2] == arom_carbon) ib = i2;
                     else ib = i1;
                     add_bond(ia, ib);
-                    vect_sub_normalize(rv, C(ia), C(ib));
+                    br.kind = BondRec::A2_DIS;
+                    br.i1 = ib;
                 } else {
-                    vect_sub_normalize(rv2, C(i2), C(i1));
-                    double rdot = 0.;
-                    for (int i = 0; i < 3; i++) rdot += (C(ia)[i] - C(i1)[i]) * rv2[i];
-                    for (int i = 0; i < 3; i++) rv[i] = C(ia)[i] - ((rdot * rv2[i]) + C(i1)[i]);
-                    vect_normalize(rv);
+                    br.kind = BondRec::A2_TWO;
+                    br.i1 = i1;
+                    br.i2 = i2;
                 }
             }
         } else if (hbond[ia] == 4) {  // A1 directional N acceptor, main.cpp:2596-2656
-            int nbond = 0;
-            double bondv[3][3], bondl[3];
+            br.kind = BondRec::A1;
+            br.nb = 0;
             for (int ib = from; ib <= to; ib++) {
                 if (ib == ia) continue;
                 const double lim = (atom_type[ib] == hydrogen || atom_type[ib] == nonHB_hydrogen) ? 1.3 : 1.7;
-                if (!distance_le(C(ia), C(ib), lim, bondv[nbond], bondl[nbond])) continue;
-                if (++nbond == 3) break;
+                double dc[3], rd;
+                if (!distance_le(C(ia), C(ib), lim, dc, rd)) continue;
+                br.nbr[br.nb] = ib;
+                if (++br.nb == 3) break;
             }
-            if (nbond == 0) warn(fmt("Nitrogen atom found with no bonded atoms, atom serial number %d", ia + 1));
-            double mean[3] = {0, 0, 0};
-            for (int b = 0; b < nbond; b++)
-                for (int i = 0; i < 3; i++) mean[i] += (bondv[b][i]) / nbond;
-            vect_normalize(mean);
-            for (int i = 0; i < 3; i++) rv[i] = -1 * mean[i];
+            if (br.nb == 0) warn(fmt("Nitrogen atom found with no bonded atoms, atom serial number %d", ia + 1));
+        }
+    }
+    eval_bond_vectors(coord.data(), rvector.data(), rvector2.data());
+}
+
+// The vector arithmetic of main.cpp:2320-2656 on the recorded topology.
+void Job::eval_bond_vectors(const double *xyz, double *rv_out, double *rv2_out) const
+{
+    auto C = [&](int a) { return &xyz[3 * (size_t)a]; };
+    std::fill(rv_out, rv_out + 3 * (size_t)n_atoms, 0.0);
+    std::fill(rv2_out, rv2_out + 3 * (size_t)n_atoms, 0.0);
+    for (int ia = 0; ia < n_atoms; ia++) {
+        const BondRec &br = bondrec[ia];
+        double *rv = rv_out + 3 * (size_t)ia, *rv2 = rv2_out + 3 * (size_t)ia;
+        switch (br.kind) {
+            case BondRec::D1:
+                for (int i = 0; i < 3; i++) rv[i] = C(ia)[i] - C(br.i1)[i];
+                vect_normalize(rv);
+                break;
+            case BondRec::A2_ONE:
+                vect_sub_normalize(rv, C(ia), C(br.i1));
+                if (br.i2 >= 0) {
+                    double d[3];
+                    for (int i = 0; i < 3; i++) d[i] = C(br.i1)[i] - C(br.i2)[i];
+                    vect_normalize(d);
+                    rv2[0] = rv[1] * d[2] - rv[2] * d[1];
+                    rv2[1] = rv[2] * d[0] - rv[0] * d[2];
+                    rv2[2] = rv[0] * d[1] - rv[1] * d[0];
+                    vect_normalize(rv2);
+                }
+                break;
+            case BondRec::A2_DIS:
+                vect_sub_normalize(rv, C(ia), C(br.i1));
+                break;
+            case BondRec::A2_TWO: {
+                vect_sub_normalize(rv2, C(br.i2), C(br.i1));
+                double rdot = 0.;
+                for (int i = 0; i < 3; i++) rdot += (C(ia)[i] - C(br.i1)[i]) * rv2[i];
+                for (int i = 0; i < 3; i++) rv[i] = C(ia)[i] - ((rdot * rv2[i]) + C(br.i1)[i]);
+                vect_normalize(rv);
+            } break;
+            case BondRec::A1: {
+                double mean[3] = {0, 0, 0};
+                for (int b = 0; b < br.nb; b++)
+                    for (int i = 0; i < 3; i++) mean[i] += (C(ia)[i] - C(br.nbr[b])[i]) / br.nb;
+                vect_normalize(mean);
+                for (int i = 0; i < 3; i++) rv[i] = -1 * mean[i];
+            } break;
+            default: break;
+        }
+    }
+}
+
+namespace {
+// Adjoint of vect_normalize (sub = false) / vect_sub_normalize (sub = true) at
+// input v: gv = J^T gy, with J = (I - y y^T)/|v| above the zero threshold and
+// J = I/threshold below it.
+void normalize_bwd(const double v[3], const double gy[3], double gv[3], bool sub)
+{
+    double rd;
+    bool below;
+    if (sub) {
+        const double rd2 = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+        below = rd2 < kApproxZero;
+        rd = below ? kApproxZero : std::sqrt(rd2);
+    } else {
+        rd = vlen(v);
+        below = rd < kApproxZero;
+        if (below) rd = kApproxZero;
+    }
+    if (below) {
+        for (int i = 0; i < 3; i++) gv[i] = gy[i] / rd;
+        return;
+    }
+    const double y[3] = {v[0] / rd, v[1] / rd, v[2] / rd};
+    const double yg = y[0] * gy[0] + y[1] * gy[1] + y[2] * gy[2];
+    for (int i = 0; i < 3; i++) gv[i] = (gy[i] - y[i] * yg) / rd;
+}
+
+inline void cross(const double a[3], const double b[3], double o[3])
+{
+    o[0] = a[1] * b[2] - a[2] * b[1];
+    o[1] = a[2] * b[0] - a[0] * b[2];
+    o[2] = a[0] * b[1] - a[1] * b[0];
+}
+}  // namespace
+
+// g_xyz += d(rvector, rvector2)/d(xyz)^T (g_rv, g_rv2), FP64, on the recorded topology.
+void Job::bond_vectors_backward(const double *xyz, const double *g_rv, const double *g_rv2, double *g_xyz) const
+{
+    auto C = [&](int a) { return &xyz[3 * (size_t)a]; };
+    auto add = [&](int a, const double g[3], double s) {
+        for (int i = 0; i < 3; i++) g_xyz[3 * (size_t)a + i] += s * g[i];
+    };
+    for (int ia = 0; ia < n_atoms; ia++) {
+        const BondRec &br = bondrec[ia];
+        const double *grv = g_rv + 3 * (size_t)ia, *grv2 = g_rv2 + 3 * (size_t)ia;
+        switch (br.kind) {
+            case BondRec::D1: {
+                double v[3], gv[3];
+                for (int i = 0; i < 3; i++) v[i] = C(ia)[i] - C(br.i1)[i];
+                normalize_bwd(v, grv, gv, false);
+                add(ia, gv, 1.);
+                add(br.i1, gv, -1.);
+            } break;
+            case BondRec::A2_ONE: {
+                double u[3], rv[3], g_rv_t[3] = {grv[0], grv[1], grv[2]};
+                for (int i = 0; i < 3; i++) u[i] = C(ia)[i] - C(br.i1)[i];
+                vect_sub_normalize(rv, C(ia), C(br.i1));
+                if (br.i2 >= 0) {
+                    double dd[3], dn[3], w[3], gw[3], t[3], gdn[3], gdd[3];
+                    for (int i = 0; i < 3; i++) dd[i] = dn[i] = C(br.i1)[i] - C(br.i2)[i];
+                    vect_normalize(dn);
+                    cross(rv, dn, w);
+                    normalize_bwd(w, grv2, gw, false);
+                    cross(dn, gw, t);  // d(rv x dn)/d rv ^T gw
+                    for (int i = 0; i < 3; i++) g_rv_t[i] += t[i];
+                    cross(gw, rv, gdn);  // d(rv x dn)/d dn ^T gw
+                    normalize_bwd(dd, gdn, gdd, false);
+                    add(br.i1, gdd, 1.);
+                    add(br.i2, gdd, -1.);
+                }
+                double gu[3];
+                normalize_bwd(u, g_rv_t, gu, true);
+                add(ia, gu, 1.);
+                add(br.i1, gu, -1.);
+            } break;
+            case BondRec::A2_DIS: {
+                double u[3], gu[3];
+                for (int i = 0; i < 3; i++) u[i] = C(ia)[i] - C(br.i1)[i];
+                normalize_bwd(u, grv, gu, true);
+                add(ia, gu, 1.);
+                add(br.i1, gu, -1.);
+            } break;
+            case BondRec::A2_TWO: {
+                double er[3], e[3], s[3], v[3], gv[3];
+                for (int i = 0; i < 3; i++) { er[i] = C(br.i2)[i] - C(br.i1)[i]; s[i] = C(ia)[i] - C(br.i1)[i]; }
+                vect_sub_normalize(e, C(br.i2), C(br.i1));
+                double rdot = 0.;
+                for (int i = 0; i < 3; i++) rdot += s[i] * e[i];
+                for (int i = 0; i < 3; i++) v[i] = C(ia)[i] - ((rdot * e[i]) + C(br.i1)[i]);
+                normalize_bwd(v, grv, gv, false);
+                const double egv = e[0] * gv[0] + e[1] * gv[1] + e[2] * gv[2];
+                double gs[3], ge[3], ger[3];
+                for (int i = 0; i < 3; i++) {
+                    gs[i] = gv[i] - e[i] * egv;                       // v = s - (s.e) e
+                    ge[i] = grv2[i] - (rdot * gv[i] + egv * s[i]);
+                }
+                normalize_bwd(er, ge, ger, true);
+                add(br.i2, ger, 1.);
+                add(br.i1, ger, -1.);
+                add(ia, gs, 1.);
+                add(br.i1, gs, -1.);
+            } break;
+            case BondRec::A1: {
+                if (br.nb == 0) break;
+                double mean[3] = {0, 0, 0}, gm[3], gmean[3];
+                for (int b = 0; b < br.nb; b++)
+                    for (int i = 0; i < 3; i++) mean[i] += (C(ia)[i] - C(br.nbr[b])[i]) / br.nb;
+                for (int i = 0; i < 3; i++) gm[i] = -grv[i];
+                normalize_bwd(mean, gm, gmean, false);
+                add(ia, gmean, 1.);
+                for (int b = 0; b < br.nb; b++) add(br.nbr[b], gmean, -1. / br.nb);
+            } break;
+            default: break;
         }
     }
 }
@@ -1116,6 +1290,24 @@ void ag_job_fail(ag_job *job, const char *message)
 }
 
 void ag_job_free(ag_job *job) { delete job; }
+
+ag_status ag_job_bond_vectors(const ag_job *job, const double *coord, double *rvector, double *rvector2)
+{
+    if (!job || !rvector || !rvector2) { agb::set_last_error("ag_job_bond_vectors: null argument"); return AG_ERR_INVALID; }
+    job->job.eval_bond_vectors(coord ? coord : job->job.coord.data(), rvector, rvector2);
+    return AG_OK;
+}
+
+ag_status ag_job_bond_vectors_backward(const ag_job *job, const double *coord, const double *g_rvector,
+                                       const double *g_rvector2, double *g_coord)
+{
+    if (!job || !g_rvector || !g_rvector2 || !g_coord) {
+        agb::set_last_error("ag_job_bond_vectors_backward: null argument");
+        return AG_ERR_INVALID;
+    }
+    job->job.bond_vectors_backward(coord ? coord : job->job.coord.data(), g_rvector, g_rvector2, g_coord);
+    return AG_OK;
+}
 
 const char *ag_last_error(void) { return agb::last_error(); }
 int32_t ag_abi_version(void) { return AG_ABI_VERSION; }

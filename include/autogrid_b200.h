@@ -262,6 +262,19 @@ ag_status          ag_job_write_maps_f64(ag_job *job, const double *maps);
 /* Record a fatal error in the job's GLG ("Unsuccessful Completion"). */
 void               ag_job_fail(ag_job *job, const char *message);
 void               ag_job_free(ag_job *job);
+/* Bond vectors (rvector, rvector2; [3N] each) at other coordinates coord
+ * ([3N], the problem's centred frame; NULL = the job's own), keeping the
+ * bonded neighbours the GPF load found (main.cpp:2320-2656: the same vector
+ * arithmetic, the neighbour search frozen).  At the job's own coordinates the
+ * result equals the problem's rvector/rvector2 bit for bit. */
+ag_status          ag_job_bond_vectors(const ag_job *job, const double *coord, double *rvector,
+                                       double *rvector2);
+/* Adjoint of ag_job_bond_vectors at coord, in FP64:
+ * g_coord += d(rvector, rvector2)/d(coord)^T (g_rvector, g_rvector2).
+ * No reference counterpart (the reference has no gradients). */
+ag_status          ag_job_bond_vectors_backward(const ag_job *job, const double *coord,
+                                                const double *g_rvector, const double *g_rvector2,
+                                                double *g_coord);
 
 #ifdef __cplusplus
 }
