@@ -6,8 +6,10 @@ Public API:
     Context(device).compute(p)   hot path on one problem (FP32 or FP64 twin)
     Context(device).plan(p)      device-resident plan for repeated runs
     Batch(ctx, problems)         many boxes in one persistent, graph-captured launch
+    Diff(ctx, p)                 differentiable mode: linear tables, hand-written adjoint
+    torch_maps.GridMaps(job)     torch.autograd binding of the differentiable mode
 """
 from ._abi import AutoGridError, load_library  # noqa: F401
-from .api import Batch, Context, Job, Plan, Problem, Stats, run_gpf  # noqa: F401
+from .api import Batch, Context, Diff, Job, Plan, Problem, Stats, run_gpf  # noqa: F401
 
-__all__ = ["AutoGridError", "Batch", "Context", "Job", "Plan", "Problem", "Stats", "load_library", "run_gpf"]
+__all__ = ["AutoGridError", "Batch", "Context", "Diff", "Job", "Plan", "Problem", "Stats", "load_library", "run_gpf"]

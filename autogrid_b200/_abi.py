@@ -29,6 +29,7 @@ STATUS_NAMES = {
 AG_PREC_FP32 = 0
 AG_PREC_FP64 = 1
 AG_TABLE_NEAREST = 0
+AG_TABLE_LINEAR = 1
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -106,6 +107,16 @@ SIGNATURES = {
     "ag_job_free": (None, [C.c_void_p]),
     "ag_job_bond_vectors": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_job_bond_vectors_backward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_diff_create": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),
+    "ag_diff_set_atoms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_diff_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "ag_diff_device_maps": (C.c_void_p, [C.c_void_p]),
+    "ag_diff_download": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_diff_closest_h": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_diff_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]),
+    "ag_diff_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "ag_diff_destroy": (C.c_int, [C.c_void_p]),
     "ag_emap_compute_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
                                           C.c_double, C.c_int32, C.c_void_p, C.c_double, C.c_double,
                                           C.c_void_p, C.c_void_p]),

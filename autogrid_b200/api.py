@@ -145,6 +145,7 @@ class Job:
         check(lib.ag_job_load(os.fsencode(gpf), os.fsencode(glg) if glg else None, C.byref(h)))
         self._h = h
         self._lib = lib
+        self.n_atoms = int(lib.ag_job_problem(h).contents.n_atoms)
 
     def problem(self) -> Problem:
         return Problem.from_struct(self._lib.ag_job_problem(self._h).contents)
@@ -160,7 +161,7 @@ class Job:
     def bond_vectors(self, coord: np.ndarray | None = None) -> tuple:
         """(rvector, rvector2) [N,3] at coord [N,3] (centred frame), with the
         bonded neighbours found at load time (ag_job_bond_vectors)."""
-        n = self.problem().n_atoms
+        n = self.n_atoms
         rv = np.zeros((n, 3)); rv2 = np.zeros((n, 3))
         c = None if coord is None else np.ascontiguousarray(coord, dtype=np.float64).reshape(n, 3)
         check(self._lib.ag_job_bond_vectors(self._h, None if c is None else c.ctypes.data_as(C.c_void_p),
@@ -169,7 +170,7 @@ class Job:
 
     def bond_vectors_backward(self, coord, g_rvector, g_rvector2) -> np.ndarray:
         """d(rvector, rvector2)/d(coord)^T (g_rvector, g_rvector2), [N,3] FP64."""
-        n = self.problem().n_atoms
+        n = self.n_atoms
         c = np.ascontiguousarray(coord, dtype=np.float64).reshape(n, 3)
         g1 = np.ascontiguousarray(g_rvector, dtype=np.float64).reshape(n, 3)
         g2 = np.ascontiguousarray(g_rvector2, dtype=np.float64).reshape(n, 3)
@@ -238,6 +239,92 @@ class Context:
     def close(self) -> None:
         if self._h:
             self._lib.ag_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Diff:
+    """Differentiable mode (ag_diff_*): maps with linearly interpolated tables
+    and their hand-written adjoint.  Arrays are FP64 numpy in the problem's
+    centred frame; maps and map gradients are in the chosen precision."""
+
+    def __init__(self, ctx: Context, problem: Problem, precision: str = "fp32"):
+        self.ctx = ctx
+        self.problem = problem
+        self._lib = ctx._lib
+        prec = _PREC[precision]
+        self.dtype = np.float64 if prec == _abi.AG_PREC_FP64 else np.float32
+        self.shape = problem.map_shape
+        self.n_atoms = problem.n_atoms
+        opts = ag_opts(precision=prec, table_mode=_abi.AG_TABLE_LINEAR)
+        s = problem.struct()
+        h = C.c_void_p()
+        check(self._lib.ag_diff_create(ctx._h, C.byref(s), C.byref(opts), C.byref(h)))
+        self._h = h
+
+    @staticmethod
+    def _ptr(a, n, cols=None):
+        if a is None:
+            return None, None
+        shape = (n,) if cols is None else (n, cols)
+        arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+        return arr, arr.ctypes.data_as(C.c_void_p)
+
+    def set_atoms(self, coord=None, charge=None, rvector=None, rvector2=None) -> None:
+        n = self.n_atoms
+        c, pc = self._ptr(coord, n, 3)
+        q, pq = self._ptr(charge, n)
+        r1, p1 = self._ptr(rvector, n, 3)
+        r2, p2 = self._ptr(rvector2, n, 3)
+        check(self._lib.ag_diff_set_atoms(self._h, pc, pq, p1, p2))
+
+    def forward(self, keep_closest_h: bool = False, device_out: int | None = None) -> None:
+        """Compute the maps (into device_out, a device pointer, or the object's buffer)."""
+        check(self._lib.ag_diff_forward(self._h, int(bool(keep_closest_h)),
+                                        None if device_out is None else C.c_void_p(int(device_out))))
+
+    def maps(self) -> np.ndarray:
+        out = np.empty(self.shape, dtype=self.dtype)
+        check(self._lib.ag_diff_download(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def closest_h(self) -> np.ndarray:
+        out = np.empty(int(np.prod(self.shape[1:])), dtype=np.int32)
+        check(self._lib.ag_diff_closest_h(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def backward(self, grad_maps=None, device_ptr: int | None = None) -> dict:
+        """Adjoint of the last forward for dL/d(maps) given as a host array or a
+        device pointer.  Returns FP64 dL/d(coord) (pair terms only), charge,
+        rvector, rvector2."""
+        n = self.n_atoms
+        gc = np.zeros((n, 3)); gq = np.zeros(n); g1 = np.zeros((n, 3)); g2 = np.zeros((n, 3))
+        if device_ptr is not None:
+            src, on_dev = C.c_void_p(int(device_ptr)), 1
+        else:
+            g = np.ascontiguousarray(grad_maps, dtype=self.dtype)
+            if g.size != int(np.prod(self.shape)):
+                raise ValueError("grad_maps must have the map shape")
+            src, on_dev = g.ctypes.data_as(C.c_void_p), 0
+        check(self._lib.ag_diff_backward(self._h, src, on_dev, gc.ctypes.data_as(C.c_void_p),
+                                         gq.ctypes.data_as(C.c_void_p), g1.ctypes.data_as(C.c_void_p),
+                                         g2.ctypes.data_as(C.c_void_p)))
+        return {"coord": gc, "charge": gq, "rvector": g1, "rvector2": g2}
+
+    def timing(self) -> tuple:
+        """(forward_ms, closest_h_ms, backward_ms) of the last calls (device events)."""
+        f, c, b = C.c_float(), C.c_float(), C.c_float()
+        check(self._lib.ag_diff_timing(self._h, C.byref(f), C.byref(c), C.byref(b)))
+        return f.value, c.value, b.value
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.ag_diff_destroy(self._h)
             self._h = None
 
     def __del__(self):

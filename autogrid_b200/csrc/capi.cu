@@ -162,6 +162,17 @@ ag_status validate(const ag_problem *p)
     return AG_OK;
 }
 
+}  // namespace
+
+// Internal accessors for the other host modules of the library.
+namespace agb {
+ag_status validate_problem(const ag_problem *p) { return validate(p); }
+cudaStream_t context_stream(const ag_context *c) { return c->stream; }
+int context_device(const ag_context *c) { return c->device; }
+}  // namespace agb
+
+namespace {
+
 template <class T>
 cudaError_t upload(BufferSet *b, const char *name, const T *src, size_t n, T **dst, cudaStream_t s, size_t *acc)
 {
@@ -665,7 +676,7 @@ ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool
     if (o) opts = *o;
     if (opts.precision != AG_PREC_FP32 && opts.precision != AG_PREC_FP64) return invalid("unknown precision");
     if (opts.table_mode != AG_TABLE_NEAREST) {
-        set_last_error("only nearest-bin tables are provided by this build");
+        set_last_error("the drop-in path reads nearest-bin tables; linear tables are the differentiable mode (ag_diff_create)");
         return AG_ERR_UNSUPPORTED;
     }
     AGB_CK(cudaSetDevice(ctx->device));

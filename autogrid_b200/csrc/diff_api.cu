@@ -1,0 +1,470 @@
+// C ABI of the differentiable mode (kernels/diff.h defines it): problem
+// binding, cell list, interpolation tables, forward and adjoint launches.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "autogrid_b200.h"
+#include "kernels/diff.h"
+
+namespace agb {
+void set_last_error(const std::string &m);
+ag_status validate_problem(const ag_problem *p);
+cudaStream_t context_stream(const ag_context *c);
+int context_device(const ag_context *c);
+}  // namespace agb
+
+using namespace agb;
+
+namespace {
+
+ag_status fail_cuda(cudaError_t e, const char *what)
+{
+    set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return AG_ERR_CUDA;
+}
+
+#define DF_CK(call)                                        \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return fail_cuda(e_, #call); \
+    } while (0)
+
+// What the atom term of atom map m does for a receptor atom of class hb and
+// disorder flag dis: the branch conditions of main.cpp:3290-3379.
+uint8_t action_of(const ag_problem *p, int m, int hb, int dis)
+{
+    if (!p->map_is_hbonder[m]) return DA_PLAIN;
+    const int mh = p->map_hbond[m];
+    const bool rec_donor = hb == 1 || hb == 2 || hb == 6;
+    if ((mh == 3 || mh == 5 || mh == 6) && rec_donor) return dis ? DA_SUMA_DIS : DA_SUMA;
+    if ((mh == 4 || mh == 6) && rec_donor) return DA_MMA;
+    if ((mh == 1 || mh == 2 || mh == 6) && (hb > 2 || hb == 6)) return dis ? DA_SUMD_DIS : DA_MMD;
+    return DA_PLAIN;
+}
+
+struct Slot {
+    int map = -1, kind = DK_ATOM, tab = -1, desolv = 0;
+    bool mm = false;
+    uint8_t act[16] = {};
+};
+
+}  // namespace
+
+struct ag_diff {
+    ag_context *ctx = nullptr;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    bool fp64 = false;
+    size_t esz = 4;
+    int N = 0, n_maps = 0, n_atom_maps = 0, elec = -1;
+    long long P = 0;
+    int n1[3] = {0, 0, 0}, ne[3] = {0, 0, 0};
+    double spacing = 0;
+    std::vector<double> coord, charge, rv, rv2;
+    std::vector<int> h_index;
+    DiffArgs args{};
+    // device
+    std::vector<void *> allocs;
+    double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr, *d_q = nullptr, *d_vol = nullptr, *d_solpar = nullptr;
+    double *d_rv = nullptr, *d_rv2 = nullptr, *d_grad = nullptr;
+    int *d_meta = nullptr, *d_h = nullptr, *d_cell_start = nullptr, *d_cell_atoms = nullptr;
+    int *d_ch = nullptr, *d_mmarg = nullptr;
+    void *d_vdw = nullptr, *d_sol = nullptr, *d_eps = nullptr, *d_maps = nullptr, *d_gmaps = nullptr;
+    cudaEvent_t ev[6] = {};
+    float fwd_ms = 0, ch_ms = 0, bwd_ms = 0;
+    bool have_ch = false, have_fwd = false;
+    const void *last_out = nullptr;
+
+    ~ag_diff()
+    {
+        cudaSetDevice(device);
+        for (void *p : allocs) cudaFree(p);
+        for (auto &e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+    template <class T> cudaError_t alloc(T **p, size_t n)
+    {
+        void *v = nullptr;
+        cudaError_t e = cudaMalloc(&v, std::max<size_t>(n, 1) * sizeof(T));
+        if (e == cudaSuccess) {
+            allocs.push_back(v);
+            *p = (T *)v;
+        }
+        return e;
+    }
+    ag_status upload_atoms();
+};
+
+namespace {
+
+template <class R>
+void build_tables(const ag_problem *p, std::vector<R2<R>> &vdw, std::vector<R2<R>> &sol, std::vector<R2<R>> &eps)
+{
+    const int nT = p->n_rec_types, nAM = p->n_atom_maps;
+    vdw.assign((size_t)std::max(nT, 1) * std::max(nAM, 1) * AG_NEINT, R2<R>{R(0), R(0)});
+    for (int t = 0; t < nT; t++)
+        for (int m = 0; m < nAM; m++) {
+            const float *src = p->e_vdw_hb + ((size_t)t * nAM + m) * AG_NEINT;
+            R2<R> *dst = vdw.data() + ((size_t)t * nAM + m) * AG_NEINT;
+            for (int b = 0; b < AG_NEINT; b++) {
+                const double v = src[b], nx = (b < AG_NEINT - 1) ? (double)src[b + 1] : v;
+                dst[b] = R2<R>{R(v), R(nx - v)};
+            }
+        }
+    sol.resize(AG_NEINT);
+    for (int b = 0; b < AG_NEINT; b++)
+        sol[b] = R2<R>{R(p->sol_fn[b]), R(p->sol_fn[b + 1] - p->sol_fn[b])};
+    eps.resize(AG_NDIEL);
+    auto f = [&](int b) { return p->dddiel ? p->r_epsilon_fn[b] * p->coeff_estat : p->invdielcal * p->coeff_estat; };
+    for (int b = 0; b < AG_NDIEL; b++) {
+        const double v = f(b), nx = (b < AG_NDIEL - 1) ? f(b + 1) : v;
+        eps[b] = R2<R>{R(v), R(nx - v)};
+    }
+}
+
+template <class R> cudaError_t put(void **dst, const std::vector<R> &v, ag_diff *d)
+{
+    R *p = nullptr;
+    cudaError_t e = d->alloc(&p, v.size());
+    if (e != cudaSuccess) return e;
+    *dst = p;
+    return cudaMemcpy(p, v.data(), v.size() * sizeof(R), cudaMemcpyHostToDevice);
+}
+
+}  // namespace
+
+// Coordinates, charges, bond vectors and the cell list of the current atoms.
+ag_status ag_diff::upload_atoms()
+{
+    std::vector<double> x(N), y(N), z(N);
+    for (int a = 0; a < N; a++) { x[a] = coord[3 * a]; y[a] = coord[3 * a + 1]; z[a] = coord[3 * a + 2]; }
+    // cell list over the grid box grown by DF_RADIUS; atoms outside it have no
+    // point within the 8 A cutoff
+    std::vector<int> cell_of(N, -1), start((size_t)args.ncx * args.ncy * args.ncz + 1, 0);
+    for (int a = 0; a < N; a++) {
+        int c[3];
+        bool in = true;
+        const double pc[3] = {x[a], y[a], z[a]};
+        const int nc[3] = {args.ncx, args.ncy, args.ncz};
+        for (int i = 0; i < 3; i++) {
+            const double u = std::floor((pc[i] - args.cell0[i]) / args.cell_size);
+            if (!(u >= 0 && u < nc[i])) { in = false; break; }
+            c[i] = (int)u;
+        }
+        if (!in) continue;
+        cell_of[a] = c[0] + args.ncx * (c[1] + args.ncy * c[2]);
+        start[cell_of[a] + 1]++;
+    }
+    for (size_t i = 1; i < start.size(); i++) start[i] += start[i - 1];
+    std::vector<int> fill(start.begin(), start.end() - 1), atoms(std::max(start.back(), 1));
+    for (int a = 0; a < N; a++)
+        if (cell_of[a] >= 0) atoms[fill[cell_of[a]]++] = a;
+    const size_t nb = (size_t)N * sizeof(double);
+    DF_CK(cudaMemcpyAsync(d_x, x.data(), nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_y, y.data(), nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_z, z.data(), nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_q, charge.data(), nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_rv, rv.data(), 3 * nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_rv2, rv2.data(), 3 * nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_cell_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_cell_atoms, atoms.data(), atoms.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaStreamSynchronize(stream));  // host vectors are locals
+    return AG_OK;
+}
+
+extern "C" {
+
+ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o, ag_diff **out)
+{
+    if (!ctx || !p || !o || !out) { set_last_error("ag_diff_create: null argument"); return AG_ERR_INVALID; }
+    *out = nullptr;
+    if (o->table_mode != AG_TABLE_LINEAR) {
+        set_last_error("ag_diff_create: opts->table_mode must be AG_TABLE_LINEAR");
+        return AG_ERR_INVALID;
+    }
+    if (o->precision != AG_PREC_FP32 && o->precision != AG_PREC_FP64) {
+        set_last_error("ag_diff_create: unknown precision");
+        return AG_ERR_INVALID;
+    }
+    ag_status st = validate_problem(p);
+    if (st != AG_OK) return st;
+    const int nAM = p->n_atom_maps;
+    // Slots: every map but the e map.  The atom term of map m and the
+    // desolvation target follow the reference's map loop (main.cpp:3286-3390):
+    // a covalent map is skipped whole; with separate desolvation maps the
+    // desolvation of map m goes to map m+1.
+    std::vector<Slot> slots;
+    std::vector<int> tab_of(std::max(nAM, 1), -1), desolv_of(std::max(nAM, 1), 0);
+    for (int m = 0; m < nAM; m++) {
+        if (p->map_is_covalent[m]) continue;
+        tab_of[m] = m;
+        int dm = m;
+        if (p->separate_desolvation_maps) dm = ++m;
+        if (dm >= nAM) {
+            set_last_error("ag_diff_create: desolvation partner past the last atom map");
+            return AG_ERR_INVALID;
+        }
+        desolv_of[dm] = 1;
+    }
+    for (int m = 0; m < nAM; m++) {
+        Slot s;
+        s.map = m;
+        s.kind = p->map_is_covalent[m] ? DK_COV : DK_ATOM;  // covalent: Gaussian added at the end
+        s.tab = tab_of[m];
+        s.desolv = desolv_of[m];
+        if (s.tab >= 0)
+            for (int dis = 0; dis < 2; dis++)
+                for (int hb = 0; hb < 8; hb++) {
+                    s.act[hb + 8 * dis] = action_of(p, s.tab, hb, dis);
+                    if (s.act[hb + 8 * dis] == DA_MMA || s.act[hb + 8 * dis] == DA_MMD) s.mm = true;
+                }
+        slots.push_back(s);
+    }
+    if (p->dsolv_map >= 0) {
+        Slot s;
+        s.map = p->dsolv_map;
+        s.kind = DK_D;
+        slots.push_back(s);
+    }
+    std::stable_partition(slots.begin(), slots.end(), [](const Slot &s) { return s.mm; });
+    const int n_mm = (int)std::count_if(slots.begin(), slots.end(), [](const Slot &s) { return s.mm; });
+    if ((int)slots.size() > DF_MAXS || n_mm > DF_MAXMM) {
+        set_last_error("ag_diff_create: the differentiable mode takes at most 16 maps besides the e map, "
+                       "at most 8 with H-bond min/max terms");
+        return AG_ERR_UNSUPPORTED;
+    }
+
+    cudaError_t ce = cudaSetDevice(context_device(ctx));
+    if (ce != cudaSuccess) return fail_cuda(ce, "cudaSetDevice");
+    std::unique_ptr<ag_diff> d(new ag_diff());
+    d->ctx = ctx;
+    d->stream = context_stream(ctx);
+    d->device = context_device(ctx);
+    d->fp64 = o->precision == AG_PREC_FP64;
+    d->esz = d->fp64 ? sizeof(double) : sizeof(float);
+    d->N = p->n_atoms;
+    d->n_maps = p->n_maps;
+    d->n_atom_maps = nAM;
+    d->elec = p->elec_map;
+    for (int i = 0; i < 3; i++) { d->n1[i] = p->n1[i]; d->ne[i] = p->ne[i]; }
+    d->spacing = p->spacing;
+    d->P = (long long)p->n1[0] * p->n1[1] * p->n1[2];
+    const int N = d->N;
+    d->coord.assign(p->coord, p->coord + 3 * (size_t)N);
+    d->charge.assign(p->charge, p->charge + N);
+    d->rv.assign(p->rvector, p->rvector + 3 * (size_t)N);
+    d->rv2.assign(p->rvector2, p->rvector2 + 3 * (size_t)N);
+    std::vector<int> meta(std::max(N, 1), 0);
+    for (int a = 0; a < N; a++) {
+        const bool skip = p->disorder_h && p->disorder[a] && p->rec_type[a] == p->hydrogen_type;
+        meta[a] = (p->rec_type[a] & DM_TYPE_MASK) | (p->hbond[a] << DM_HB_SHIFT) | ((p->rexp[a] & 7) << DM_REXP_SHIFT) |
+                  (p->disorder[a] ? DM_DIS : 0) | (skip ? DM_SKIP : 0);
+        if (p->hbond[a] == 1 || p->hbond[a] == 2) d->h_index.push_back(a);
+    }
+
+    DiffArgs &A = d->args;
+    std::memset(&A, 0, sizeof A);
+    A.n_atoms = N;
+    A.n1x = p->n1[0]; A.n1y = p->n1[1]; A.n1z = p->n1[2];
+    A.nex = p->ne[0]; A.ney = p->ne[1]; A.nez = p->ne[2];
+    A.P = d->P;
+    A.spacing = p->spacing;
+    A.disorder_h = p->disorder_h;
+    A.hydrogen_type = p->hydrogen_type;
+    A.n_rec_types = p->n_rec_types;
+    A.n_atom_maps = nAM;
+    A.solpar_q = p->solpar_q;
+    A.n_h = (int)d->h_index.size();
+    for (int i = 0; i < 3; i++) A.cov_pos[i] = p->cov_pos[i];
+    A.cov_half_width = p->cov_half_width;
+    A.cov_barrier = p->cov_barrier;
+    A.elec_map = p->elec_map;
+    A.n_slots = (int)slots.size();
+    A.n_mm = n_mm;
+    for (int s = 0; s < A.n_slots; s++) {
+        const Slot &sl = slots[s];
+        A.slot_map[s] = sl.map;
+        A.slot_kind[s] = sl.kind;
+        A.slot_tab[s] = sl.tab;
+        A.slot_mm[s] = sl.mm ? s : -1;
+        A.slot_desolv[s] = sl.desolv;
+        A.slot_sp[s] = (sl.kind != DK_D) ? p->map_solpar_probe[sl.map] : 0.0;
+        A.slot_vp[s] = (sl.kind != DK_D) ? p->map_vol_probe[sl.map] : 0.0;
+        std::memcpy(A.act[s], sl.act, 16);
+    }
+    // cell list geometry: at most 6 cells per axis around a brick
+    const double span = (DF_BRICK_X - 1) * p->spacing + 2 * DF_RADIUS;
+    A.cell_size = std::max(4.0, span / 5.0);
+    for (int i = 0; i < 3; i++) {
+        const double lo = -p->ne[i] * p->spacing - DF_RADIUS, hi = p->ne[i] * p->spacing + DF_RADIUS;
+        A.cell0[i] = lo;
+        const int n = (int)std::ceil((hi - lo) / A.cell_size) + 1;
+        if (i == 0) A.ncx = n; else if (i == 1) A.ncy = n; else A.ncz = n;
+    }
+    const size_t ncells = (size_t)A.ncx * A.ncy * A.ncz;
+
+    DF_CK(d->alloc(&d->d_x, N)); DF_CK(d->alloc(&d->d_y, N)); DF_CK(d->alloc(&d->d_z, N));
+    DF_CK(d->alloc(&d->d_q, N)); DF_CK(d->alloc(&d->d_vol, N)); DF_CK(d->alloc(&d->d_solpar, N));
+    DF_CK(d->alloc(&d->d_rv, 3 * (size_t)N)); DF_CK(d->alloc(&d->d_rv2, 3 * (size_t)N));
+    DF_CK(d->alloc(&d->d_meta, N)); DF_CK(d->alloc(&d->d_h, d->h_index.size()));
+    DF_CK(d->alloc(&d->d_cell_start, ncells + 1)); DF_CK(d->alloc(&d->d_cell_atoms, N));
+    DF_CK(d->alloc(&d->d_ch, d->P)); DF_CK(d->alloc(&d->d_mmarg, 2 * (size_t)std::max(n_mm, 1) * d->P));
+    DF_CK(d->alloc(&d->d_grad, 10 * (size_t)N));
+    unsigned char *mp = nullptr;
+    DF_CK(d->alloc(&mp, d->esz * d->P * d->n_maps)); d->d_maps = mp;
+    unsigned char *gp = nullptr;
+    DF_CK(d->alloc(&gp, d->esz * d->P * d->n_maps)); d->d_gmaps = gp;
+    DF_CK(cudaMemcpy(d->d_vol, p->vol, N * sizeof(double), cudaMemcpyHostToDevice));
+    DF_CK(cudaMemcpy(d->d_solpar, p->solpar, N * sizeof(double), cudaMemcpyHostToDevice));
+    DF_CK(cudaMemcpy(d->d_meta, meta.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+    if (!d->h_index.empty())
+        DF_CK(cudaMemcpy(d->d_h, d->h_index.data(), d->h_index.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (d->fp64) {
+        std::vector<R2<double>> vdw, sol, eps;
+        build_tables(p, vdw, sol, eps);
+        DF_CK(put(&d->d_vdw, vdw, d.get())); DF_CK(put(&d->d_sol, sol, d.get())); DF_CK(put(&d->d_eps, eps, d.get()));
+    } else {
+        std::vector<R2<float>> vdw, sol, eps;
+        build_tables(p, vdw, sol, eps);
+        DF_CK(put(&d->d_vdw, vdw, d.get())); DF_CK(put(&d->d_sol, sol, d.get())); DF_CK(put(&d->d_eps, eps, d.get()));
+    }
+    A.x = d->d_x; A.y = d->d_y; A.z = d->d_z; A.q = d->d_q; A.vol = d->d_vol; A.solpar = d->d_solpar;
+    A.rv = d->d_rv; A.rv2 = d->d_rv2; A.meta = d->d_meta; A.h_index = d->d_h;
+    A.cell_start = d->d_cell_start; A.cell_atoms = d->d_cell_atoms;
+    for (auto &e : d->ev) DF_CK(cudaEventCreate(&e));
+    st = d->upload_atoms();
+    if (st != AG_OK) return st;
+    *out = d.release();
+    return AG_OK;
+}
+
+ag_status ag_diff_set_atoms(ag_diff *d, const double *coord, const double *charge, const double *rvector,
+                            const double *rvector2)
+{
+    if (!d) { set_last_error("ag_diff_set_atoms: null argument"); return AG_ERR_INVALID; }
+    const size_t N = d->N;
+    for (size_t i = 0; coord && i < 3 * N; i++)
+        if (!std::isfinite(coord[i])) { set_last_error("ag_diff_set_atoms: non-finite coordinate"); return AG_ERR_INVALID; }
+    for (size_t i = 0; charge && i < N; i++)
+        if (!std::isfinite(charge[i])) { set_last_error("ag_diff_set_atoms: non-finite charge"); return AG_ERR_INVALID; }
+    DF_CK(cudaSetDevice(d->device));
+    if (coord) d->coord.assign(coord, coord + 3 * N);
+    if (charge) d->charge.assign(charge, charge + N);
+    if (rvector) d->rv.assign(rvector, rvector + 3 * N);
+    if (rvector2) d->rv2.assign(rvector2, rvector2 + 3 * N);
+    return d->upload_atoms();
+}
+
+ag_status ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out)
+{
+    if (!d) { set_last_error("ag_diff_forward: null argument"); return AG_ERR_INVALID; }
+    DF_CK(cudaSetDevice(d->device));
+    cudaStream_t s = d->stream;
+    unsigned char *out = device_out ? (unsigned char *)device_out : (unsigned char *)d->d_maps;
+    const DiffArgs &A = d->args;
+    const bool search = !keep_closest_h || !d->have_ch;
+    bool timed_search = false;
+    if (search) {
+        d->have_ch = false;
+        if (d->n_atom_maps > 0) {
+            if (A.n_h == 0) {
+                set_last_error("no closestH atom was found");  // main.cpp:3011-3014
+                return AG_ERR_NO_CLOSEST_H;
+            }
+            DF_CK(cudaEventRecord(d->ev[4], s));
+            DF_CK(launch_closest_h(A, d->d_ch, s));
+            DF_CK(cudaEventRecord(d->ev[5], s));
+            timed_search = true;
+        } else {
+            DF_CK(cudaMemsetAsync(d->d_ch, 0xff, sizeof(int) * d->P, s));
+        }
+    }
+    DF_CK(cudaEventRecord(d->ev[0], s));
+    if (d->elec >= 0) DF_CK(launch_emap_lin(d->fp64, A, d->d_eps, out + d->esz * d->P * d->elec, s));
+    DF_CK(launch_near_lin(d->fp64, A, d->d_vdw, d->d_sol, out, d->d_ch, d->d_mmarg, s));
+    DF_CK(cudaEventRecord(d->ev[1], s));
+    DF_CK(cudaStreamSynchronize(s));
+    DF_CK(cudaEventElapsedTime(&d->fwd_ms, d->ev[0], d->ev[1]));
+    d->ch_ms = 0;
+    if (timed_search) DF_CK(cudaEventElapsedTime(&d->ch_ms, d->ev[4], d->ev[5]));
+    d->have_ch = true;
+    d->have_fwd = true;
+    d->last_out = out;
+    return AG_OK;
+}
+
+const void *ag_diff_device_maps(const ag_diff *d) { return d ? d->d_maps : nullptr; }
+
+ag_status ag_diff_download(ag_diff *d, void *host_maps)
+{
+    if (!d || !host_maps) { set_last_error("ag_diff_download: null argument"); return AG_ERR_INVALID; }
+    DF_CK(cudaSetDevice(d->device));
+    DF_CK(cudaMemcpyAsync(host_maps, d->d_maps, d->esz * d->P * d->n_maps, cudaMemcpyDeviceToHost, d->stream));
+    DF_CK(cudaStreamSynchronize(d->stream));
+    return AG_OK;
+}
+
+ag_status ag_diff_closest_h(ag_diff *d, int32_t *host_out)
+{
+    if (!d || !host_out) { set_last_error("ag_diff_closest_h: null argument"); return AG_ERR_INVALID; }
+    if (!d->have_ch) { set_last_error("ag_diff_closest_h: no forward yet"); return AG_ERR_INVALID; }
+    DF_CK(cudaSetDevice(d->device));
+    DF_CK(cudaMemcpyAsync(host_out, d->d_ch, sizeof(int) * d->P, cudaMemcpyDeviceToHost, d->stream));
+    DF_CK(cudaStreamSynchronize(d->stream));
+    return AG_OK;
+}
+
+ag_status ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_device, double *g_coord,
+                           double *g_charge, double *g_rvector, double *g_rvector2)
+{
+    if (!d || !grad_maps) { set_last_error("ag_diff_backward: null argument"); return AG_ERR_INVALID; }
+    if (!d->have_fwd) { set_last_error("ag_diff_backward: no forward to differentiate"); return AG_ERR_INVALID; }
+    DF_CK(cudaSetDevice(d->device));
+    cudaStream_t s = d->stream;
+    const size_t N = d->N;
+    const unsigned char *gm = (const unsigned char *)grad_maps;
+    if (!grad_on_device) {
+        DF_CK(cudaMemcpyAsync(d->d_gmaps, grad_maps, d->esz * d->P * d->n_maps, cudaMemcpyHostToDevice, s));
+        gm = (const unsigned char *)d->d_gmaps;
+    }
+    DiffGrads g;
+    g.xyz = d->d_grad;
+    g.q = d->d_grad + 3 * N;
+    g.rv = d->d_grad + 4 * N;
+    g.rv2 = d->d_grad + 7 * N;
+    DF_CK(cudaMemsetAsync(d->d_grad, 0, 10 * N * sizeof(double), s));
+    DF_CK(cudaEventRecord(d->ev[2], s));
+    if (d->elec >= 0) DF_CK(launch_emap_lin_adj(d->fp64, d->args, d->d_eps, gm + d->esz * d->P * d->elec, g, s));
+    DF_CK(launch_near_lin_adj(d->fp64, d->args, d->d_vdw, d->d_sol, gm, d->d_ch, d->d_mmarg, g, s));
+    DF_CK(cudaEventRecord(d->ev[3], s));
+    if (g_coord) DF_CK(cudaMemcpyAsync(g_coord, g.xyz, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (g_charge) DF_CK(cudaMemcpyAsync(g_charge, g.q, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (g_rvector) DF_CK(cudaMemcpyAsync(g_rvector, g.rv, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (g_rvector2) DF_CK(cudaMemcpyAsync(g_rvector2, g.rv2, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DF_CK(cudaStreamSynchronize(s));
+    DF_CK(cudaEventElapsedTime(&d->bwd_ms, d->ev[2], d->ev[3]));
+    return AG_OK;
+}
+
+ag_status ag_diff_timing(const ag_diff *d, float *forward_ms, float *closest_h_ms, float *backward_ms)
+{
+    if (!d) { set_last_error("ag_diff_timing: null argument"); return AG_ERR_INVALID; }
+    if (forward_ms) *forward_ms = d->fwd_ms;
+    if (closest_h_ms) *closest_h_ms = d->ch_ms;
+    if (backward_ms) *backward_ms = d->bwd_ms;
+    return AG_OK;
+}
+
+ag_status ag_diff_destroy(ag_diff *d)
+{
+    delete d;
+    return AG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,79 @@
+"""torch.autograd binding of the differentiable mode (optional; needs torch).
+
+    job = Job("rec.gpf")
+    maps_fn = GridMaps(job, device=0)                  # FP32 kernels
+    coords = torch.tensor(job.problem().arrays["coord"], requires_grad=True)
+    charges = torch.tensor(job.problem().arrays["charge"], requires_grad=True)
+    maps = maps_fn(coords, charges)                    # [n_maps, n1z, n1y, n1x] on cuda
+    loss = (w * maps).sum(); loss.backward()           # coords.grad, charges.grad
+
+Coordinates are in the problem's centred frame.  The forward recomputes the
+bond vectors at the given coordinates with the bonded neighbours found at load
+time (ag_job_bond_vectors); the backward runs the hand-written adjoint kernels
+(ag_diff_backward) and chains the bond-vector gradients back to the
+coordinates in FP64 (ag_job_bond_vectors_backward).  The closest DS/D1 atom of
+each grid point is searched at the first forward and kept afterwards
+(keep_closest_h=False searches it at every forward).
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .api import Context, Diff, Job
+
+
+class GridMaps:
+    """Callable (coords [N,3], charges [N]) -> maps, differentiable in both."""
+
+    def __init__(self, job: Job, device: int = 0, precision: str = "fp32", keep_closest_h: bool = True):
+        self.job = job
+        self.problem = job.problem()
+        self.device = torch.device("cuda", device)
+        self.ctx = Context(device)
+        self.diff = Diff(self.ctx, self.problem, precision)
+        self.dtype = torch.float64 if precision == "fp64" else torch.float32
+        self.keep_closest_h = keep_closest_h
+        self.generation = 0
+        self._searched = False
+
+    def __call__(self, coords: torch.Tensor, charges: torch.Tensor) -> torch.Tensor:
+        return _GridMapsFn.apply(coords, charges, self)
+
+    def _run(self, coord: np.ndarray, charge: np.ndarray, out: torch.Tensor) -> None:
+        rv, rv2 = self.job.bond_vectors(coord)
+        self.diff.set_atoms(coord, charge, rv, rv2)
+        torch.cuda.current_stream(self.device).synchronize()  # out may reuse memory torch just released
+        self.diff.forward(keep_closest_h=self.keep_closest_h and self._searched, device_out=out.data_ptr())
+        self._searched = True
+        self.generation += 1
+
+
+class _GridMapsFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, coords, charges, engine: GridMaps):
+        coord = coords.detach().to("cpu", torch.float64).numpy().reshape(-1, 3)
+        charge = charges.detach().to("cpu", torch.float64).numpy().reshape(-1)
+        out = torch.empty(engine.diff.shape, dtype=engine.dtype, device=engine.device)
+        engine._run(coord, charge, out)
+        ctx.engine = engine
+        ctx.generation = engine.generation
+        ctx.coord, ctx.charge = coord, charge
+        ctx.shapes = (coords.shape, coords.dtype, coords.device, charges.shape, charges.dtype, charges.device)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad):
+        engine: GridMaps = ctx.engine
+        if engine.generation != ctx.generation:  # another forward ran since: recompute this one
+            scratch = torch.empty(engine.diff.shape, dtype=engine.dtype, device=engine.device)
+            keep = engine.keep_closest_h
+            engine._run(ctx.coord, ctx.charge, scratch)
+            engine.keep_closest_h = keep
+        g = grad.to(device=engine.device, dtype=engine.dtype).contiguous()
+        torch.cuda.current_stream(engine.device).synchronize()
+        out = engine.diff.backward(device_ptr=g.data_ptr())
+        g_coord = out["coord"] + engine.job.bond_vectors_backward(ctx.coord, out["rvector"], out["rvector2"])
+        cs, cdt, cdev, qs, qdt, qdev = ctx.shapes
+        return (torch.from_numpy(g_coord).reshape(cs).to(device=cdev, dtype=cdt),
+                torch.from_numpy(out["charge"]).reshape(qs).to(device=qdev, dtype=qdt), None)

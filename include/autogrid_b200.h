@@ -124,7 +124,9 @@ typedef struct ag_problem {
 
 enum { AG_PREC_FP32 = 0,   /* production path                                  */
        AG_PREC_FP64 = 1 }; /* FP64 GPU twin: the stated error oracle           */
-enum { AG_TABLE_NEAREST = 0 }; /* reference nearest-bin tables (drop-in)       */
+enum { AG_TABLE_NEAREST = 0,   /* reference nearest-bin tables (drop-in)       */
+       AG_TABLE_LINEAR = 1 }; /* linear interpolation between bins: the
+                                 differentiable mode (ag_diff_*)               */
 
 typedef struct ag_opts {
     int32_t precision;   /* AG_PREC_*                                          */
@@ -245,6 +247,59 @@ ag_status    ag_batch_destroy(ag_batch *batch);
  * device, [n_maps_i][P_i] each), destroy. */
 ag_status    ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *problems, int32_t n,
                                    const ag_opts *opts, float *const *maps);
+
+/*
+ * Differentiable mode.  No counterpart in the reference (which has no
+ * gradients).  The maps of the hot path with every distance table read by
+ * linear interpolation between bins, the short-range terms switched to zero
+ * over the last bin before the 8 A cutoff, the D1 ramp evaluated for every D1
+ * pair and the two A2 angular branches made to meet at cos_theta = 0, so the
+ * maps are continuous in the receptor coordinates and charges.  Discrete
+ * choices are frozen: each point's closest DS/D1 atom (kept from an earlier
+ * forward on request), the bonded neighbours behind the bond vectors (see
+ * ag_job_bond_vectors) and, for the adjoint, the atoms attaining each H-bond
+ * min/max.  The nearest-bin drop-in (ag_maps_compute) is unchanged.
+ *
+ * Limits: at most 16 maps besides the e map, at most 8 of which keep an H-bond
+ * min/max (AG_ERR_UNSUPPORTED otherwise).
+ *
+ * Arrays: coord [3N] centred (the problem's frame), charge [N], rvector and
+ * rvector2 [3N], all FP64 host memory.  Maps and map gradients are
+ * [n_maps][P] in the precision of opts->precision (float or double); P =
+ * n1x*n1y*n1z.
+ */
+typedef struct ag_diff ag_diff;
+/* Bind a problem (copied: atoms, types, tables); opts->precision selects the
+ * FP32 kernels or their FP64 twin, opts->table_mode must be AG_TABLE_LINEAR. */
+ag_status   ag_diff_create(ag_context *ctx, const ag_problem *problem, const ag_opts *opts,
+                           ag_diff **out);
+/* Replace atom coordinates, charges and bond vectors (NULL keeps the current). */
+ag_status   ag_diff_set_atoms(ag_diff *d, const double *coord, const double *charge,
+                              const double *rvector, const double *rvector2);
+/* Compute all maps.  keep_closest_h = 1 reuses the closest DS/D1 atoms of the
+ * previous forward (0, or no previous forward: search them at the current
+ * coordinates, as main.cpp:2986-3015 does).  device_out: a device buffer of
+ * [n_maps][P] elements to write, or NULL for the object's own buffer.
+ * Returns when the maps are in place. */
+ag_status   ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out);
+const void *ag_diff_device_maps(const ag_diff *d);            /* own buffer     */
+ag_status   ag_diff_download(ag_diff *d, void *host_maps);     /* own buffer     */
+/* [P] file index of each point's closest DS/D1 atom (-1: none needed). */
+ag_status   ag_diff_closest_h(ag_diff *d, int32_t *host_out);
+/* Adjoint of the last forward for L with dL/d(maps) = grad_maps ([n_maps][P],
+ * device memory if grad_on_device, else host).  Writes dL/d(coord) through the
+ * pair terms only, dL/d(charge), dL/d(rvector), dL/d(rvector2) (FP64 host
+ * arrays, any may be NULL).  The bond vectors' own dependence on the
+ * coordinates is ag_job_bond_vectors_backward.  Pair terms are recomputed, not
+ * stored. */
+ag_status   ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_device,
+                             double *g_coord, double *g_charge, double *g_rvector,
+                             double *g_rvector2);
+/* Device times (ms) of the last forward (e map + short-range maps), of the
+ * last closest-H search and of the last backward. */
+ag_status   ag_diff_timing(const ag_diff *d, float *forward_ms, float *closest_h_ms,
+                           float *backward_ms);
+ag_status   ag_diff_destroy(ag_diff *d);
 
 /* Front / back end (replaces main.cpp:214-2776 and :3481-3565) ------------- */
 typedef struct ag_job ag_job;

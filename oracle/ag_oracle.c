@@ -300,3 +300,194 @@ int32_t ag_oracle_points(const ag_problem *p, int64_t n_pts, const int64_t *pt_i
     free(hb12); free(E); free(hbmin); free(hbmax); free(hbflag);
     return rc;
 }
+
+/*
+ * Differentiable (linear-table) mode, FP64: the same loop with every table
+ * read by linear interpolation, T(x) = T[b] + (x - b)(T[b+1] - T[b]),
+ * b = floor(x), constant past the last bin; LOOP 2 terms multiplied by
+ * w = min(1, NEINT - A_DIV r); Hramp evaluated for every D1 pair; the A2
+ * cos_theta < 0 branch scaled by (1 + sin(2 ti)/9).  closest_h: [n_pts]
+ * frozen closest DS/D1 atom per point, or NULL to search it as main.cpp:2986
+ * does.  This restates the mode from the reference loop (not from the GPU
+ * code), for the GPU parity tests of ag_diff_forward.
+ */
+static double lin_tab_f(const float *t, int n, double x)
+{
+    if (x <= 0) return t[0];
+    int b = (int)x;
+    if (b >= n - 1) return t[n - 1];
+    return (double)t[b] + (x - b) * ((double)t[b + 1] - (double)t[b]);
+}
+static double lin_tab_d(const double *t, int n, double x)
+{
+    if (x <= 0) return t[0];
+    int b = (int)x;
+    if (b >= n - 1) return t[n - 1];
+    return t[b] + (x - b) * (t[b + 1] - t[b]);
+}
+
+int32_t ag_oracle_points_lin(const ag_problem *p, int64_t n_pts, const int64_t *pt_index,
+                             const int32_t *closest_h, double *out)
+{
+    const int nA = p->n_atoms, nM = p->n_maps, nAM = p->n_atom_maps;
+    const int64_t n1x = p->n1[0], n1y = p->n1[1], n1z = p->n1[2];
+    const int64_t P = n1x * n1y * n1z;
+    const double ln_half = log(0.5);
+    if (nM <= 0 || nM > AG_MAX_MAPS || nAM < 0 || nAM > nM || (pt_index == NULL && n_pts != P))
+        return AG_ERR_INVALID;
+    int *hb12 = (int *)malloc(sizeof(int) * (nA > 0 ? nA : 1));
+    int nhb12 = 0;
+    for (int ia = 0; ia < nA; ia++)
+        if (p->hbond[ia] == 1 || p->hbond[ia] == 2) hb12[nhb12++] = ia;
+    double *E = (double *)malloc(sizeof(double) * nM);
+    double *hbmin = (double *)malloc(sizeof(double) * (nAM > 0 ? nAM : 1));
+    double *hbmax = (double *)malloc(sizeof(double) * (nAM > 0 ? nAM : 1));
+    char *hbflag = (char *)malloc(nAM > 0 ? nAM : 1);
+    double *sol_ext = (double *)malloc(sizeof(double) * (AG_NEINT + 1));
+    for (int b = 0; b <= AG_NEINT; b++) sol_ext[b] = p->sol_fn[b];
+    int32_t rc = 0;
+    for (int64_t ip = 0; ip < n_pts; ip++) {
+        int64_t lin = pt_index ? pt_index[ip] : ip;
+        if (lin < 0 || lin >= P) { rc = AG_ERR_INVALID; break; }
+        int ix = (int)(lin % n1x), iy = (int)((lin / n1x) % n1y), iz = (int)(lin / (n1x * n1y));
+        double c[3];
+        c[2] = ((double)(iz - p->ne[2])) * p->spacing;
+        c[1] = ((double)(iy - p->ne[1])) * p->spacing;
+        c[0] = ((double)(ix - p->ne[0])) * p->spacing;
+        for (int m = 0; m < nM; m++) E[m] = 0.0;
+        for (int j = 0; j < nAM; j++) if (p->map_is_covalent[j]) {
+            double d0 = p->cov_pos[0] - c[0], d1 = p->cov_pos[1] - c[1], d2 = p->cov_pos[2] - c[2];
+            double rcov = sqrt(d0 * d0 + d1 * d1 + d2 * d2) / p->cov_half_width;
+            if (rcov < O_APPROX_ZERO) rcov = O_APPROX_ZERO;
+            E[j] = p->cov_barrier * (1. - exp(ln_half * rcov * rcov));
+        }
+        for (int m = 0; m < nAM; m++) { hbmin[m] = 999999.; hbmax[m] = -999999.; hbflag[m] = 0; }
+        if (p->elec_map >= 0) {
+            double e = 0;
+            for (int ia = 0; ia < nA; ia++) {
+                const double *a = p->coord + 3 * ia;
+                double d0 = a[0] - c[0], d1 = a[1] - c[1], d2 = a[2] - c[2];
+                double r = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                if (r < O_APPROX_ZERO) r = O_APPROX_ZERO;
+                double T = p->dddiel ? lin_tab_d(p->r_epsilon_fn, AG_NDIEL, r * AG_A_DIV) : p->invdielcal;
+                e += p->charge[ia] * T * p->coeff_estat / dmax(r, 0.5);
+            }
+            E[p->elec_map] = e;
+        }
+        int closestH = -1;
+        if (nAM > 0) {
+            if (closest_h) {
+                closestH = closest_h[ip];
+            } else {
+                double rminH = 999999.;
+                for (int inh = 0; inh < nhb12; inh++) {
+                    const double *a = p->coord + 3 * hb12[inh];
+                    double d0 = a[0] - c[0], d1 = a[1] - c[1], d2 = a[2] - c[2];
+                    double r = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                    if (r < rminH) { rminH = r; closestH = hb12[inh]; }
+                }
+            }
+            if (closestH < 0) { rc = AG_ERR_NO_CLOSEST_H; break; }
+        }
+        if (nAM > 0 || p->dsolv_map >= 0) {
+            for (int ia = 0; ia < nA; ia++) {
+                const double *a = p->coord + 3 * ia;
+                const double *rv = p->rvector + 3 * ia;
+                const double *rv2 = p->rvector2 + 3 * ia;
+                double d[3], dnorm[3];
+                for (int i = 0; i < 3; i++) d[i] = a[i] - c[i];
+                double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                if (r > O_SOFTNBC) continue;
+                if (p->disorder_h && p->disorder[ia] && p->rec_type[ia] == p->hydrogen_type) continue;
+                if (r < O_APPROX_ZERO) r = O_APPROX_ZERO;
+                for (int i = 0; i < 3; i++) dnorm[i] = d[i] / r;
+                const double x = r * AG_A_DIV;
+                const double w = dmin(1.0, AG_NEINT - x);
+                const double sol = lin_tab_d(sol_ext, AG_NEINT + 1, x);
+                double racc = 1., rdon = 1., Hramp = 1.;
+                const int hb = p->hbond[ia];
+                double cos_theta = 0.;
+                for (int i = 0; i < 3; i++) cos_theta -= dnorm[i] * rv[i];
+                if (hb == 2) {
+                    if (cos_theta <= 0.) racc = 0.;
+                    else if (p->rexp[ia] == 2) racc = cos_theta * cos_theta;
+                    else if (p->rexp[ia] == 4) racc = pow(cos_theta, 4.);
+                    else racc = cos_theta;
+                    if (ia != closestH) {
+                        const double *rvh = p->rvector + 3 * closestH;
+                        double ct = rvh[0] * rv[0] + rvh[1] * rv[1] + rvh[2] * rv[2];
+                        ct = dmax(dmin(ct, 1.0), -1.0);
+                        Hramp = 0.5 - 0.5 * cos(acos(ct) * 120. / 90.);
+                    }
+                } else if (hb == 4) {
+                    rdon = (cos_theta <= 0.) ? 0. : cos_theta * cos_theta;
+                } else if (hb == 5 && !p->disorder[ia]) {
+                    double t0 = 0.;
+                    for (int i = 0; i < 3; i++) t0 += dnorm[i] * rv2[i];
+                    t0 = dmax(dmin(t0, 1.), -1.);
+                    t0 = O_PI / 2. - acos(t0);
+                    double cr[3];
+                    cr[0] = dnorm[1] * rv2[2] - dnorm[2] * rv2[1];
+                    cr[1] = dnorm[2] * rv2[0] - dnorm[0] * rv2[2];
+                    cr[2] = dnorm[0] * rv2[1] - dnorm[1] * rv2[0];
+                    double rd2 = dmax(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2], O_APPROX_ZERO);
+                    double ti = 0.;
+                    for (int i = 0; i < 3; i++) ti += cr[i] / sqrt(rd2) * rv[i];
+                    ti = dmax(dmin(ti, 1.), -1.);
+                    ti = fabs(acos(ti) - O_PI / 2.);
+                    if (cos_theta >= 0.) rdon = (0.9 + 0.1 * sin(ti + ti)) * cos(t0);
+                    else if (cos_theta >= -0.34202)
+                        rdon = 562.25 * pow(0.116978 - cos_theta * cos_theta, 3.) * cos(t0) * (1. + sin(ti + ti) / 9.);
+                    else rdon = 0.;
+                } else if (hb == 5) {
+                    double ct = dmax(dmin(cos_theta, 1.), -1.);
+                    double theta = acos(ct);
+                    racc = rdon = (theta <= 1.24791 + O_PI / 2.) ? pow(cos(theta - 1.24791), 4.) : 0.;
+                }
+                const int ta = p->rec_type[ia];
+                for (int m = 0; m < nAM; m++) {
+                    if (p->map_is_covalent[m]) continue;
+                    const float *row = p->e_vdw_hb + ((size_t)ta * nAM + m) * AG_NEINT;
+                    double T = lin_tab_f(row, AG_NEINT, x);
+                    double rsph = dmin(dmax(T / 100., 0.), 1.);
+                    const float *hrow = p->hydrogen_type >= 0
+                        ? p->e_vdw_hb + ((size_t)p->hydrogen_type * nAM + m) * AG_NEINT : NULL;
+                    double TH = hrow ? lin_tab_f(hrow, AG_NEINT, (r - 1.10) * AG_A_DIV) : 0.;
+                    if (p->map_is_hbonder[m]) {
+                        const int mh = p->map_hbond[m];
+                        if ((mh == 3 || mh == 5 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) {
+                            E[m] += w * (p->disorder[ia] ? TH : T) * Hramp * (racc + (1. - racc) * rsph);
+                        } else if ((mh == 4 || mh == 6) && (hb == 1 || hb == 2 || hb == 6)) {
+                            double v = w * T * (racc + (1. - racc) * rsph);
+                            hbmin[m] = dmin(hbmin[m], v);
+                            hbmax[m] = dmax(hbmax[m], v);
+                            hbflag[m] = 1;
+                        } else if ((mh == 1 || mh == 2 || mh == 6) && (hb > 2 || hb == 6)) {
+                            if (p->disorder[ia]) {
+                                E[m] += w * TH * Hramp * (rdon + (1. - rdon) * rsph);
+                            } else {
+                                double v = w * T * (rdon + (1. - rdon) * rsph);
+                                hbmin[m] = dmin(hbmin[m], v);
+                                hbmax[m] = dmax(hbmax[m], v);
+                                hbflag[m] = 1;
+                            }
+                        } else {
+                            E[m] += w * T;
+                        }
+                    } else {
+                        E[m] += w * T;
+                    }
+                    if (p->separate_desolvation_maps) m++;
+                    E[m] += w * sol * (p->map_solpar_probe[m] * p->vol[ia] +
+                                       (p->solpar[ia] + p->solpar_q * fabs(p->charge[ia])) * p->map_vol_probe[m]);
+                }
+                if (p->dsolv_map >= 0) E[p->dsolv_map] += w * p->solpar_q * p->vol[ia] * sol;
+            }
+            for (int m = 0; m < nAM; m++)
+                if (hbflag[m]) E[m] += (hbmin[m] + dmax(hbmax[m], 0));
+        }
+        for (int m = 0; m < nM; m++) out[(size_t)m * n_pts + ip] = E[m];
+    }
+    free(hb12); free(E); free(hbmin); free(hbmax); free(hbflag); free(sol_ext);
+    return rc;
+}

@@ -40,6 +40,9 @@ def lib() -> C.CDLL:
         _lib = C.CDLL(str(ORACLE_LIB))
         _lib.ag_oracle_points.restype = C.c_int32
         _lib.ag_oracle_points.argtypes = [C.POINTER(ag_problem), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.ag_oracle_points_lin.restype = C.c_int32
+        _lib.ag_oracle_points_lin.argtypes = [C.POINTER(ag_problem), C.c_int64, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]
     return _lib
 
 
@@ -61,6 +64,30 @@ def oracle_points(problem, points: np.ndarray | None = None):
     if rc != 0:
         raise RuntimeError(f"oracle returned status {rc}")
     return out, flags
+
+
+def oracle_points_lin(problem, points: np.ndarray | None = None, closest_h: np.ndarray | None = None):
+    """FP64 energies of the differentiable (linear-table) mode at `points`
+    (linear indices; None = all), with the closest DS/D1 atom of each point
+    frozen to closest_h (per point; None = searched).  Returns maps[n_maps, n_pts]."""
+    s = problem.struct()
+    if points is None:
+        n = problem.points
+        idx_ptr = None
+    else:
+        points = np.ascontiguousarray(points, dtype=np.int64)
+        n = int(points.shape[0])
+        idx_ptr = points.ctypes.data_as(C.c_void_p)
+    ch_ptr = None
+    if closest_h is not None:
+        closest_h = np.ascontiguousarray(closest_h, dtype=np.int32)
+        assert closest_h.shape[0] == n
+        ch_ptr = closest_h.ctypes.data_as(C.c_void_p)
+    out = np.zeros((problem.n_maps, n), dtype=np.float64)
+    rc = lib().ag_oracle_points_lin(C.byref(s), n, idx_ptr, ch_ptr, out.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise RuntimeError(f"oracle returned status {rc}")
+    return out
 
 
 def read_map(path: str | Path) -> np.ndarray:
