@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-ensemble comparison")
     ap.add_argument("--batch-instances", type=int, default=256)
+    ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-mode measurement")
     return ap.parse_args()
 
 
@@ -253,6 +254,8 @@ def main():
         }
         if not args.no_batch and world == 1:
             line["batched"] = batched_ensemble(ctx, args.batch_instances, work, stream)
+        if not args.no_diff and world == 1:
+            line["differentiable"] = differentiable_maps(ctx, work, stream)
         if not args.no_cpu_baseline and world == 1:
             threads = min(32, os.cpu_count() or 1)
             res = reference_sample(rec, spec, work, threads)
@@ -340,6 +343,87 @@ def batched_ensemble(ctx, n, work: Path, stream):
             "plain_per_box_ms": plain_ms, "plain_per_box_evals_per_s": evals / (plain_ms * 1e-3),
             "speedup_vs_plain_per_box": plain_ms / batch_ms, "max_diff_over_tolerance": worst,
             "create_s": create_s, "tuning": tune}
+
+
+def differentiable_maps(ctx, work: Path, stream, reps: int = 10):
+    """The differentiable form: 4,000-atom receptor (same generator), npts
+    60^3, 8 maps, linear-table mode.  Forward and adjoint device times of the
+    FP32 kernels (ag_diff_timing events; L2 flushed before each), the
+    end-to-end forward + backward through the torch.autograd binding, and the
+    gradient checks of autogrid_b200.gradcheck on 64 random atoms for
+    L = sum(w * maps), w ~ N(0, 1)."""
+    import torch
+    from autogrid_b200 import Diff, Job, gradcheck, synth
+    from autogrid_b200.torch_maps import GridMaps
+    d = work / "diff"
+    rec = synth.make_receptor(4000, seed=7, center=(0.0, 0.0, 0.0))
+    spec = synth.GridSpec(npts=(60, 60, 60))
+    g = synth.write_case(d, "c3", rec, spec)
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        job = Job(g.name, None)
+    finally:
+        os.chdir(cwd)
+    prob = job.problem()
+    P, M = prob.points, prob.n_maps
+    rng = np.random.default_rng(0)
+    w = rng.normal(size=prob.map_shape)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    df = Diff(ctx, prob, "fp32")
+    w32 = w.astype(np.float32)
+    df.forward()
+    ch_ms = df.timing()[1]
+    df.backward(w32)
+    fw, bw = [], []
+    for _ in range(reps):
+        flush.zero_(); torch.cuda.synchronize()
+        df.forward(keep_closest_h=True)
+        fw.append(df.timing()[0])
+        flush.zero_(); torch.cuda.synchronize()
+        df.backward(w32)
+        bw.append(df.timing()[2])
+    df.close()
+    fwd_ms, bwd_ms = float(np.median(fw)), float(np.median(bw))
+    # end to end through torch: host coordinates in, gradients out
+    fn = GridMaps(job, device=torch.cuda.current_device(), precision="fp32")
+    wt = torch.tensor(w32, device="cuda")
+    coords0 = torch.tensor(prob.arrays["coord"].reshape(-1, 3))
+    charges0 = torch.tensor(prob.arrays["charge"])
+    e2e = []
+    for k in range(reps + 1):
+        c = coords0.clone().requires_grad_(True)
+        q = charges0.clone().requires_grad_(True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = (wt * fn(c, q)).sum()
+        loss.backward()
+        torch.cuda.synchronize()
+        if k:
+            e2e.append(time.perf_counter() - t0)
+    atoms = rng.choice(prob.n_atoms, 64, replace=False)
+    hs = (1e-3, 1e-5)
+    chk = gradcheck.check(job, prob, ctx, atoms, w, h_coord=hs)
+    return {
+        "workload": "diff_4000_61cube_8maps", "atoms": prob.n_atoms, "points": P, "maps": M,
+        "tables": "linear interpolation between bins (AG_TABLE_LINEAR)", "dtype": "f32 (FP64 twin as error oracle)",
+        "forward_ms": fwd_ms, "backward_ms": bwd_ms, "adjoint_over_forward": bwd_ms / fwd_ms,
+        "closest_h_search_ms": ch_ms,
+        "forward_evals_per_s": P * M / (fwd_ms * 1e-3),
+        "e2e_torch_forward_backward_ms": float(np.median(e2e)) * 1e3,
+        "gradcheck": {
+            "atoms_checked": len(atoms), "loss": "sum(w * maps), w ~ N(0,1) seeded",
+            "h_charge": chk["h_charge"], "h_coord": list(hs),
+            "fp32_vs_fp64_adjoint_coord": chk["fp32_vs_fp64_coord"],
+            "fp32_vs_fp64_adjoint_charge": chk["fp32_vs_fp64_charge"],
+            "fp64_adjoint_vs_fd_charge": chk["fp64_vs_fd_charge"],
+            "fp32_adjoint_vs_fd_charge": chk["fp32_vs_fd_charge"],
+            "fp64_adjoint_vs_fd_coord": {str(h): chk["fp64_vs_fd_coord"][h] for h in hs},
+            "fp32_adjoint_vs_fd_coord": {str(h): chk["fp32_vs_fd_coord"][h] for h in hs},
+            "error_norm": "||a - b||_2 / ||b||_2 over the checked components",
+            "seconds": chk["fd_seconds"],
+        },
+    }
 
 
 def far_kernel_ms(ctx, plan, stream, steps):

@@ -4,8 +4,12 @@
   mode (oracle/ag_oracle.c ag_oracle_points_lin) to 1e-9, the FP32 kernels to
   the drop-in parity bar; closest DS/D1 atoms vs the reference's search;
 * adjoint: FP64 adjoint vs central differences of the FP64 forward
-  (h = 1e-3 A on coordinates, 1e-4 e on charges, closest hydrogens and bonded
-  neighbours frozen), FP32 adjoint vs FP64 adjoint;
+  (1e-4 e on charges; 1e-3 down to 1e-6 A on coordinates, closest hydrogens
+  and bonded neighbours frozen), FP32 adjoint vs FP64 adjoint.  The tables
+  are piecewise linear over bins of 1/128 A, so a coordinate step straddles
+  slope kinks of the loss; each straddled kink adds a finite-difference error
+  of fixed size and their number grows with h, so the agreement is asserted
+  to tighten as h shrinks;
 * the torch.autograd binding returns the same gradients as the C ABI.
 """
 import numpy as np
@@ -94,9 +98,15 @@ def test_adjoint_matches_central_differences(tmp_path, gpu_ctx, name):
     half = np.array(prob.ne) * prob.scalars["spacing"]
     near_box = np.flatnonzero(np.all(np.abs(c) < half + 4.0, axis=1))
     atoms = rng.choice(near_box, 16, replace=False)
-    r = gradcheck.check(job, prob, gpu_ctx, atoms, w)
+    hs = (1e-3, 1e-4, 1e-5, 1e-6)
+    r = gradcheck.check(job, prob, gpu_ctx, atoms, w, h_coord=hs)
+    err = r["fp64_vs_fd_coord"]
+    print({h: f"{e:.3g}" for h, e in err.items()}, r["fp64_vs_fd_charge"], r["fp32_vs_fp64_coord"])
     assert r["fp64_vs_fd_charge"] < 1e-6, r["fp64_vs_fd_charge"]
-    assert r["fp64_vs_fd_coord"] < 1e-3, r["fp64_vs_fd_coord"]
+    # table kinks every 1/128 A: the finite-difference error falls with h
+    assert err[1e-6] < 1e-4, err
+    assert err[1e-5] < 1e-3, err
+    assert err[1e-3] < 2e-2, err
     assert r["fp32_vs_fp64_coord"] < 1e-3, r["fp32_vs_fp64_coord"]
     assert r["fp32_vs_fp64_charge"] < 1e-3, r["fp32_vs_fp64_charge"]
 
@@ -116,7 +126,7 @@ def test_torch_binding_matches_c_abi(tmp_path, gpu_ctx):
     (w * maps).sum().backward()
     d = Diff(gpu_ctx, prob, "fp64")
     d.forward()
-    np.testing.assert_allclose(maps.cpu().numpy(), d.maps(), rtol=0, atol=0)
+    np.testing.assert_allclose(maps.detach().cpu().numpy(), d.maps(), rtol=0, atol=0)
     gc, gq = gradcheck.full_gradient(job, d, prob.arrays["coord"].reshape(-1, 3), w.cpu().numpy())
     np.testing.assert_allclose(coords.grad.numpy(), gc, rtol=1e-9, atol=1e-9)
     np.testing.assert_allclose(charges.grad.numpy(), gq, rtol=1e-9, atol=1e-9)
