@@ -105,10 +105,15 @@ SIGNATURES = {
     "ag_job_write_maps_f64": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ag_job_fail": (None, [C.c_void_p, C.c_char_p]),
     "ag_job_free": (None, [C.c_void_p]),
+    "ag_job_vina_problem": (C.c_int32, [C.c_void_p, C.POINTER(C.POINTER(ag_problem))]),
     "ag_job_bond_vectors": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_job_bond_vectors_backward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_diff_create": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),
+    "ag_diff_create_batch": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_int32,
+                                       C.POINTER(C.c_void_p)]),
+    "ag_diff_conformers": (C.c_int32, [C.c_void_p]),
     "ag_diff_set_atoms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_diff_set_conformer": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_diff_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "ag_diff_device_maps": (C.c_void_p, [C.c_void_p]),
     "ag_diff_download": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -158,6 +158,13 @@ class Job:
             m = np.ascontiguousarray(m, dtype=np.float32)
             check(self._lib.ag_job_write_maps_f32(self._h, m.ctypes.data_as(C.c_void_p)))
 
+    def vina_problem(self) -> Problem:
+        """The job with Vina-potential tables (ag_job_vina_problem): atom maps
+        only, plain sums, no desolvation."""
+        out = C.POINTER(ag_problem)()
+        check(self._lib.ag_job_vina_problem(self._h, C.byref(out)))
+        return Problem.from_struct(out.contents)
+
     def bond_vectors(self, coord: np.ndarray | None = None) -> tuple:
         """(rvector, rvector2) [N,3] at coord [N,3] (centred frame), with the
         bonded neighbours found at load time (ag_job_bond_vectors)."""
@@ -251,20 +258,24 @@ class Context:
 class Diff:
     """Differentiable mode (ag_diff_*): maps with linearly interpolated tables
     and their hand-written adjoint.  Arrays are FP64 numpy in the problem's
-    centred frame; maps and map gradients are in the chosen precision."""
+    centred frame; maps and map gradients are in the chosen precision.  With
+    conformers > 1 the object holds that many coordinate sets of the receptor,
+    evaluated together; maps, closest-H indices and gradients gain a leading
+    conformer axis."""
 
-    def __init__(self, ctx: Context, problem: Problem, precision: str = "fp32"):
+    def __init__(self, ctx: Context, problem: Problem, precision: str = "fp32", conformers: int = 1):
         self.ctx = ctx
         self.problem = problem
         self._lib = ctx._lib
         prec = _PREC[precision]
         self.dtype = np.float64 if prec == _abi.AG_PREC_FP64 else np.float32
-        self.shape = problem.map_shape
+        self.conformers = int(conformers)
+        self.shape = problem.map_shape if self.conformers == 1 else (self.conformers,) + problem.map_shape
         self.n_atoms = problem.n_atoms
         opts = ag_opts(precision=prec, table_mode=_abi.AG_TABLE_LINEAR)
         s = problem.struct()
         h = C.c_void_p()
-        check(self._lib.ag_diff_create(ctx._h, C.byref(s), C.byref(opts), C.byref(h)))
+        check(self._lib.ag_diff_create_batch(ctx._h, C.byref(s), C.byref(opts), self.conformers, C.byref(h)))
         self._h = h
 
     @staticmethod
@@ -275,13 +286,13 @@ class Diff:
         arr = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
         return arr, arr.ctypes.data_as(C.c_void_p)
 
-    def set_atoms(self, coord=None, charge=None, rvector=None, rvector2=None) -> None:
+    def set_atoms(self, coord=None, charge=None, rvector=None, rvector2=None, conformer: int = 0) -> None:
         n = self.n_atoms
         c, pc = self._ptr(coord, n, 3)
         q, pq = self._ptr(charge, n)
         r1, p1 = self._ptr(rvector, n, 3)
         r2, p2 = self._ptr(rvector2, n, 3)
-        check(self._lib.ag_diff_set_atoms(self._h, pc, pq, p1, p2))
+        check(self._lib.ag_diff_set_conformer(self._h, int(conformer), pc, pq, p1, p2))
 
     def forward(self, keep_closest_h: bool = False, device_out: int | None = None) -> None:
         """Compute the maps (into device_out, a device pointer, or the object's buffer)."""
@@ -294,16 +305,19 @@ class Diff:
         return out
 
     def closest_h(self) -> np.ndarray:
-        out = np.empty(int(np.prod(self.shape[1:])), dtype=np.int32)
+        P = int(np.prod(self.problem.map_shape[1:]))
+        out = np.empty(P * self.conformers, dtype=np.int32)
         check(self._lib.ag_diff_closest_h(self._h, out.ctypes.data_as(C.c_void_p)))
-        return out
+        return out if self.conformers == 1 else out.reshape(self.conformers, P)
 
     def backward(self, grad_maps=None, device_ptr: int | None = None) -> dict:
         """Adjoint of the last forward for dL/d(maps) given as a host array or a
         device pointer.  Returns FP64 dL/d(coord) (pair terms only), charge,
         rvector, rvector2."""
-        n = self.n_atoms
-        gc = np.zeros((n, 3)); gq = np.zeros(n); g1 = np.zeros((n, 3)); g2 = np.zeros((n, 3))
+        n, k = self.n_atoms, self.conformers
+        lead = () if k == 1 else (k,)
+        gc = np.zeros(lead + (n, 3)); gq = np.zeros(lead + (n,))
+        g1 = np.zeros(lead + (n, 3)); g2 = np.zeros(lead + (n, 3))
         if device_ptr is not None:
             src, on_dev = C.c_void_p(int(device_ptr)), 1
         else:

@@ -62,11 +62,11 @@ struct ag_diff {
     int device = 0;
     bool fp64 = false;
     size_t esz = 4;
-    int N = 0, n_maps = 0, n_atom_maps = 0, elec = -1;
+    int N = 0, n_conf = 1, n_maps = 0, n_atom_maps = 0, elec = -1;
+    bool need_h = false;
     long long P = 0;
-    int n1[3] = {0, 0, 0}, ne[3] = {0, 0, 0};
-    double spacing = 0;
-    std::vector<double> coord, charge, rv, rv2;
+    size_t ncells = 0;
+    std::vector<double> coord, charge, rv, rv2;  // [conf][...]
     std::vector<int> h_index;
     DiffArgs args{};
     // device
@@ -79,7 +79,6 @@ struct ag_diff {
     cudaEvent_t ev[6] = {};
     float fwd_ms = 0, ch_ms = 0, bwd_ms = 0;
     bool have_ch = false, have_fwd = false;
-    const void *last_out = nullptr;
 
     ~ag_diff()
     {
@@ -98,7 +97,8 @@ struct ag_diff {
         }
         return e;
     }
-    ag_status upload_atoms();
+    size_t map_bytes() const { return esz * (size_t)P * n_maps * n_conf; }
+    ag_status upload_conformer(int k);
 };
 
 namespace {
@@ -137,21 +137,25 @@ template <class R> cudaError_t put(void **dst, const std::vector<R> &v, ag_diff 
     return cudaMemcpy(p, v.data(), v.size() * sizeof(R), cudaMemcpyHostToDevice);
 }
 
+bool act_uses_angles(uint8_t a) { return a != DA_PLAIN && a != DA_NONE; }
+bool act_uses_ramp(uint8_t a) { return a == DA_SUMA || a == DA_SUMA_DIS || a == DA_SUMD_DIS; }
+
 }  // namespace
 
-// Coordinates, charges, bond vectors and the cell list of the current atoms.
-ag_status ag_diff::upload_atoms()
+// Coordinates, charges, bond vectors and cell list of conformer k.
+ag_status ag_diff::upload_conformer(int k)
 {
+    const size_t o1 = (size_t)k * N, o3 = 3 * o1;
     std::vector<double> x(N), y(N), z(N);
-    for (int a = 0; a < N; a++) { x[a] = coord[3 * a]; y[a] = coord[3 * a + 1]; z[a] = coord[3 * a + 2]; }
+    for (int a = 0; a < N; a++) { x[a] = coord[o3 + 3 * a]; y[a] = coord[o3 + 3 * a + 1]; z[a] = coord[o3 + 3 * a + 2]; }
     // cell list over the grid box grown by DF_RADIUS; atoms outside it have no
     // point within the 8 A cutoff
-    std::vector<int> cell_of(N, -1), start((size_t)args.ncx * args.ncy * args.ncz + 1, 0);
+    std::vector<int> cell_of(N, -1), start(ncells + 1, 0);
+    const int nc[3] = {args.ncx, args.ncy, args.ncz};
     for (int a = 0; a < N; a++) {
         int c[3];
         bool in = true;
         const double pc[3] = {x[a], y[a], z[a]};
-        const int nc[3] = {args.ncx, args.ncy, args.ncz};
         for (int i = 0; i < 3; i++) {
             const double u = std::floor((pc[i] - args.cell0[i]) / args.cell_size);
             if (!(u >= 0 && u < nc[i])) { in = false; break; }
@@ -162,28 +166,34 @@ ag_status ag_diff::upload_atoms()
         start[cell_of[a] + 1]++;
     }
     for (size_t i = 1; i < start.size(); i++) start[i] += start[i - 1];
-    std::vector<int> fill(start.begin(), start.end() - 1), atoms(std::max(start.back(), 1));
+    std::vector<int> fill(start.begin(), start.end() - 1), atoms(std::max(N, 1), 0);
     for (int a = 0; a < N; a++)
         if (cell_of[a] >= 0) atoms[fill[cell_of[a]]++] = a;
     const size_t nb = (size_t)N * sizeof(double);
-    DF_CK(cudaMemcpyAsync(d_x, x.data(), nb, cudaMemcpyHostToDevice, stream));
-    DF_CK(cudaMemcpyAsync(d_y, y.data(), nb, cudaMemcpyHostToDevice, stream));
-    DF_CK(cudaMemcpyAsync(d_z, z.data(), nb, cudaMemcpyHostToDevice, stream));
-    DF_CK(cudaMemcpyAsync(d_q, charge.data(), nb, cudaMemcpyHostToDevice, stream));
-    DF_CK(cudaMemcpyAsync(d_rv, rv.data(), 3 * nb, cudaMemcpyHostToDevice, stream));
-    DF_CK(cudaMemcpyAsync(d_rv2, rv2.data(), 3 * nb, cudaMemcpyHostToDevice, stream));
-    DF_CK(cudaMemcpyAsync(d_cell_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
-    DF_CK(cudaMemcpyAsync(d_cell_atoms, atoms.data(), atoms.size() * sizeof(int), cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_x + o1, x.data(), nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_y + o1, y.data(), nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_z + o1, z.data(), nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_q + o1, charge.data() + o1, nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_rv + o3, rv.data() + o3, 3 * nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_rv2 + o3, rv2.data() + o3, 3 * nb, cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_cell_start + (size_t)k * (ncells + 1), start.data(), start.size() * sizeof(int),
+                          cudaMemcpyHostToDevice, stream));
+    DF_CK(cudaMemcpyAsync(d_cell_atoms + o1, atoms.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, stream));
     DF_CK(cudaStreamSynchronize(stream));  // host vectors are locals
     return AG_OK;
 }
 
 extern "C" {
 
-ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o, ag_diff **out)
+ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_opts *o, int32_t n_conformers,
+                               ag_diff **out)
 {
     if (!ctx || !p || !o || !out) { set_last_error("ag_diff_create: null argument"); return AG_ERR_INVALID; }
     *out = nullptr;
+    if (n_conformers < 1 || n_conformers > 4096) {
+        set_last_error("ag_diff_create_batch: n_conformers out of range [1, 4096]");
+        return AG_ERR_INVALID;
+    }
     if (o->table_mode != AG_TABLE_LINEAR) {
         set_last_error("ag_diff_create: opts->table_mode must be AG_TABLE_LINEAR");
         return AG_ERR_INVALID;
@@ -192,9 +202,11 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
         set_last_error("ag_diff_create: unknown precision");
         return AG_ERR_INVALID;
     }
-    ag_status st = validate_problem(p);
-    if (st != AG_OK) return st;
+    // the closest-hydrogen requirement is checked below, only if a map uses Hramp
+    ag_problem pv = *p;
     const int nAM = p->n_atom_maps;
+    ag_status st = validate_problem(&pv);
+    if (st != AG_OK && st != AG_ERR_NO_CLOSEST_H) return st;
     // Slots: every map but the e map.  The atom term of map m and the
     // desolvation target follow the reference's map loop (main.cpp:3286-3390):
     // a covalent map is skipped whole; with separate desolvation maps the
@@ -212,17 +224,22 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
         }
         desolv_of[dm] = 1;
     }
+    bool need_ang = false, need_h = false;
     for (int m = 0; m < nAM; m++) {
         Slot s;
         s.map = m;
         s.kind = p->map_is_covalent[m] ? DK_COV : DK_ATOM;  // covalent: Gaussian added at the end
         s.tab = tab_of[m];
-        s.desolv = desolv_of[m];
+        // a desolvation term with zero probe parameters adds exactly zero
+        s.desolv = desolv_of[m] && (p->map_solpar_probe[m] != 0.0 || p->map_vol_probe[m] != 0.0);
         if (s.tab >= 0)
             for (int dis = 0; dis < 2; dis++)
                 for (int hb = 0; hb < 8; hb++) {
-                    s.act[hb + 8 * dis] = action_of(p, s.tab, hb, dis);
-                    if (s.act[hb + 8 * dis] == DA_MMA || s.act[hb + 8 * dis] == DA_MMD) s.mm = true;
+                    const uint8_t a = action_of(p, s.tab, hb, dis);
+                    s.act[hb + 8 * dis] = a;
+                    if (a == DA_MMA || a == DA_MMD) s.mm = true;
+                    need_ang |= act_uses_angles(a);
+                    need_h |= act_uses_ramp(a);
                 }
         slots.push_back(s);
     }
@@ -232,6 +249,7 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
         s.kind = DK_D;
         slots.push_back(s);
     }
+    if (need_h && st == AG_ERR_NO_CLOSEST_H) return st;
     std::stable_partition(slots.begin(), slots.end(), [](const Slot &s) { return s.mm; });
     const int n_mm = (int)std::count_if(slots.begin(), slots.end(), [](const Slot &s) { return s.mm; });
     if ((int)slots.size() > DF_MAXS || n_mm > DF_MAXMM) {
@@ -249,21 +267,26 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
     d->fp64 = o->precision == AG_PREC_FP64;
     d->esz = d->fp64 ? sizeof(double) : sizeof(float);
     d->N = p->n_atoms;
+    d->n_conf = n_conformers;
     d->n_maps = p->n_maps;
     d->n_atom_maps = nAM;
     d->elec = p->elec_map;
-    for (int i = 0; i < 3; i++) { d->n1[i] = p->n1[i]; d->ne[i] = p->ne[i]; }
-    d->spacing = p->spacing;
+    d->need_h = need_h;
     d->P = (long long)p->n1[0] * p->n1[1] * p->n1[2];
-    const int N = d->N;
-    d->coord.assign(p->coord, p->coord + 3 * (size_t)N);
-    d->charge.assign(p->charge, p->charge + N);
-    d->rv.assign(p->rvector, p->rvector + 3 * (size_t)N);
-    d->rv2.assign(p->rvector2, p->rvector2 + 3 * (size_t)N);
+    const int N = d->N, K = n_conformers;
+    for (int k = 0; k < K; k++) {
+        d->coord.insert(d->coord.end(), p->coord, p->coord + 3 * (size_t)N);
+        d->charge.insert(d->charge.end(), p->charge, p->charge + N);
+        d->rv.insert(d->rv.end(), p->rvector, p->rvector + 3 * (size_t)N);
+        d->rv2.insert(d->rv2.end(), p->rvector2, p->rvector2 + 3 * (size_t)N);
+    }
     std::vector<int> meta(std::max(N, 1), 0);
     for (int a = 0; a < N; a++) {
         const bool skip = p->disorder_h && p->disorder[a] && p->rec_type[a] == p->hydrogen_type;
-        meta[a] = (p->rec_type[a] & DM_TYPE_MASK) | (p->hbond[a] << DM_HB_SHIFT) | ((p->rexp[a] & 7) << DM_REXP_SHIFT) |
+        // without directional terms the hbond class changes nothing: drop it so
+        // the kernels skip the angular factors
+        const int hb = need_ang ? p->hbond[a] : 0;
+        meta[a] = (p->rec_type[a] & DM_TYPE_MASK) | (hb << DM_HB_SHIFT) | ((p->rexp[a] & 7) << DM_REXP_SHIFT) |
                   (p->disorder[a] ? DM_DIS : 0) | (skip ? DM_SKIP : 0);
         if (p->hbond[a] == 1 || p->hbond[a] == 2) d->h_index.push_back(a);
     }
@@ -275,6 +298,7 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
     A.nex = p->ne[0]; A.ney = p->ne[1]; A.nez = p->ne[2];
     A.P = d->P;
     A.spacing = p->spacing;
+    A.n_conf = K;
     A.disorder_h = p->disorder_h;
     A.hydrogen_type = p->hydrogen_type;
     A.n_rec_types = p->n_rec_types;
@@ -287,6 +311,7 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
     A.elec_map = p->elec_map;
     A.n_slots = (int)slots.size();
     A.n_mm = n_mm;
+    A.n_maps_out = p->n_maps;
     for (int s = 0; s < A.n_slots; s++) {
         const Slot &sl = slots[s];
         A.slot_map[s] = sl.map;
@@ -307,19 +332,19 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
         const int n = (int)std::ceil((hi - lo) / A.cell_size) + 1;
         if (i == 0) A.ncx = n; else if (i == 1) A.ncy = n; else A.ncz = n;
     }
-    const size_t ncells = (size_t)A.ncx * A.ncy * A.ncz;
+    d->ncells = (size_t)A.ncx * A.ncy * A.ncz;
+    const size_t NK = (size_t)N * K;
 
-    DF_CK(d->alloc(&d->d_x, N)); DF_CK(d->alloc(&d->d_y, N)); DF_CK(d->alloc(&d->d_z, N));
-    DF_CK(d->alloc(&d->d_q, N)); DF_CK(d->alloc(&d->d_vol, N)); DF_CK(d->alloc(&d->d_solpar, N));
-    DF_CK(d->alloc(&d->d_rv, 3 * (size_t)N)); DF_CK(d->alloc(&d->d_rv2, 3 * (size_t)N));
+    DF_CK(d->alloc(&d->d_x, NK)); DF_CK(d->alloc(&d->d_y, NK)); DF_CK(d->alloc(&d->d_z, NK));
+    DF_CK(d->alloc(&d->d_q, NK)); DF_CK(d->alloc(&d->d_vol, N)); DF_CK(d->alloc(&d->d_solpar, N));
+    DF_CK(d->alloc(&d->d_rv, 3 * NK)); DF_CK(d->alloc(&d->d_rv2, 3 * NK));
     DF_CK(d->alloc(&d->d_meta, N)); DF_CK(d->alloc(&d->d_h, d->h_index.size()));
-    DF_CK(d->alloc(&d->d_cell_start, ncells + 1)); DF_CK(d->alloc(&d->d_cell_atoms, N));
-    DF_CK(d->alloc(&d->d_ch, d->P)); DF_CK(d->alloc(&d->d_mmarg, 2 * (size_t)std::max(n_mm, 1) * d->P));
-    DF_CK(d->alloc(&d->d_grad, 10 * (size_t)N));
+    DF_CK(d->alloc(&d->d_cell_start, (d->ncells + 1) * K)); DF_CK(d->alloc(&d->d_cell_atoms, NK));
+    DF_CK(d->alloc(&d->d_ch, (size_t)d->P * K));
+    DF_CK(d->alloc(&d->d_mmarg, 2 * (size_t)n_mm * d->P * K));
+    DF_CK(d->alloc(&d->d_grad, 10 * NK));
     unsigned char *mp = nullptr;
-    DF_CK(d->alloc(&mp, d->esz * d->P * d->n_maps)); d->d_maps = mp;
-    unsigned char *gp = nullptr;
-    DF_CK(d->alloc(&gp, d->esz * d->P * d->n_maps)); d->d_gmaps = gp;
+    DF_CK(d->alloc(&mp, d->map_bytes())); d->d_maps = mp;
     DF_CK(cudaMemcpy(d->d_vol, p->vol, N * sizeof(double), cudaMemcpyHostToDevice));
     DF_CK(cudaMemcpy(d->d_solpar, p->solpar, N * sizeof(double), cudaMemcpyHostToDevice));
     DF_CK(cudaMemcpy(d->d_meta, meta.data(), N * sizeof(int), cudaMemcpyHostToDevice));
@@ -338,27 +363,41 @@ ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o,
     A.rv = d->d_rv; A.rv2 = d->d_rv2; A.meta = d->d_meta; A.h_index = d->d_h;
     A.cell_start = d->d_cell_start; A.cell_atoms = d->d_cell_atoms;
     for (auto &e : d->ev) DF_CK(cudaEventCreate(&e));
-    st = d->upload_atoms();
-    if (st != AG_OK) return st;
+    for (int k = 0; k < K; k++) {
+        st = d->upload_conformer(k);
+        if (st != AG_OK) return st;
+    }
     *out = d.release();
     return AG_OK;
 }
 
-ag_status ag_diff_set_atoms(ag_diff *d, const double *coord, const double *charge, const double *rvector,
-                            const double *rvector2)
+ag_status ag_diff_create(ag_context *ctx, const ag_problem *p, const ag_opts *o, ag_diff **out)
 {
-    if (!d) { set_last_error("ag_diff_set_atoms: null argument"); return AG_ERR_INVALID; }
-    const size_t N = d->N;
+    return ag_diff_create_batch(ctx, p, o, 1, out);
+}
+
+ag_status ag_diff_set_conformer(ag_diff *d, int32_t k, const double *coord, const double *charge,
+                                const double *rvector, const double *rvector2)
+{
+    if (!d) { set_last_error("ag_diff_set_conformer: null argument"); return AG_ERR_INVALID; }
+    if (k < 0 || k >= d->n_conf) { set_last_error("ag_diff_set_conformer: conformer out of range"); return AG_ERR_INVALID; }
+    const size_t N = d->N, o1 = (size_t)k * N, o3 = 3 * o1;
     for (size_t i = 0; coord && i < 3 * N; i++)
         if (!std::isfinite(coord[i])) { set_last_error("ag_diff_set_atoms: non-finite coordinate"); return AG_ERR_INVALID; }
     for (size_t i = 0; charge && i < N; i++)
         if (!std::isfinite(charge[i])) { set_last_error("ag_diff_set_atoms: non-finite charge"); return AG_ERR_INVALID; }
     DF_CK(cudaSetDevice(d->device));
-    if (coord) d->coord.assign(coord, coord + 3 * N);
-    if (charge) d->charge.assign(charge, charge + N);
-    if (rvector) d->rv.assign(rvector, rvector + 3 * N);
-    if (rvector2) d->rv2.assign(rvector2, rvector2 + 3 * N);
-    return d->upload_atoms();
+    if (coord) std::copy(coord, coord + 3 * N, d->coord.begin() + o3);
+    if (charge) std::copy(charge, charge + N, d->charge.begin() + o1);
+    if (rvector) std::copy(rvector, rvector + 3 * N, d->rv.begin() + o3);
+    if (rvector2) std::copy(rvector2, rvector2 + 3 * N, d->rv2.begin() + o3);
+    return d->upload_conformer(k);
+}
+
+ag_status ag_diff_set_atoms(ag_diff *d, const double *coord, const double *charge, const double *rvector,
+                            const double *rvector2)
+{
+    return ag_diff_set_conformer(d, 0, coord, charge, rvector, rvector2);
 }
 
 ag_status ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out)
@@ -372,7 +411,7 @@ ag_status ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out)
     bool timed_search = false;
     if (search) {
         d->have_ch = false;
-        if (d->n_atom_maps > 0) {
+        if (d->need_h) {
             if (A.n_h == 0) {
                 set_last_error("no closestH atom was found");  // main.cpp:3011-3014
                 return AG_ERR_NO_CLOSEST_H;
@@ -381,8 +420,8 @@ ag_status ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out)
             DF_CK(launch_closest_h(A, d->d_ch, s));
             DF_CK(cudaEventRecord(d->ev[5], s));
             timed_search = true;
-        } else {
-            DF_CK(cudaMemsetAsync(d->d_ch, 0xff, sizeof(int) * d->P, s));
+        } else {  // no map reads Hramp
+            DF_CK(cudaMemsetAsync(d->d_ch, 0xff, sizeof(int) * (size_t)d->P * d->n_conf, s));
         }
     }
     DF_CK(cudaEventRecord(d->ev[0], s));
@@ -395,7 +434,6 @@ ag_status ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out)
     if (timed_search) DF_CK(cudaEventElapsedTime(&d->ch_ms, d->ev[4], d->ev[5]));
     d->have_ch = true;
     d->have_fwd = true;
-    d->last_out = out;
     return AG_OK;
 }
 
@@ -405,7 +443,7 @@ ag_status ag_diff_download(ag_diff *d, void *host_maps)
 {
     if (!d || !host_maps) { set_last_error("ag_diff_download: null argument"); return AG_ERR_INVALID; }
     DF_CK(cudaSetDevice(d->device));
-    DF_CK(cudaMemcpyAsync(host_maps, d->d_maps, d->esz * d->P * d->n_maps, cudaMemcpyDeviceToHost, d->stream));
+    DF_CK(cudaMemcpyAsync(host_maps, d->d_maps, d->map_bytes(), cudaMemcpyDeviceToHost, d->stream));
     DF_CK(cudaStreamSynchronize(d->stream));
     return AG_OK;
 }
@@ -415,7 +453,8 @@ ag_status ag_diff_closest_h(ag_diff *d, int32_t *host_out)
     if (!d || !host_out) { set_last_error("ag_diff_closest_h: null argument"); return AG_ERR_INVALID; }
     if (!d->have_ch) { set_last_error("ag_diff_closest_h: no forward yet"); return AG_ERR_INVALID; }
     DF_CK(cudaSetDevice(d->device));
-    DF_CK(cudaMemcpyAsync(host_out, d->d_ch, sizeof(int) * d->P, cudaMemcpyDeviceToHost, d->stream));
+    DF_CK(cudaMemcpyAsync(host_out, d->d_ch, sizeof(int) * (size_t)d->P * d->n_conf, cudaMemcpyDeviceToHost,
+                          d->stream));
     DF_CK(cudaStreamSynchronize(d->stream));
     return AG_OK;
 }
@@ -427,10 +466,15 @@ ag_status ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_de
     if (!d->have_fwd) { set_last_error("ag_diff_backward: no forward to differentiate"); return AG_ERR_INVALID; }
     DF_CK(cudaSetDevice(d->device));
     cudaStream_t s = d->stream;
-    const size_t N = d->N;
+    const size_t N = d->N, K = d->n_conf;
     const unsigned char *gm = (const unsigned char *)grad_maps;
     if (!grad_on_device) {
-        DF_CK(cudaMemcpyAsync(d->d_gmaps, grad_maps, d->esz * d->P * d->n_maps, cudaMemcpyHostToDevice, s));
+        if (!d->d_gmaps) {
+            unsigned char *gp = nullptr;
+            DF_CK(d->alloc(&gp, d->map_bytes()));
+            d->d_gmaps = gp;
+        }
+        DF_CK(cudaMemcpyAsync(d->d_gmaps, grad_maps, d->map_bytes(), cudaMemcpyHostToDevice, s));
         gm = (const unsigned char *)d->d_gmaps;
     }
     DiffGrads g;
@@ -438,15 +482,20 @@ ag_status ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_de
     g.q = d->d_grad + 3 * N;
     g.rv = d->d_grad + 4 * N;
     g.rv2 = d->d_grad + 7 * N;
-    DF_CK(cudaMemsetAsync(d->d_grad, 0, 10 * N * sizeof(double), s));
+    DF_CK(cudaMemsetAsync(d->d_grad, 0, 10 * N * K * sizeof(double), s));
     DF_CK(cudaEventRecord(d->ev[2], s));
     if (d->elec >= 0) DF_CK(launch_emap_lin_adj(d->fp64, d->args, d->d_eps, gm + d->esz * d->P * d->elec, g, s));
     DF_CK(launch_near_lin_adj(d->fp64, d->args, d->d_vdw, d->d_sol, gm, d->d_ch, d->d_mmarg, g, s));
     DF_CK(cudaEventRecord(d->ev[3], s));
-    if (g_coord) DF_CK(cudaMemcpyAsync(g_coord, g.xyz, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (g_charge) DF_CK(cudaMemcpyAsync(g_charge, g.q, N * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (g_rvector) DF_CK(cudaMemcpyAsync(g_rvector, g.rv, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (g_rvector2) DF_CK(cudaMemcpyAsync(g_rvector2, g.rv2, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    for (size_t k = 0; k < K; k++) {
+        const double *base = d->d_grad + 10 * N * k;
+        if (g_coord) DF_CK(cudaMemcpyAsync(g_coord + 3 * N * k, base, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (g_charge) DF_CK(cudaMemcpyAsync(g_charge + N * k, base + 3 * N, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (g_rvector)
+            DF_CK(cudaMemcpyAsync(g_rvector + 3 * N * k, base + 4 * N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (g_rvector2)
+            DF_CK(cudaMemcpyAsync(g_rvector2 + 3 * N * k, base + 7 * N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
     DF_CK(cudaStreamSynchronize(s));
     DF_CK(cudaEventElapsedTime(&d->bwd_ms, d->ev[2], d->ev[3]));
     return AG_OK;
@@ -460,6 +509,8 @@ ag_status ag_diff_timing(const ag_diff *d, float *forward_ms, float *closest_h_m
     if (backward_ms) *backward_ms = d->bwd_ms;
     return AG_OK;
 }
+
+int32_t ag_diff_conformers(const ag_diff *d) { return d ? d->n_conf : 0; }
 
 ag_status ag_diff_destroy(ag_diff *d)
 {

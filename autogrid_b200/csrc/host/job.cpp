@@ -227,6 +227,12 @@ struct Job {
     std::vector<int32_t> m_is_cov, m_is_hb, m_hbond;
     std::vector<double> m_solpar, m_vol;
     ag_problem prob{};
+    // Vina-potential image of the same job (built on request)
+    std::vector<float> vina_tab;
+    std::vector<int32_t> vina_is_hb;
+    std::vector<double> vina_zero;
+    ag_problem vina_prob{};
+    bool vina_built = false;
     bool finished = false;
 
     ~Job()
@@ -290,6 +296,7 @@ struct Job {
     void bond_vectors_backward(const double *xyz, const double *g_rv, const double *g_rv2, double *g_xyz) const;
     void build_disorder();
     void make_problem();
+    void build_vina_problem();
     void write_maps(const double *maps64, const float *maps32);
 };
 
@@ -1111,6 +1118,81 @@ void Job::build_disorder()
     }
 }
 
+// xs radii of read_parameter_library.cc:323-339 (an ADVINA-only table in the
+// reference); 1.8 for a type missing from it (:352-354).
+static double vina_xs_radius(const std::string &t)
+{
+    static const struct { const char *name; float value; } kXs[] = {
+        {"C", 1.9f}, {"A", 1.9f}, {"N", 1.8f}, {"NA", 1.8f}, {"NS", 1.8f}, {"O", 1.7f}, {"OA", 1.7f},
+        {"OS", 1.7f}, {"S", 2.0f}, {"SA", 2.0f}, {"P", 2.1f}, {"F", 1.5f}, {"Mg", 1.2f}};
+    for (const auto &e : kXs)
+        if (t == e.name) return (double)e.value;
+    return (double)1.8f;
+}
+
+// Vina-potential tables of main.cpp:2081-2126 (compiled out of the reference
+// build by use_vina_potential = FALSE, main.cpp:263), restated as written:
+// float weights, float table accumulating each term in turn, bin 0 left at
+// zero, no smoothing.  The terms act on the surface distance
+// d = r - (xs(receptor type) + xs(ligand type)): two Gaussians, d^2 repulsion
+// for d < 0, the H-bond step for hbonder pairs (d <= 0.7 adds the weight, and
+// -0.7 < d <= 0 subtracts (d/0.7) of it), and the hydrophobic step for pairs
+// that are hbonders neither way -- the second test reads gridmap[i].hbonder[ia]
+// with the receptor-type index i as a map index (main.cpp:2117), restated with
+// 0 where that map does not exist.
+// The problem keeps the job's atoms and grid; its maps are the atom maps only
+// (the reference skips the e and d maps and desolvation under Vina,
+// main.cpp:2968, :3379, :3391) and every pair term is a plain sum.
+void Job::build_vina_problem()
+{
+    if (vina_built) return;
+    if (separate_desolvation_maps) fatal("separate_desolvation_maps has no Vina counterpart", AG_ERR_UNSUPPORTED);
+    const double wt_gauss1 = (double)-0.035579f, wt_gauss2 = (double)-0.005156f;
+    const double wt_repulsion = (double)0.840245f, wt_hydrogen = (double)-0.587439f;
+    const double wt_hydrophobic = (double)-0.035069f;
+    const int nR = std::max(receptor_types_ct, 1), nAM = std::max(num_atom_maps, 1);
+    vina_tab.assign((size_t)nR * nAM * AG_NEINT, 0.0f);
+    for (int ia = 0; ia < num_atom_maps; ia++) {
+        const MapObj &g = gridmap[ia];
+        if (g.is_covalent) continue;
+        const double Rij = vina_xs_radius(ligand_types[ia]);
+        for (int i = 0; i < receptor_types_ct; i++) {
+            const float map_Rij = (float)vina_xs_radius(receptor_types[i]);
+            float *t = &vina_tab[((size_t)i * num_atom_maps + ia) * AG_NEINT];
+            const int alias = (i < num_maps && ia < AG_MAX_REC_TYPES) ? gridmap[i].hbonder[ia] : 0;
+            for (int k = 1; k < AG_NEINT; k++) {
+                const double r = angstrom(k);
+                const double d = r - (map_Rij + Rij);
+                double de = wt_gauss1 * std::exp(-std::pow(d / 0.5, 2)) + wt_gauss2 * std::exp(-std::pow((d - 3.) / 2., 2));
+                t[k] = (float)((double)t[k] + de);
+                if (d < 0) t[k] = (float)((double)t[k] + wt_repulsion * std::pow(d, 2));
+                if (g.hbonder[i] > 0) {
+                    if (d <= 0.7) t[k] = (float)((double)t[k] + 1 * wt_hydrogen);
+                    if ((-0.7 < d) && (d <= 0.)) t[k] = (float)((double)t[k] - (d / 0.7) * wt_hydrogen);
+                }
+                if (g.hbonder[i] == 0 && alias == 0) {
+                    de = 0.;
+                    if (d < 0.5) de = 1 * wt_hydrophobic;
+                    else if (d < 1.5) de = (0.5 - d) * wt_hydrophobic;
+                    t[k] = (float)((double)t[k] + de);
+                }
+            }
+        }
+    }
+    vina_is_hb.assign(nAM, 0);
+    vina_zero.assign(nAM, 0.0);
+    vina_prob = prob;
+    vina_prob.n_maps = num_atom_maps;
+    vina_prob.elec_map = -1;
+    vina_prob.dsolv_map = -1;
+    vina_prob.map_is_hbonder = vina_is_hb.data();
+    vina_prob.map_solpar_probe = vina_zero.data();
+    vina_prob.map_vol_probe = vina_zero.data();
+    vina_prob.e_vdw_hb = vina_tab.data();
+    vina_prob.separate_desolvation_maps = 0;
+    vina_built = true;
+}
+
 void Job::make_problem()
 {
     m_is_cov.assign(std::max(num_atom_maps, 1), 0);
@@ -1290,6 +1372,20 @@ void ag_job_fail(ag_job *job, const char *message)
 }
 
 void ag_job_free(ag_job *job) { delete job; }
+
+ag_status ag_job_vina_problem(ag_job *job, const ag_problem **out)
+{
+    if (!job || !out) { agb::set_last_error("ag_job_vina_problem: null argument"); return AG_ERR_INVALID; }
+    *out = nullptr;
+    try {
+        job->job.build_vina_problem();
+    } catch (const Fatal &f) {
+        agb::set_last_error(f.what());
+        return f.status;
+    }
+    *out = &job->job.vina_prob;
+    return AG_OK;
+}
 
 ag_status ag_job_bond_vectors(const ag_job *job, const double *coord, double *rvector, double *rvector2)
 {

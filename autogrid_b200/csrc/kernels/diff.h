@@ -47,24 +47,31 @@ enum : uint8_t {
 
 enum : int { DK_ATOM = 0, DK_D = 1, DK_COV = 2 };
 
+// Conformers.  n_conf coordinate sets of one receptor (same atoms, types,
+// tables and grid) are evaluated by one launch: per conformer k the arrays
+// marked [conf] below start at k times their per-conformer length (x, y, z, q:
+// N; rv, rv2: 3N; cell_start: ncells + 1; cell_atoms: N; maps: n_maps * P;
+// closest H: P; min/max atoms: 2 * n_mm * P; gradients: 10 N).
 struct DiffArgs {
     int n_atoms, n1x, n1y, n1z, nex, ney, nez;
     long long P;
     double spacing;
+    int n_conf;
     // atoms in file order, centred frame, FP64
-    const double *x, *y, *z, *q, *vol, *solpar, *rv, *rv2;  // rv, rv2: [3N]
+    const double *x, *y, *z, *q, *rv, *rv2;  // [conf]; rv, rv2: [3N]
+    const double *vol, *solpar;
     const int *meta;          // type | hbond << 5 | rexp << 8 | disorder << 11 | skip << 12
     int disorder_h, hydrogen_type, n_rec_types, n_atom_maps;
     double solpar_q;
     // DS/D1 atoms (hbond 1 or 2) in file order
     int n_h;
     const int *h_index;
-    // cell list over the grid box grown by DF_RADIUS
+    // cell list over the grid box grown by DF_RADIUS, [conf]
     int ncx, ncy, ncz;
     double cell0[3], cell_size;
     const int *cell_start, *cell_atoms;
-    // slots: every map except the e map
-    int n_slots, n_mm;
+    // slots: every map except the e map; maps per conformer in the output
+    int n_slots, n_mm, n_maps_out;
     int slot_map[DF_MAXS];       // output map index
     int slot_kind[DF_MAXS];      // DK_*
     int slot_tab[DF_MAXS];       // atom-map index of the pair term (-1: none)
@@ -85,8 +92,30 @@ constexpr int DM_DIS = 1 << 11, DM_SKIP = 1 << 12;
 template <class R> struct R2 { R v, d; };
 
 struct DiffGrads {
-    double *xyz, *q, *rv, *rv2;  // [3N], [N], [3N], [3N]
+    double *xyz, *q, *rv, *rv2;  // [3N], [N], [3N], [3N] of conformer 0; stride 10N
 };
+
+// Per-conformer views of the [conf] arrays.
+struct ConfView {
+    const double *x, *y, *z, *q, *rv, *rv2;
+    const int *cell_start, *cell_atoms;
+    DiffGrads g;
+};
+__host__ __device__ inline ConfView conf_view(const DiffArgs &a, DiffGrads g, int k)
+{
+    const long long N = a.n_atoms, nc = (long long)a.ncx * a.ncy * a.ncz + 1;
+    ConfView v;
+    v.x = a.x + k * N; v.y = a.y + k * N; v.z = a.z + k * N; v.q = a.q + k * N;
+    v.rv = a.rv + 3 * k * N; v.rv2 = a.rv2 + 3 * k * N;
+    v.cell_start = a.cell_start + k * nc;
+    v.cell_atoms = a.cell_atoms + k * N;
+    const long long go = 10 * k * N;
+    v.g.xyz = g.xyz ? g.xyz + go : nullptr;
+    v.g.q = g.q ? g.q + go : nullptr;
+    v.g.rv = g.rv ? g.rv + go : nullptr;
+    v.g.rv2 = g.rv2 ? g.rv2 + go : nullptr;
+    return v;
+}
 
 cudaError_t launch_closest_h(const DiffArgs &a, int *ch, cudaStream_t s);
 cudaError_t launch_emap_lin(bool fp64, const DiffArgs &a, const void *eps, void *emap, cudaStream_t s);

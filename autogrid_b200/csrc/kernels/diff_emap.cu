@@ -62,6 +62,8 @@ __global__ void __launch_bounds__(EL_THREADS) k_emap_lin(DiffArgs a, const R2<R>
     R2<R> *s_tab = reinterpret_cast<R2<R> *>(smem_raw);
     V4 *s_atom = reinterpret_cast<V4 *>(smem_raw + sizeof(R2<R>) * AG_NDIEL);
     for (int i = threadIdx.x; i < AG_NDIEL; i += EL_THREADS) s_tab[i] = gtab[i];
+    const ConfView v = conf_view(a, DiffGrads{}, blockIdx.y);  // blockIdx.y: conformer
+    emap += (long long)blockIdx.y * a.n_maps_out * a.P;
 
     const long long lin = (long long)blockIdx.x * EL_THREADS + threadIdx.x;
     const bool valid = lin < a.P;
@@ -74,9 +76,9 @@ __global__ void __launch_bounds__(EL_THREADS) k_emap_lin(DiffArgs a, const R2<R>
         const int na = min(EL_TILE, a.n_atoms - a0);
         __syncthreads();
         for (int i = threadIdx.x; i < na; i += EL_THREADS) {
-            V4 v;
-            v.x = (R)a.x[a0 + i]; v.y = (R)a.y[a0 + i]; v.z = (R)a.z[a0 + i]; v.w = (R)a.q[a0 + i];
-            s_atom[i] = v;
+            V4 t;
+            t.x = (R)v.x[a0 + i]; t.y = (R)v.y[a0 + i]; t.z = (R)v.z[a0 + i]; t.w = (R)v.q[a0 + i];
+            s_atom[i] = t;
         }
         __syncthreads();
         R acc = 0;
@@ -95,18 +97,22 @@ __global__ void __launch_bounds__(EL_THREADS) k_emap_lin(DiffArgs a, const R2<R>
 
 template <class R>
 __global__ void __launch_bounds__(EL_THREADS)
-k_emap_lin_adj(DiffArgs a, const R2<R> *__restrict__ gtab, const R *__restrict__ g_e, DiffGrads g, int points_per_block)
+k_emap_lin_adj(DiffArgs a, const R2<R> *__restrict__ gtab, const R *__restrict__ g_e, DiffGrads g_all,
+               int points_per_block)
 {
     using V4 = typename Vec4<R>::T;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     R2<R> *s_tab = reinterpret_cast<R2<R> *>(smem_raw);
     V4 *s_pt = reinterpret_cast<V4 *>(smem_raw + sizeof(R2<R>) * AG_NDIEL);
     for (int i = threadIdx.x; i < AG_NDIEL; i += EL_THREADS) s_tab[i] = gtab[i];
+    const ConfView cv = conf_view(a, g_all, blockIdx.z);  // blockIdx.z: conformer
+    const DiffGrads g = cv.g;
+    g_e += (long long)blockIdx.z * a.n_maps_out * a.P;
 
     const int at = blockIdx.x * EL_THREADS + threadIdx.x;
     const bool valid = at < a.n_atoms;
-    const R xa = valid ? (R)a.x[at] : (R)0, ya = valid ? (R)a.y[at] : (R)0, za = valid ? (R)a.z[at] : (R)0;
-    const R qa = valid ? (R)a.q[at] : (R)0;
+    const R xa = valid ? (R)cv.x[at] : (R)0, ya = valid ? (R)cv.y[at] : (R)0, za = valid ? (R)cv.z[at] : (R)0;
+    const R qa = valid ? (R)cv.q[at] : (R)0;
     R gx = 0, gy = 0, gz = 0, gq = 0;
     const long long p_begin = (long long)blockIdx.y * points_per_block;
     const long long p_end = min(a.P, p_begin + points_per_block);
@@ -161,7 +167,7 @@ template <class R> cudaError_t set_smem(const void *fn)
 cudaError_t launch_emap_lin(bool fp64, const DiffArgs &a, const void *eps, void *emap, cudaStream_t s)
 {
     if (a.P == 0) return cudaSuccess;
-    const unsigned nb = (unsigned)((a.P + EL_THREADS - 1) / EL_THREADS);
+    const dim3 nb((unsigned)((a.P + EL_THREADS - 1) / EL_THREADS), (unsigned)a.n_conf);
     cudaError_t e;
     if (fp64) {
         if ((e = set_smem<double>((const void *)k_emap_lin<double>)) != cudaSuccess) return e;
@@ -184,7 +190,7 @@ cudaError_t launch_emap_lin_adj(bool fp64, const DiffArgs &a, const void *eps, c
     ppb = ((ppb + EL_TILE - 1) / EL_TILE) * EL_TILE;
     if (ppb < EL_TILE) ppb = EL_TILE;
     ranges = (a.P + ppb - 1) / ppb;
-    dim3 grid((unsigned)atom_blocks, (unsigned)ranges);
+    dim3 grid((unsigned)atom_blocks, (unsigned)ranges, (unsigned)a.n_conf);
     cudaError_t e;
     if (fp64) {
         if ((e = set_smem<double>((const void *)k_emap_lin_adj<double>)) != cudaSuccess) return e;

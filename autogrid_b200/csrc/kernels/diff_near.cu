@@ -34,16 +34,20 @@ template <class R> struct NearLinSmem {
 struct Brick {
     int ix0, iy0, iz0;
     int ix, iy, iz;
+    int conf;
     bool valid;
     long long lin;
 };
 
+// blockIdx.z runs over (z bricks) x (conformers)
 __device__ __forceinline__ Brick brick_of(const DiffArgs &a)
 {
     Brick b;
+    const int nbz = (a.n1z + DF_BRICK_Z - 1) / DF_BRICK_Z;
+    b.conf = blockIdx.z / nbz;
     b.ix0 = blockIdx.x * DF_BRICK_X;
     b.iy0 = blockIdx.y * DF_BRICK_Y;
-    b.iz0 = blockIdx.z * DF_BRICK_Z;
+    b.iz0 = (blockIdx.z % nbz) * DF_BRICK_Z;
     const int t = threadIdx.x;
     b.ix = b.ix0 + t % DF_BRICK_X;
     b.iy = b.iy0 + (t / DF_BRICK_X) % DF_BRICK_Y;
@@ -55,7 +59,8 @@ __device__ __forceinline__ Brick brick_of(const DiffArgs &a)
 
 // Cells whose box lies within DF_RADIUS of the brick's box, in cell order,
 // with the running offsets of their atoms.
-template <class R> __device__ void brick_cells(const DiffArgs &a, const Brick &bk, NearLinSmem<R> &sm)
+template <class R>
+__device__ void brick_cells(const DiffArgs &a, const ConfView &v, const Brick &bk, NearLinSmem<R> &sm)
 {
     const int ix1 = min(bk.ix0 + DF_BRICK_X - 1, a.n1x - 1), iy1 = min(bk.iy0 + DF_BRICK_Y - 1, a.n1y - 1),
               iz1 = min(bk.iz0 + DF_BRICK_Z - 1, a.n1z - 1);
@@ -83,7 +88,7 @@ template <class R> __device__ void brick_cells(const DiffArgs &a, const Brick &b
             d2 += g * g;
         }
         const int cid = cx + a.ncx * (cy + a.ncy * cz);
-        const int cnt = a.cell_start[cid + 1] - a.cell_start[cid];
+        const int cnt = v.cell_start[cid + 1] - v.cell_start[cid];
         sm.ok[k] = (d2 <= DF_RADIUS * DF_RADIUS && cnt > 0) ? cid : -1;
     }
     __syncthreads();
@@ -94,7 +99,7 @@ template <class R> __device__ void brick_cells(const DiffArgs &a, const Brick &b
             if (cid < 0) continue;
             sm.cells[m] = cid;
             sm.off[m] = tot;
-            tot += a.cell_start[cid + 1] - a.cell_start[cid];
+            tot += v.cell_start[cid + 1] - v.cell_start[cid];
             m++;
         }
         sm.off[m] = tot;
@@ -105,7 +110,8 @@ template <class R> __device__ void brick_cells(const DiffArgs &a, const Brick &b
 }
 
 // Stage candidates [c0, c0 + DF_STAGE) of the brick into shared memory.
-template <class R> __device__ void stage_chunk(const DiffArgs &a, NearLinSmem<R> &sm, int c0)
+template <class R>
+__device__ void stage_chunk(const DiffArgs &a, const ConfView &v, NearLinSmem<R> &sm, int c0)
 {
     const int k = c0 + threadIdx.x;
     if (threadIdx.x < DF_STAGE && k < sm.total) {
@@ -115,13 +121,13 @@ template <class R> __device__ void stage_chunk(const DiffArgs &a, NearLinSmem<R>
             if (sm.off[mid] <= k) lo = mid;
             else hi = mid - 1;
         }
-        const int ia = a.cell_atoms[a.cell_start[sm.cells[lo]] + (k - sm.off[lo])];
+        const int ia = v.cell_atoms[v.cell_start[sm.cells[lo]] + (k - sm.off[lo])];
         Atom<R> &t = sm.at[threadIdx.x];
-        t.x = (R)a.x[ia]; t.y = (R)a.y[ia]; t.z = (R)a.z[ia];
-        t.q = (R)a.q[ia]; t.vol = (R)a.vol[ia]; t.solpar = (R)a.solpar[ia];
+        t.x = (R)v.x[ia]; t.y = (R)v.y[ia]; t.z = (R)v.z[ia];
+        t.q = (R)v.q[ia]; t.vol = (R)a.vol[ia]; t.solpar = (R)a.solpar[ia];
         for (int i = 0; i < 3; i++) {
-            t.rv[i] = (R)a.rv[3 * ia + i];
-            t.rv2[i] = (R)a.rv2[3 * ia + i];
+            t.rv[i] = (R)v.rv[3 * ia + i];
+            t.rv2[i] = (R)v.rv2[3 * ia + i];
         }
         t.meta = a.meta[ia];
         t.idx = ia;
@@ -144,12 +150,16 @@ k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ 
 {
     __shared__ NearLinSmem<R> sm;
     const Brick bk = brick_of(a);
+    const ConfView v = conf_view(a, DiffGrads{}, bk.conf);
+    chs += bk.conf * a.P;
+    maps += (long long)bk.conf * a.n_maps_out * a.P;
+    mmarg += 2LL * bk.conf * a.n_mm * a.P;
     const R px = (R)((bk.ix - a.nex) * a.spacing), py = (R)((bk.iy - a.ney) * a.spacing),
             pz = (R)((bk.iz - a.nez) * a.spacing);
     const int ch = bk.valid ? chs[bk.lin] : -1;
     R rvh[3] = {0, 0, 0};
     if (ch >= 0)
-        for (int i = 0; i < 3; i++) rvh[i] = (R)a.rv[3 * ch + i];
+        for (int i = 0; i < 3; i++) rvh[i] = (R)v.rv[3 * ch + i];
     R E[DF_MAXS], hmin[DF_MAXMM], hmax[DF_MAXMM];
     int amin[DF_MAXMM], amax[DF_MAXMM];
 #pragma unroll
@@ -157,10 +167,10 @@ k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ 
 #pragma unroll
     for (int s = 0; s < DF_MAXMM; s++) { hmin[s] = (R)999999.; hmax[s] = (R)-999999.; amin[s] = -1; amax[s] = -1; }
 
-    brick_cells(a, bk, sm);
+    brick_cells(a, v, bk, sm);
     for (int c0 = 0; c0 < sm.total; c0 += DF_STAGE) {
         __syncthreads();
-        stage_chunk(a, sm, c0);
+        stage_chunk(a, v, sm, c0);
         __syncthreads();
         const int n = min(DF_STAGE, sm.total - c0);
         if (!bk.valid) continue;
@@ -201,16 +211,22 @@ template <class R> __device__ __forceinline__ R warp_sum(R v)
 template <class R>
 __global__ void __launch_bounds__(DF_THREADS)
 k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ sol,
-               const R *__restrict__ g_maps, const int *__restrict__ chs, const int *__restrict__ mmarg, DiffGrads gr)
+               const R *__restrict__ g_maps, const int *__restrict__ chs, const int *__restrict__ mmarg,
+               DiffGrads gr_all)
 {
     __shared__ NearLinSmem<R> sm;
     const Brick bk = brick_of(a);
+    const ConfView v = conf_view(a, gr_all, bk.conf);
+    const DiffGrads gr = v.g;
+    chs += bk.conf * a.P;
+    g_maps += (long long)bk.conf * a.n_maps_out * a.P;
+    mmarg += 2LL * bk.conf * a.n_mm * a.P;
     const R px = (R)((bk.ix - a.nex) * a.spacing), py = (R)((bk.iy - a.ney) * a.spacing),
             pz = (R)((bk.iz - a.nez) * a.spacing);
     const int ch = bk.valid ? chs[bk.lin] : -1;
     R rvh[3] = {0, 0, 0}, g_rvh[3] = {0, 0, 0};
     if (ch >= 0)
-        for (int i = 0; i < 3; i++) rvh[i] = (R)a.rv[3 * ch + i];
+        for (int i = 0; i < 3; i++) rvh[i] = (R)v.rv[3 * ch + i];
     R gs[DF_MAXS];
     int amin[DF_MAXMM], amax[DF_MAXMM];
 #pragma unroll
@@ -224,10 +240,10 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
     }
     const int lane = threadIdx.x & 31;
 
-    brick_cells(a, bk, sm);
+    brick_cells(a, v, bk, sm);
     for (int c0 = 0; c0 < sm.total; c0 += DF_STAGE) {
         __syncthreads();
-        stage_chunk(a, sm, c0);
+        stage_chunk(a, v, sm, c0);
         __syncthreads();
         const int n = min(DF_STAGE, sm.total - c0);
         for (int j = 0; j < n; j++) {
@@ -280,6 +296,8 @@ __global__ void __launch_bounds__(CH_THREADS) k_closest_h(DiffArgs a, int *__res
 {
     __shared__ double sx[CH_THREADS], sy[CH_THREADS], sz[CH_THREADS];
     __shared__ int sidx[CH_THREADS];
+    const ConfView v = conf_view(a, DiffGrads{}, blockIdx.y);
+    ch += blockIdx.y * a.P;
     const long long lin = (long long)blockIdx.x * CH_THREADS + threadIdx.x;
     const bool valid = lin < a.P;
     const long long l = valid ? lin : 0;
@@ -293,7 +311,7 @@ __global__ void __launch_bounds__(CH_THREADS) k_closest_h(DiffArgs a, int *__res
         __syncthreads();
         if (threadIdx.x < nh) {
             const int ia = a.h_index[h0 + threadIdx.x];
-            sx[threadIdx.x] = a.x[ia]; sy[threadIdx.x] = a.y[ia]; sz[threadIdx.x] = a.z[ia];
+            sx[threadIdx.x] = v.x[ia]; sy[threadIdx.x] = v.y[ia]; sz[threadIdx.x] = v.z[ia];
             sidx[threadIdx.x] = ia;
         }
         __syncthreads();
@@ -309,7 +327,7 @@ __global__ void __launch_bounds__(CH_THREADS) k_closest_h(DiffArgs a, int *__res
 dim3 brick_grid(const DiffArgs &a)
 {
     return dim3((unsigned)((a.n1x + DF_BRICK_X - 1) / DF_BRICK_X), (unsigned)((a.n1y + DF_BRICK_Y - 1) / DF_BRICK_Y),
-                (unsigned)((a.n1z + DF_BRICK_Z - 1) / DF_BRICK_Z));
+                (unsigned)((a.n1z + DF_BRICK_Z - 1) / DF_BRICK_Z * a.n_conf));
 }
 
 }  // namespace
@@ -317,7 +335,7 @@ dim3 brick_grid(const DiffArgs &a)
 cudaError_t launch_closest_h(const DiffArgs &a, int *ch, cudaStream_t s)
 {
     if (a.P == 0) return cudaSuccess;
-    k_closest_h<<<(unsigned)((a.P + CH_THREADS - 1) / CH_THREADS), CH_THREADS, 0, s>>>(a, ch);
+    k_closest_h<<<dim3((unsigned)((a.P + CH_THREADS - 1) / CH_THREADS), (unsigned)a.n_conf), CH_THREADS, 0, s>>>(a, ch);
     return cudaGetLastError();
 }
 

@@ -267,15 +267,29 @@ ag_status    ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *pro
  * rvector2 [3N], all FP64 host memory.  Maps and map gradients are
  * [n_maps][P] in the precision of opts->precision (float or double); P =
  * n1x*n1y*n1z.
+ *
+ * Conformers: an object may hold K coordinate sets (conformers) of the same
+ * receptor -- same atoms, types, tables and grid -- evaluated together, each
+ * forward and each backward one launch per kernel over all K.  Per-conformer
+ * arrays are then stacked: maps [K][n_maps][P], closest H [K][P], gradients
+ * [K][3N] / [K][N].
  */
 typedef struct ag_diff ag_diff;
 /* Bind a problem (copied: atoms, types, tables); opts->precision selects the
  * FP32 kernels or their FP64 twin, opts->table_mode must be AG_TABLE_LINEAR. */
 ag_status   ag_diff_create(ag_context *ctx, const ag_problem *problem, const ag_opts *opts,
                            ag_diff **out);
-/* Replace atom coordinates, charges and bond vectors (NULL keeps the current). */
+/* Same with n_conformers (1..4096) conformers, each starting at the
+ * problem's coordinates. */
+ag_status   ag_diff_create_batch(ag_context *ctx, const ag_problem *problem, const ag_opts *opts,
+                                 int32_t n_conformers, ag_diff **out);
+int32_t     ag_diff_conformers(const ag_diff *d);
+/* Replace atom coordinates, charges and bond vectors of conformer 0 / of
+ * conformer k (NULL keeps the current). */
 ag_status   ag_diff_set_atoms(ag_diff *d, const double *coord, const double *charge,
                               const double *rvector, const double *rvector2);
+ag_status   ag_diff_set_conformer(ag_diff *d, int32_t k, const double *coord, const double *charge,
+                                  const double *rvector, const double *rvector2);
 /* Compute all maps.  keep_closest_h = 1 reuses the closest DS/D1 atoms of the
  * previous forward (0, or no previous forward: search them at the current
  * coordinates, as main.cpp:2986-3015 does).  device_out: a device buffer of
@@ -317,6 +331,15 @@ ag_status          ag_job_write_maps_f64(ag_job *job, const double *maps);
 /* Record a fatal error in the job's GLG ("Unsuccessful Completion"). */
 void               ag_job_fail(ag_job *job, const char *message);
 void               ag_job_free(ag_job *job);
+/* The job with Vina-potential tables in place of the AD4 ones: the table
+ * fill of main.cpp:2081-2126 (compiled out of the reference build,
+ * use_vina_potential = FALSE at main.cpp:263) with the xs radii of
+ * read_parameter_library.cc:323-339 (1.8 A for other types), restated as
+ * written.  The problem has the job's atoms, grid and atom maps only (the
+ * reference drops the e and d maps and desolvation under Vina), no H-bond
+ * directionality (plain sums) and no desolvation; it is owned by the job.
+ * AG_ERR_UNSUPPORTED with separate_desolvation_maps. */
+ag_status          ag_job_vina_problem(ag_job *job, const ag_problem **out);
 /* Bond vectors (rvector, rvector2; [3N] each) at other coordinates coord
  * ([3N], the problem's centred frame; NULL = the job's own), keeping the
  * bonded neighbours the GPF load found (main.cpp:2320-2656: the same vector
