@@ -103,18 +103,22 @@ struct ag_diff {
 
 namespace {
 
+// vdW rows [type][bin][stride]: slot s holds the table of its atom map
+// (slot_tab[s]; zero for slots without a pair term).
 template <class R>
-void build_tables(const ag_problem *p, std::vector<R2<R>> &vdw, std::vector<R2<R>> &sol, std::vector<R2<R>> &eps)
+void build_tables(const ag_problem *p, const DiffArgs &A, std::vector<R2<R>> &vdw, std::vector<R2<R>> &sol,
+                  std::vector<R2<R>> &eps)
 {
-    const int nT = p->n_rec_types, nAM = p->n_atom_maps;
-    vdw.assign((size_t)std::max(nT, 1) * std::max(nAM, 1) * AG_NEINT, R2<R>{R(0), R(0)});
+    const int nT = p->n_rec_types, nAM = p->n_atom_maps, W = A.tab_stride;
+    vdw.assign((size_t)std::max(nT, 1) * AG_NEINT * W, R2<R>{R(0), R(0)});
     for (int t = 0; t < nT; t++)
-        for (int m = 0; m < nAM; m++) {
+        for (int s = 0; s < A.n_slots; s++) {
+            const int m = A.slot_tab[s];
+            if (m < 0) continue;
             const float *src = p->e_vdw_hb + ((size_t)t * nAM + m) * AG_NEINT;
-            R2<R> *dst = vdw.data() + ((size_t)t * nAM + m) * AG_NEINT;
             for (int b = 0; b < AG_NEINT; b++) {
                 const double v = src[b], nx = (b < AG_NEINT - 1) ? (double)src[b + 1] : v;
-                dst[b] = R2<R>{R(v), R(nx - v)};
+                vdw[((size_t)t * AG_NEINT + b) * W + s] = R2<R>{R(v), R(nx - v)};
             }
         }
     sol.resize(AG_NEINT);
@@ -312,6 +316,7 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
     A.n_slots = (int)slots.size();
     A.n_mm = n_mm;
     A.n_maps_out = p->n_maps;
+    A.tab_stride = std::max(4, (A.n_slots + 3) / 4 * 4);
     for (int s = 0; s < A.n_slots; s++) {
         const Slot &sl = slots[s];
         A.slot_map[s] = sl.map;
@@ -352,11 +357,11 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
         DF_CK(cudaMemcpy(d->d_h, d->h_index.data(), d->h_index.size() * sizeof(int), cudaMemcpyHostToDevice));
     if (d->fp64) {
         std::vector<R2<double>> vdw, sol, eps;
-        build_tables(p, vdw, sol, eps);
+        build_tables(p, A, vdw, sol, eps);
         DF_CK(put(&d->d_vdw, vdw, d.get())); DF_CK(put(&d->d_sol, sol, d.get())); DF_CK(put(&d->d_eps, eps, d.get()));
     } else {
         std::vector<R2<float>> vdw, sol, eps;
-        build_tables(p, vdw, sol, eps);
+        build_tables(p, A, vdw, sol, eps);
         DF_CK(put(&d->d_vdw, vdw, d.get())); DF_CK(put(&d->d_sol, sol, d.get())); DF_CK(put(&d->d_eps, eps, d.get()));
     }
     A.x = d->d_x; A.y = d->d_y; A.z = d->d_z; A.q = d->d_q; A.vol = d->d_vol; A.solpar = d->d_solpar;

@@ -70,8 +70,9 @@ struct DiffArgs {
     int ncx, ncy, ncz;
     double cell0[3], cell_size;
     const int *cell_start, *cell_atoms;
-    // slots: every map except the e map; maps per conformer in the output
-    int n_slots, n_mm, n_maps_out;
+    // slots: every map except the e map; maps per conformer in the output;
+    // slots per (type, bin) row of the vdW table
+    int n_slots, n_mm, n_maps_out, tab_stride;
     int slot_map[DF_MAXS];       // output map index
     int slot_kind[DF_MAXS];      // DK_*
     int slot_tab[DF_MAXS];       // atom-map index of the pair term (-1: none)
@@ -87,8 +88,9 @@ constexpr int DM_TYPE_MASK = 31, DM_HB_SHIFT = 5, DM_REXP_SHIFT = 8;
 constexpr int DM_DIS = 1 << 11, DM_SKIP = 1 << 12;
 
 // Interpolation tables, (value, next - value) per bin, in the working
-// precision: vdw [n_rec_types][n_atom_maps][NEINT], sol [NEINT], eps [NDIEL]
-// (dielectric factor * coeff_estat).
+// precision: vdw [n_rec_types][NEINT][tab_stride] (slot s of a row holds the
+// table of the slot's atom map, so one pair's slots are one contiguous read),
+// sol [NEINT], eps [NDIEL] (dielectric factor * coeff_estat).
 template <class R> struct R2 { R v, d; };
 
 struct DiffGrads {

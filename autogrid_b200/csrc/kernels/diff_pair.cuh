@@ -215,17 +215,18 @@ DF_HD bool geom(const R2<R> *sol, const Atom<R> &at, R px, R py, R pz, Geom<R> &
 
 // T_H(r - 1.10): the hydrogen row at xh = A_DIV (r - 1.10) (main.cpp:3309-3313).
 template <class R>
-DF_HD R th_lookup(const DiffArgs &a, const R2<R> *vdw, int m, R x, R &dth)
+DF_HD R th_lookup(const DiffArgs &a, const R2<R> *vdw, int s, R x, R &dth)
 {
     dth = R(0);
     if (a.hydrogen_type < 0 || a.hydrogen_type >= a.n_rec_types) return R(0);
-    const R2<R> *row = vdw + ((size_t)a.hydrogen_type * a.n_atom_maps + m) * AG_NEINT;
+    const R2<R> *row = vdw + (size_t)a.hydrogen_type * AG_NEINT * a.tab_stride + s;
     const R xh = x - R(1.10 * AG_A_DIV);
     if (xh <= R(0)) return row[0].v;
     int bh = (int)xh;
     bh = bh < AG_NEINT - 1 ? bh : AG_NEINT - 1;
-    dth = row[bh].d;
-    return lerp(row[bh], xh - R(bh));
+    const R2<R> e = row[(size_t)bh * a.tab_stride];
+    dth = e.d;
+    return lerp(e, xh - R(bh));
 }
 
 // The value v of an H-bond-aware pair term and its partials (main.cpp:3297-3375).
@@ -234,10 +235,10 @@ template <class R> struct Term {
 };
 
 template <class R>
-DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, int type, int m, const Geom<R> &g, const Ang<R> &an,
+DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, int type, int s, const Geom<R> &g, const Ang<R> &an,
                 Term<R> &t)
 {
-    const R2<R> te = vdw[((size_t)type * a.n_atom_maps + m) * AG_NEINT + g.b];
+    const R2<R> te = vdw[((size_t)type * AG_NEINT + g.b) * a.tab_stride + s];
     const R T = lerp(te, g.fx);
     R drs;
     const R rs = rsph(T, drs);
@@ -255,7 +256,7 @@ DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, int type, int m, c
             t.dH = T * f;
         } break;
         case DA_SUMA_DIS: {
-            const R TH = th_lookup(a, vdw, m, g.x, dth);
+            const R TH = th_lookup(a, vdw, s, g.x, dth);
             const R f = an.racc + (R(1) - an.racc) * rs;
             t.v = TH * an.H * f;
             t.dTH = an.H * f;
@@ -270,7 +271,7 @@ DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, int type, int m, c
             t.dracc = T * (R(1) - rs);
         } break;
         case DA_SUMD_DIS: {
-            const R TH = th_lookup(a, vdw, m, g.x, dth);
+            const R TH = th_lookup(a, vdw, s, g.x, dth);
             const R f = an.rdon + (R(1) - an.rdon) * rs;
             t.v = TH * an.H * f;
             t.dTH = an.H * f;
@@ -315,7 +316,7 @@ DF_HD void pair_fwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
             const int act = a.act[s][cls];
             if (act != DA_NONE) {
                 Term<R> t;
-                term(a, vdw, act, type, m, g, an, t);
+                term(a, vdw, act, type, s, g, an, t);
                 const R val = g.w * t.v;
                 if (act_is_mm(act)) {
                     if (s < DF_MAXMM) {  // min/max slots come first
@@ -370,7 +371,7 @@ DF_HD void pair_bwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
                 }
                 if (gv != R(0)) {
                     Term<R> t;
-                    term(a, vdw, act, type, m, g, an, t);
+                    term(a, vdw, act, type, s, g, an, t);
                     G_x += gv * (g.dw * t.v + g.w * t.dx);
                     G_racc += gv * g.w * t.dracc;
                     G_rdon += gv * g.w * t.drdon;

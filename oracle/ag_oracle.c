@@ -377,7 +377,7 @@ int32_t ag_oracle_points_lin(const ag_problem *p, int64_t n_pts, const int64_t *
         int closestH = -1;
         if (nAM > 0) {
             if (closest_h) {
-                closestH = closest_h[ip];
+                closestH = closest_h[ip];  /* -1: frozen "none", Hramp stays 1 */
             } else {
                 double rminH = 999999.;
                 for (int inh = 0; inh < nhb12; inh++) {
@@ -387,7 +387,7 @@ int32_t ag_oracle_points_lin(const ag_problem *p, int64_t n_pts, const int64_t *
                     if (r < rminH) { rminH = r; closestH = hb12[inh]; }
                 }
             }
-            if (closestH < 0) { rc = AG_ERR_NO_CLOSEST_H; break; }
+            if (closestH < 0 && !closest_h) { rc = AG_ERR_NO_CLOSEST_H; break; }
         }
         if (nAM > 0 || p->dsolv_map >= 0) {
             for (int ia = 0; ia < nA; ia++) {
@@ -413,7 +413,7 @@ int32_t ag_oracle_points_lin(const ag_problem *p, int64_t n_pts, const int64_t *
                     else if (p->rexp[ia] == 2) racc = cos_theta * cos_theta;
                     else if (p->rexp[ia] == 4) racc = pow(cos_theta, 4.);
                     else racc = cos_theta;
-                    if (ia != closestH) {
+                    if (closestH >= 0 && ia != closestH) {
                         const double *rvh = p->rvector + 3 * closestH;
                         double ct = rvh[0] * rv[0] + rvh[1] * rv[1] + rvh[2] * rv[2];
                         ct = dmax(dmin(ct, 1.0), -1.0);

@@ -30,7 +30,8 @@ struct Case {
     std::vector<int> ch;
 };
 
-void make_table(std::vector<R2<double>> &t, size_t off, double A, double B, double clamp)
+// slot s of type t: rows [t][bin][stride]
+void make_table(std::vector<R2<double>> &tab, int t, int s, int stride, double A, double B, double clamp)
 {
     std::vector<double> v(AG_NEINT);
     for (int b = 0; b < AG_NEINT; b++) {
@@ -38,7 +39,8 @@ void make_table(std::vector<R2<double>> &t, size_t off, double A, double B, doub
         v[b] = std::min(A / std::pow(r, 12) - B / std::pow(r, 6), clamp);
     }
     v[AG_NEINT - 1] = 0;
-    for (int b = 0; b < AG_NEINT; b++) t[off + b] = R2<double>{v[b], b < AG_NEINT - 1 ? v[b + 1] - v[b] : 0.0};
+    for (int b = 0; b < AG_NEINT; b++)
+        tab[((size_t)t * AG_NEINT + b) * stride + s] = R2<double>{v[b], b < AG_NEINT - 1 ? v[b + 1] - v[b] : 0.0};
 }
 
 double loss(const Case &c, const std::vector<Atom<double>> &atoms)
@@ -166,11 +168,12 @@ int main(int argc, char **argv)
     a.slot_map[NAM] = NAM;
     a.slot_kind[NAM] = DK_D;
     a.slot_tab[NAM] = -1;
-    c.vdw.assign((size_t)NT * NAM * AG_NEINT, R2<double>{0, 0});
+    a.tab_stride = 8;
+    c.vdw.assign((size_t)NT * AG_NEINT * a.tab_stride, R2<double>{0, 0});
     for (int t = 0; t < NT; t++)
         for (int m = 0; m < NAM; m++)
-            make_table(c.vdw, ((size_t)t * NAM + m) * AG_NEINT, 2000.0 * (1 + 0.3 * t) * (1 + 0.1 * m),
-                       40.0 * (1 + 0.2 * m), 100000.0);
+            make_table(c.vdw, t, m, a.tab_stride, 2000.0 * (1 + 0.3 * t) * (1 + 0.1 * m), 40.0 * (1 + 0.2 * m),
+                       100000.0);
     c.sol.resize(AG_NEINT);
     std::vector<double> sv(AG_NEINT + 1);
     for (int b = 0; b <= AG_NEINT; b++) { const double r = b / 128.0; sv[b] = 0.1711 * std::exp(-r * r / 25.92); }

@@ -99,8 +99,13 @@ def test_vina_adjoint_matches_central_differences(tmp_path, gpu_ctx):
     atoms = rng.choice(near_box, 16, replace=False)
     r = gradcheck.check(job, vp, gpu_ctx, atoms, w, h_coord=(1e-3, 1e-6))
     err = r["fp64_vs_fd_coord"]
-    assert err[1e-6] < 1e-4, err
-    assert err[1e-3] < 2e-2, err
+    # The table as written steps by the H-bond weight at d = 0.7 and d = -0.7
+    # and by the hydrophobic weight at d = 0.5; interpolated, each step is one
+    # bin with a slope of ~75 kcal/mol/A, so a straddled bin edge costs a
+    # finite difference ~100x more than in the AD4 tables.
+    assert err[1e-6] < 1e-3, err
+    assert err[1e-3] < 2e-1, err
+    assert err[1e-6] < err[1e-3] / 20, err
     assert r["fp32_vs_fp64_coord"] < 1e-3, r["fp32_vs_fp64_coord"]
     # Vina maps do not depend on charges
     assert np.abs(r["fp64_charge"]).max() == 0.0
