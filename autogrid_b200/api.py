@@ -65,8 +65,15 @@ class Problem:
         return self.n1[0] * self.n1[1] * self.n1[2]
 
     @property
+    def n_out(self) -> int:
+        """Output arrays: the n_maps energy maps, then the floating-grid and
+        constriction maps when requested."""
+        return (self.n_maps + int(bool(self.scalars.get("floating_grid", 0)))
+                + int(bool(self.scalars.get("constriction_grid", 0))))
+
+    @property
     def map_shape(self) -> tuple:
-        return (self.n_maps, self.n1[2], self.n1[1], self.n1[0])
+        return (self.n_out, self.n1[2], self.n1[1], self.n1[0])
 
     def struct(self) -> ag_problem:
         a = self.arrays

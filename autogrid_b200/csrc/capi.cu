@@ -95,6 +95,8 @@ struct ag_plan {
     std::vector<NearGroup> groups;
     int mpad = 4, n_chunks = 0, chunk_atoms = 0;
     bool any_cov = false;
+    int floating = 0, constriction = 0;  // distance maps after the n_maps energy maps
+    double constriction_cutoff = 7.5;
     float *maps32 = nullptr;
     double *maps64 = nullptr;
     double *cov = nullptr;
@@ -133,10 +135,7 @@ ag_status validate(const ag_problem *p)
     if (p->n_atom_maps + (p->elec_map >= 0) + (p->dsolv_map >= 0) != p->n_maps)
         return invalid("n_maps != n_atom_maps + elec + dsolv");
     if (p->n_rec_types < 0 || p->n_rec_types > AG_MAX_REC_TYPES) return invalid("n_rec_types out of range");
-    if (p->floating_grid || p->constriction_grid) {
-        set_last_error("floating (fmap) and constriction (cmap) grids are not provided by this build");
-        return AG_ERR_UNSUPPORTED;
-    }
+    if (p->constriction_grid && !std::isfinite(p->constriction_cutoff)) return invalid("constriction_cutoff must be finite");
     const int N = p->n_atoms;
     if (N > 0 && (!p->coord || !p->charge || !p->vol || !p->solpar || !p->rec_type || !p->hbond || !p->rexp ||
                   !p->rvector || !p->rvector2 || !p->disorder))
@@ -417,12 +416,16 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
     // outputs and scratch
     void *v = nullptr;
     const size_t P = (size_t)d.P;
+    pl->floating = p->floating_grid ? 1 : 0;
+    pl->constriction = p->constriction_grid ? 1 : 0;
+    pl->constriction_cutoff = p->constriction_cutoff;
+    const size_t n_out = (size_t)p->n_maps + pl->floating + pl->constriction;
     if (pl->opts.precision == AG_PREC_FP64) {
-        AGB_CK(B->ensure("maps64", (size_t)p->n_maps * P * sizeof(double), &v));
+        AGB_CK(B->ensure("maps64", n_out * P * sizeof(double), &v));
         pl->maps64 = (double *)v;
         pl->maps32 = nullptr;
     } else {
-        AGB_CK(B->ensure("maps32", (size_t)p->n_maps * P * sizeof(float), &v));
+        AGB_CK(B->ensure("maps32", n_out * P * sizeof(float), &v));
         pl->maps32 = (float *)v;
         pl->maps64 = nullptr;
     }
@@ -486,6 +489,17 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
     }
     if (pl->any_cov) {
         AGB_CK(launch_covalent(d, pl->cov, s));
+        launches++;
+    }
+    if (pl->floating || pl->constriction) {
+        const size_t P = (size_t)d.P, f = (size_t)d.n_maps * P, c = f + (size_t)pl->floating * P;
+        if (exact)
+            AGB_CK(launch_distance_maps(d, pl->constriction_cutoff, nullptr, nullptr,
+                                        pl->floating ? pl->maps64 + f : nullptr,
+                                        pl->constriction ? pl->maps64 + c : nullptr, s));
+        else
+            AGB_CK(launch_distance_maps(d, pl->constriction_cutoff, pl->floating ? pl->maps32 + f : nullptr,
+                                        pl->constriction ? pl->maps32 + c : nullptr, nullptr, nullptr, s));
         launches++;
     }
     const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || (!exact && d.elec_map >= 0);
@@ -758,8 +772,8 @@ static ag_status compute_common(ag_context *ctx, const ag_problem *problem, cons
     st = run_plan(pl, ctx->stream);
     if (st != AG_OK) return st;
     const void *src = elem == 8 ? (const void *)pl->maps64 : (const void *)pl->maps32;
-    AGB_CK(cudaMemcpyAsync(maps, src, (size_t)problem->n_maps * (size_t)pl->dp.P * elem, cudaMemcpyDefault,
-                           ctx->stream));
+    const size_t n_out = (size_t)problem->n_maps + pl->floating + pl->constriction;
+    AGB_CK(cudaMemcpyAsync(maps, src, n_out * (size_t)pl->dp.P * elem, cudaMemcpyDefault, ctx->stream));
     AGB_CK(cudaStreamSynchronize(ctx->stream));
     return finish_stats(pl);
 }
@@ -803,7 +817,8 @@ ag_status ag_plan_download(ag_plan *plan, float *host_maps)
 {
     if (!plan || !host_maps) return invalid("null argument");
     ag_context *c = plan->ctx;
-    AGB_CK(cudaMemcpyAsync(host_maps, plan->maps32, (size_t)plan->dp.n_maps * (size_t)plan->dp.P * sizeof(float),
+    AGB_CK(cudaMemcpyAsync(host_maps, plan->maps32,
+                           ((size_t)plan->dp.n_maps + plan->floating + plan->constriction) * (size_t)plan->dp.P * sizeof(float),
                            cudaMemcpyDefault, c->stream));
     AGB_CK(cudaStreamSynchronize(c->stream));
     return finish_stats(plan);
@@ -831,6 +846,10 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     std::unique_ptr<ag_batch> b(new ag_batch());
     b->ctx = ctx;
     for (int i = 0; i < n; i++) {
+        if (problems[i] && (problems[i]->floating_grid || problems[i]->constriction_grid)) {
+            set_last_error("ag_batch_create: batches compute the energy maps only (no fmap/cmap)");
+            return AG_ERR_UNSUPPORTED;
+        }
         ag_plan *pl = nullptr;
         ag_status st = make_plan(ctx, problems[i], &o, true, &pl);
         if (st != AG_OK) {

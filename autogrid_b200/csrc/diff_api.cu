@@ -206,6 +206,10 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
         set_last_error("ag_diff_create: unknown precision");
         return AG_ERR_INVALID;
     }
+    if (p->floating_grid || p->constriction_grid) {
+        set_last_error("ag_diff_create: the differentiable mode computes the energy maps only (no fmap/cmap)");
+        return AG_ERR_UNSUPPORTED;
+    }
     // the closest-hydrogen requirement is checked below, only if a map uses Hramp
     ag_problem pv = *p;
     const int nAM = p->n_atom_maps;

@@ -47,15 +47,16 @@ int main(int argc, char **argv)
     ag_context *ctx = nullptr;
     st = ag_context_create(device, &ctx);
     const size_t P = (size_t)p->n1[0] * p->n1[1] * p->n1[2];
+    const size_t n_out = (size_t)p->n_maps + (p->floating_grid ? 1 : 0) + (p->constriction_grid ? 1 : 0);
     if (st == AG_OK) {
         ag_opts o{};
         o.precision = fp64 ? AG_PREC_FP64 : AG_PREC_FP32;
         if (fp64) {
-            std::vector<double> maps((size_t)p->n_maps * P);
+            std::vector<double> maps(n_out * P);
             st = ag_maps_compute_f64(ctx, p, &o, maps.data());
             if (st == AG_OK) st = ag_job_write_maps_f64(job, maps.data());
         } else {
-            std::vector<float> maps((size_t)p->n_maps * P);
+            std::vector<float> maps(n_out * P);
             st = ag_maps_compute(ctx, p, &o, maps.data());
             if (st == AG_OK) st = ag_job_write_maps_f32(job, maps.data());
         }

@@ -1280,6 +1280,34 @@ void Job::write_maps(const double *m64, const float *m32)
         std::fclose(g.fp);
         g.fp = nullptr;
     }
+    // distance maps follow the energy maps (main.cpp:3498-3514): fmap as %.3f of
+    // round3dp, cmap as an integer count
+    size_t k = (size_t)num_maps;
+    auto dist = [&](size_t a) { return m64 ? m64[k * P + a] : (double)m32[k * P + a]; };
+    if (floating_grid && floating_fp) {
+        buf.clear();
+        for (size_t a = 0; a < P; a++) {
+            char tmp[64];
+            const float v = (float)(std::round((long double)dist(a) * 1000.0L) / 1000.0L);
+            const int n = std::snprintf(tmp, sizeof tmp, "%.3f\n", (double)v);
+            buf.insert(buf.end(), tmp, tmp + n);
+        }
+        if (std::fwrite(buf.data(), 1, buf.size(), floating_fp) != buf.size()) problem = true;
+        std::fclose(floating_fp);
+        floating_fp = nullptr;
+        k++;
+    }
+    if (constriction_grid && constriction_fp) {
+        buf.clear();
+        for (size_t a = 0; a < P; a++) {
+            char tmp[32];
+            const int n = std::snprintf(tmp, sizeof tmp, "%d\n", (int)dist(a));
+            buf.insert(buf.end(), tmp, tmp + n);
+        }
+        if (std::fwrite(buf.data(), 1, buf.size(), constriction_fp) != buf.size()) problem = true;
+        std::fclose(constriction_fp);
+        constriction_fp = nullptr;
+    }
     if (problem) fatal("Problems writing grid maps - there may not be enough disk space.", AG_ERR_IO);
     log("\nGrid\tAtom\tMinimum   \tMaximum\nMap \tType\tEnergy    \tEnergy \n\t\t(kcal/mol)\t(kcal/mol)\n"
         "____\t____\t_____________\t_____________\n");

@@ -41,6 +41,8 @@ cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_be
                                   unsigned long long *counter, int tile, int ctas_per_sm, cudaStream_t s);
 cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s);
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s);
+cudaError_t launch_distance_maps(const DevProblem &p, double cutoff, float *fmap32, float *cmap32, double *fmap64,
+                                 double *cmap64, cudaStream_t s);
 int near_bricks(const DevProblem &p, int shape);
 cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int shape,
                         cudaStream_t s);

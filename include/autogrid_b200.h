@@ -117,8 +117,8 @@ typedef struct ag_problem {
     double  cov_pos[3];          /* covalent attachment point (centred)           */
     double  cov_half_width;
     double  cov_barrier;
-    int32_t floating_grid;       /* fmap requested (not provided by this build)  */
-    int32_t constriction_grid;   /* cmap requested (not provided by this build)  */
+    int32_t floating_grid;       /* fmap: distance to the nearest atom            */
+    int32_t constriction_grid;   /* cmap: atoms within constriction_cutoff        */
     double  constriction_cutoff;
 } ag_problem;
 
@@ -163,7 +163,9 @@ ag_status   ag_context_stats(const ag_context *ctx, ag_stats *out);
  * Hot path (replaces main.cpp:2805-3464).
  *
  * maps: [problem->n_maps][n1[2]][n1[1]][n1[0]] with X fastest, one contiguous
- * array per map, in the reference's gridmap order (main.cpp:321-322).  The
+ * array per map, in the reference's gridmap order (main.cpp:321-322),
+ * followed by the floating-grid map (Angstrom) and then the constriction map
+ * (atom counts) when the problem asks for them (main.cpp:2947-2966).  The
  * problem arrays are host memory; `maps` may be host (pinned or pageable) or
  * device memory (CUDA unified addressing decides).  Device buffers are owned by
  * the context and reused across calls; the call returns when the maps are in

@@ -491,3 +491,38 @@ int32_t ag_oracle_points_lin(const ag_problem *p, int64_t n_pts, const int64_t *
     free(hb12); free(E); free(hbmin); free(hbmax); free(hbflag); free(sol_ext);
     return rc;
 }
+
+/*
+ * Distance maps of LOOP 1, main.cpp:2947-2966: out[0][ip] the floating grid
+ * (min over atoms of the hypot distance clamped at APPROX_ZERO, BIG = 1e12
+ * without atoms, autocomm.h:73), then the constriction count (atoms with that
+ * distance <= constriction_cutoff), for whichever the problem requests.
+ */
+int32_t ag_oracle_distance_maps(const ag_problem *p, int64_t n_pts, const int64_t *pt_index, double *out)
+{
+    const int64_t n1x = p->n1[0], n1y = p->n1[1], n1z = p->n1[2];
+    const int64_t P = n1x * n1y * n1z;
+    if (pt_index == NULL && n_pts != P) return AG_ERR_INVALID;
+    for (int64_t ip = 0; ip < n_pts; ip++) {
+        int64_t lin = pt_index ? pt_index[ip] : ip;
+        if (lin < 0 || lin >= P) return AG_ERR_INVALID;
+        int ix = (int)(lin % n1x), iy = (int)((lin / n1x) % n1y), iz = (int)(lin / (n1x * n1y));
+        double c[3];
+        c[2] = ((double)(iz - p->ne[2])) * p->spacing;
+        c[1] = ((double)(iy - p->ne[1])) * p->spacing;
+        c[0] = ((double)(ix - p->ne[0])) * p->spacing;
+        double r_min = 1.0E12;
+        int count = 0;
+        for (int ia = 0; ia < p->n_atoms; ia++) {
+            const double *a = p->coord + 3 * ia;
+            double r = hypot(a[0] - c[0], hypot(a[1] - c[1], a[2] - c[2]));
+            if (r < O_APPROX_ZERO) r = O_APPROX_ZERO;
+            r_min = dmin(r, r_min);
+            if (r <= p->constriction_cutoff) count++;
+        }
+        int k = 0;
+        if (p->floating_grid) out[(size_t)(k++) * n_pts + ip] = r_min;
+        if (p->constriction_grid) out[(size_t)k * n_pts + ip] = (double)count;
+    }
+    return 0;
+}

@@ -40,6 +40,8 @@ def lib() -> C.CDLL:
         _lib = C.CDLL(str(ORACLE_LIB))
         _lib.ag_oracle_points.restype = C.c_int32
         _lib.ag_oracle_points.argtypes = [C.POINTER(ag_problem), C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.ag_oracle_distance_maps.restype = C.c_int32
+        _lib.ag_oracle_distance_maps.argtypes = [C.POINTER(ag_problem), C.c_int64, C.c_void_p, C.c_void_p]
         _lib.ag_oracle_points_lin.restype = C.c_int32
         _lib.ag_oracle_points_lin.argtypes = [C.POINTER(ag_problem), C.c_int64, C.c_void_p, C.c_void_p,
                                               C.c_void_p]
@@ -64,6 +66,24 @@ def oracle_points(problem, points: np.ndarray | None = None):
     if rc != 0:
         raise RuntimeError(f"oracle returned status {rc}")
     return out, flags
+
+
+def oracle_distance_maps(problem, points: np.ndarray | None = None) -> np.ndarray:
+    """FP64 floating-grid and constriction maps ([n_dist, n_pts]) of LOOP 1."""
+    s = problem.struct()
+    if points is None:
+        n = problem.points
+        idx_ptr = None
+    else:
+        points = np.ascontiguousarray(points, dtype=np.int64)
+        n = int(points.shape[0])
+        idx_ptr = points.ctypes.data_as(C.c_void_p)
+    k = problem.n_out - problem.n_maps
+    out = np.zeros((k, n), dtype=np.float64)
+    rc = lib().ag_oracle_distance_maps(C.byref(s), n, idx_ptr, out.ctypes.data_as(C.c_void_p))
+    if rc != 0:
+        raise RuntimeError(f"oracle returned status {rc}")
+    return out
 
 
 def oracle_points_lin(problem, points: np.ndarray | None = None, closest_h: np.ndarray | None = None):

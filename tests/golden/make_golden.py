@@ -9,7 +9,7 @@ PDBQT text, the map names, the full-precision maps (float64 of the printed
 float values), the %.3f maps, and the .fld text.
 
 Run here, where the reference sources exist:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [case ...]
 """
 from __future__ import annotations
 
@@ -49,6 +49,10 @@ CASES = {
     # one ligand map and no d map; a single grid point
     "tiny_onepoint": dict(n=200, seed=16, radius=8.0, spec=dict(
         npts=(1, 1, 1), ligand_types=["OA"], dsolvmap=False)),
+    # floating grid and constriction grid (main.cpp:2947-2966, :3498-3514)
+    "distance_maps": dict(n=300, seed=17, radius=10.0, dist=["f", "c"], spec=dict(
+        npts=(10, 8, 12), ligand_types=["C", "OA"],
+        extra_lines=["fmap g.f.map", "constriction_distance_cutoff 5.5", "cmap g.c.map"])),
 }
 
 
@@ -80,21 +84,30 @@ def make(name: str, case: dict) -> Path:
     with tempfile.TemporaryDirectory() as td:
         d = Path(td)
         gpf = synth.write_case(d, "g", rec, spec)
+        dist = case.get("dist", [])
         run_reference(orc.REF_FULLPREC_BIN, d, "g")
         full = [orc.read_map(d / f"g.{n}.map") for n in names]
+        dist_full = [orc.read_map(d / f"g.{n}.map") for n in dist]
         fld = (d / "g.maps.fld").read_text()
         run_reference(orc.REF_BIN, d, "g")
         rounded = [orc.read_map(d / f"g.{n}.map") for n in names]
+        dist_3dp = [orc.read_map(d / f"g.{n}.map") for n in dist]
         out = OUT / f"{name}.npz"
+        extra = {}
+        if dist:
+            extra = dict(dist_names=np.array(dist), dist_full=np.array(dist_full), dist_3dp=np.array(dist_3dp))
         np.savez_compressed(out, gpf=gpf.read_text(), pdbqt=(d / "g.pdbqt").read_text(),
                             names=np.array(names), maps_full=np.array(full), maps_3dp=np.array(rounded),
-                            fld=fld, npts=np.array(spec.npts))
+                            fld=fld, npts=np.array(spec.npts), **extra)
     return out
 
 
 def main():
     orc.build(ref=True)
+    only = sys.argv[1:]
     for name, case in CASES.items():
+        if only and name not in only:
+            continue
         p = make(name, case)
         print(f"{p.name}: {p.stat().st_size} bytes")
 

@@ -17,18 +17,27 @@ def test_fp32_matches_reference(path, tmp_path, gpu_ctx):
     from oracle.oracle import oracle_points
     z, job, prob = load_golden(path, tmp_path)
     ref = z["maps_full"]
-    got = gpu_ctx.compute(prob, "fp32").reshape(prob.n_maps, -1)
+    out = gpu_ctx.compute(prob, "fp32").reshape(prob.n_out, -1)
+    got = out[:prob.n_maps]
     _, flags = oracle_points(prob)  # FP64-ambiguous points (bin edge within 1e-12) are exempt
     ok = tolerance_ok(got, ref) | (flags[None, :] != 0)
     bad = np.argwhere(~ok)
     assert bad.size == 0, f"{len(bad)} values outside 1e-3/1e-4; first {bad[:3].tolist()}"
+    if "dist_full" in z.files:
+        dist = out[prob.n_maps:]
+        assert np.all(np.abs(dist[0] - z["dist_full"][0]) <= 1e-6 * np.abs(z["dist_full"][0]))
+        assert np.array_equal(dist[1], z["dist_full"][1])
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
 def test_fp64_twin_matches_reference(path, tmp_path, gpu_ctx):
     z, job, prob = load_golden(path, tmp_path)
-    got = gpu_ctx.compute(prob, "fp64").reshape(prob.n_maps, -1)
-    assert full_precision_ok(got, z["maps_full"]).all()
+    out = gpu_ctx.compute(prob, "fp64").reshape(prob.n_out, -1)
+    assert full_precision_ok(out[:prob.n_maps], z["maps_full"]).all()
+    if "dist_full" in z.files:
+        dist = out[prob.n_maps:]
+        assert np.all(np.abs(dist[0] - z["dist_full"][0]) <= 1.5e-7 * np.abs(z["dist_full"][0]))
+        assert np.array_equal(dist[1], z["dist_full"][1])
 
 
 @pytest.mark.parametrize("path", GOLDEN, ids=[p.stem for p in GOLDEN])
@@ -57,6 +66,11 @@ def test_cli_drop_in(path, tmp_path, built):
         small = np.abs(full) < 10.0
         if small.sum() > 20:
             assert np.mean(d[small] == 0) > 0.9, name
+    if "dist_names" in z.files:  # fmap text: %.3f of round3dp; cmap: integers
+        for i, name in enumerate(z["dist_names"]):
+            mine = read_map(tmp_path / f"g.{name}.map")
+            assert np.all(np.abs(mine - z["dist_3dp"][i]) <= 1.0005e-3), name
+        assert np.array_equal(read_map(tmp_path / "g.c.map"), z["dist_3dp"][1])
     drop = ("# Created by", "#GRID_PARAMETER_FILE")
     a = [ln for ln in (tmp_path / "g.maps.fld").read_text().splitlines() if not ln.startswith(drop)]
     b = [ln for ln in str(z["fld"]).splitlines() if not ln.startswith(drop)]

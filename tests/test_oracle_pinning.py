@@ -54,6 +54,12 @@ def test_oracle_matches_reference_golden(path, tmp_path, built):
     ok = full_precision_ok(got, ref)
     bad = np.argwhere(~ok)
     assert bad.size == 0, f"{len(bad)} values differ, first {bad[:3].tolist()}"
+    if "dist_full" in z.files:  # floating grid (Angstrom, printed like a map) and constriction counts
+        from oracle.oracle import oracle_distance_maps
+        dist = oracle_distance_maps(prob)
+        assert dist.shape == z["dist_full"].shape
+        assert np.all(np.abs(dist[0] - z["dist_full"][0]) <= 1.5e-7 * np.abs(z["dist_full"][0]))
+        assert np.array_equal(dist[1], z["dist_full"][1])
 
 
 def test_golden_set_is_present():
