@@ -4,9 +4,12 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -27,12 +30,48 @@ struct DevBuf {
     size_t cap = 0;
 };
 
+// Bump allocator over a few large device blocks, released together: the
+// buffers of a batch's instance plans (one cudaMalloc per 256 MiB instead of
+// one per buffer per instance).  Thread-safe.
+struct Arena {
+    std::vector<void *> blocks;
+    char *cur = nullptr;
+    size_t left = 0;
+    std::mutex mu;
+    static constexpr size_t kBlock = size_t(256) << 20, kAlign = 256;
+    ~Arena()
+    {
+        for (void *b : blocks) cudaFree(b);
+    }
+    cudaError_t alloc(size_t bytes, void **out)
+    {
+        bytes = (bytes + kAlign - 1) / kAlign * kAlign;
+        std::lock_guard<std::mutex> lock(mu);
+        if (bytes > left) {
+            void *b = nullptr;
+            const size_t sz = std::max(bytes, kBlock);
+            cudaError_t e = cudaMalloc(&b, sz);
+            if (e != cudaSuccess) return e;
+            blocks.push_back(b);
+            cur = (char *)b;
+            left = sz;
+        }
+        *out = cur;
+        cur += bytes;
+        left -= bytes;
+        return cudaSuccess;
+    }
+};
+
 // Grow-only device buffers keyed by role; a context keeps one set so repeated
-// one-shot calls do not re-allocate.
+// one-shot calls do not re-allocate.  With an arena, buffers come from it and
+// are released with it.
 struct BufferSet {
     std::map<std::string, DevBuf> bufs;
+    Arena *arena = nullptr;
     ~BufferSet()
     {
+        if (arena) return;
         for (auto &kv : bufs)
             if (kv.second.p) cudaFree(kv.second.p);
     }
@@ -41,10 +80,10 @@ struct BufferSet {
         DevBuf &b = bufs[name];
         if (bytes == 0) bytes = 16;
         if (b.cap < bytes) {
-            if (b.p) cudaFree(b.p);
+            if (b.p && !arena) cudaFree(b.p);
             b.p = nullptr;
             b.cap = 0;
-            cudaError_t e = cudaMalloc(&b.p, bytes);
+            cudaError_t e = arena ? arena->alloc(bytes, &b.p) : cudaMalloc(&b.p, bytes);
             if (e != cudaSuccess) return e;
             b.cap = bytes;
         }
@@ -539,12 +578,14 @@ ag_status settle_stats(ag_context *c)
 
 ag_status finish_stats(ag_plan *pl) { return settle_stats(pl->ctx); }
 
-ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out);
+ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out,
+                    Arena *arena = nullptr);
 
 }  // namespace
 
 struct ag_batch {
     ag_context *ctx = nullptr;
+    std::unique_ptr<Arena> arena;  // declared before the plans: released after them
     std::vector<std::unique_ptr<ag_plan>> plans;
     std::vector<FarArgs> far;         // per instance, in work order
     std::vector<NearInst> near;       // per (instance, group), in work order
@@ -683,7 +724,7 @@ ag_status batch_autotune(ag_batch *b)
     return AG_OK;
 }
 
-ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out)
+ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out, Arena *arena)
 {
     if (!ctx || !p || !out) return invalid("null argument");
     ag_opts opts{};
@@ -699,6 +740,7 @@ ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool
     pl->opts = opts;
     if (own) {
         pl->own.reset(new BufferSet());
+        pl->own->arena = arena;
         pl->bufs = pl->own.get();
     } else {
         pl->bufs = &ctx->pool;
@@ -845,19 +887,37 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     AGB_CK(cudaSetDevice(ctx->device));
     std::unique_ptr<ag_batch> b(new ag_batch());
     b->ctx = ctx;
-    for (int i = 0; i < n; i++) {
+    b->arena.reset(new Arena());
+    for (int i = 0; i < n; i++)
         if (problems[i] && (problems[i]->floating_grid || problems[i]->constriction_grid)) {
             set_last_error("ag_batch_create: batches compute the energy maps only (no fmap/cmap)");
             return AG_ERR_UNSUPPORTED;
         }
-        ag_plan *pl = nullptr;
-        ag_status st = make_plan(ctx, problems[i], &o, true, &pl);
-        if (st != AG_OK) {
-            set_last_error("instance " + std::to_string(i) + ": " + ag_last_error());
-            return st;
+    // Instance plans (validation, cell lists, packed atoms, tables, uploads)
+    // are built by a pool of host threads; device buffers come from the arena.
+    b->plans.resize(n);
+    std::vector<ag_status> sts(n, AG_OK);
+    std::vector<std::string> errs(n);
+    std::atomic<int> next{0};
+    auto worker = [&]() {
+        if (cudaSetDevice(ctx->device) != cudaSuccess) return;
+        for (int i; (i = next.fetch_add(1)) < n;) {
+            ag_plan *pl = nullptr;
+            sts[i] = make_plan(ctx, problems[i], &o, true, &pl, b->arena.get());
+            if (sts[i] != AG_OK) errs[i] = ag_last_error();
+            b->plans[i].reset(pl);
         }
-        b->plans.emplace_back(pl);
-    }
+    };
+    const int nthreads = std::max(1, std::min({n, 16, (int)std::thread::hardware_concurrency()}));
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nthreads; t++) pool.emplace_back(worker);
+    worker();
+    for (auto &t : pool) t.join();
+    for (int i = 0; i < n; i++)
+        if (sts[i] != AG_OK || !b->plans[i]) {
+            set_last_error("instance " + std::to_string(i) + ": " + errs[i]);
+            return sts[i] != AG_OK ? sts[i] : AG_ERR_CUDA;
+        }
     // work order: instances by decreasing far work (largest units first)
     std::vector<int> order(n);
     for (int i = 0; i < n; i++) order[i] = i;
