@@ -433,12 +433,16 @@ class Batch:
             pass
 
 
-def compute_batch(ctx: Context, problems: list) -> list:
+def compute_batch(ctx: Context, problems: list, outs: list | None = None) -> list:
     """One-shot batched computation (ag_maps_compute_batch): host inputs in,
-    host maps out, no autotuning."""
+    host maps out (into `outs` when given), no autotuning."""
     structs = [p.struct() for p in problems]
     arr = (C.POINTER(ag_problem) * len(structs))(*[C.pointer(s) for s in structs])
-    outs = [np.empty(p.map_shape, dtype=np.float32) for p in problems]
+    if outs is None:
+        outs = [np.empty(p.map_shape, dtype=np.float32) for p in problems]
+    for p, o in zip(problems, outs):
+        if o.dtype != np.float32 or not o.flags.c_contiguous or o.size != int(np.prod(p.map_shape)):
+            raise ValueError("each output must be a C-contiguous float32 array of its problem's map shape")
     ptrs = (C.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
     opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST)
     check(ctx._lib.ag_maps_compute_batch(ctx._h, arr, len(problems), C.byref(opts), ptrs))
