@@ -339,6 +339,7 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
     }
     pl->groups.clear();
     pl->any_cov = false;
+    std::vector<uint8_t> skip_map(std::max(nAM, 1), 0);  // ACT_SKIP for every class: table column left zero
     size_t im = 0, ip = 0;
     do {
         NearGroup g;
@@ -356,10 +357,20 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
             g.cov[k] = (uint8_t)(p->map_is_covalent[m] ? 1 : 0);
             if (g.cov[k]) pl->any_cov = true;
             for (int hb = 0; hb < 8; hb++) g.actw[hb] |= (unsigned long long)act[m][hb] << (3 * k);
+            skip_map[m] = 1;
+            for (int hb = 0; hb < 8; hb++) skip_map[m] &= act[m][hb] == ACT_SKIP ? 1 : 0;
             // desolvation lands on the affinity map, or on its partner when maps are separate
             const bool gets_desolv = !g.cov[k] && (p->separate_desolvation_maps ? (bool)is_partner[m] : true);
             g.sp[k] = gets_desolv ? p->map_solpar_probe[m] : 0.0;
             g.vp[k] = gets_desolv ? p->map_vol_probe[m] : 0.0;
+        }
+        for (int hb = 0; hb < 8; hb++) {
+            bool plain = true;
+            for (int k = 0; k < g.ng; k++) {
+                const int a = (int)((g.actw[hb] >> (3 * k)) & 7ull);
+                plain &= (a == ACT_PLAIN || a == ACT_SKIP);
+            }
+            if (plain) g.plain_hb |= 1u << hb;
         }
         pl->groups.push_back(g);
     } while (im < mm_maps.size() || ip < plain_maps.size());
@@ -371,6 +382,7 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
     for (const NearGroup &g : pl->groups)
         for (int k = 0; k < g.ng; k++) {
             const int m = g.out_map[k];
+            if (skip_map[m]) continue;
             for (int t = 0; t < p->n_rec_types; t++)
                 for (int b = 0; b < AG_NEINT; b++)
                     vdwT[((size_t)t * AG_NEINT + b) * pl->mpad + g.col0 + k] =

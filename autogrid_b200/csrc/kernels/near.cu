@@ -46,23 +46,44 @@ struct PairQ {
 
 // FP64, expression-for-expression restatement of main.cpp:3037-3272 for one
 // (point, atom) pair.  Explicit _rn intrinsics keep nvcc from contracting.
-__device__ __noinline__ void pair_exact(const DevProblem &p, int ia, double cx, double cy, double cz,
-                                        int ch, PairQ<double> &o)
+// The distance part: LOOP 2's distance, cutoff and bins (main.cpp:3037-3046,
+// :3309-3311) and LOOP 1's nested-hypot distance and 1/max(r, 0.5)
+// (main.cpp:2951-2956).  Returns the pair vector and r.
+template <class R>
+__device__ __forceinline__ void dist_exact(const DevProblem &p, int ia, double cx, double cy, double cz, PairQ<R> &o,
+                                           double &d0, double &d1, double &d2, double &r_out)
 {
-    const double d0 = __dsub_rn(p.x[ia], cx), d1 = __dsub_rn(p.y[ia], cy), d2 = __dsub_rn(p.z[ia], cz);
+    d0 = __dsub_rn(p.x[ia], cx); d1 = __dsub_rn(p.y[ia], cy); d2 = __dsub_rn(p.z[ia], cz);
     double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
     double re = hypot(d0, hypot(d1, d2));
     o.ad4_in = !(r > AG_NBC);
     if (p.disorder_h && p.disorder[ia] && p.type[ia] == p.hydrogen_type) o.ad4_in = 0;
     if (r < APPROX_ZERO_D) r = APPROX_ZERO_D;
     if (re < APPROX_ZERO_D) re = APPROX_ZERO_D;
-    o.r = r;
-    o.inv_rmax = __ddiv_rn(1.0, re > 0.5 ? re : 0.5);
+    o.r = (R)r;
+    o.inv_rmax = (R)__ddiv_rn(1.0, re > 0.5 ? re : 0.5);
     o.bin = __double2int_rz(__dmul_rn(r, (double)AG_A_DIV));
     o.bin_e = __double2int_rz(__dmul_rn(re, (double)AG_A_DIV));
     int ih = __double2int_rz(__dmul_rn(__dsub_rn(r, 1.10), (double)AG_A_DIV));
     ih = ih < 0 ? 0 : ih;
     o.ih = ih > AG_NEINT - 1 ? AG_NEINT - 1 : ih;
+    r_out = r;
+}
+
+// Distance part only, for FP32 pairs whose distance lies within its error
+// bound of a bin edge; the directional factors stay FP32.
+__device__ __noinline__ void dist_exact_f(const DevProblem &p, int ia, double cx, double cy, double cz,
+                                          PairQ<float> &o)
+{
+    double d0, d1, d2, r;
+    dist_exact(p, ia, cx, cy, cz, o, d0, d1, d2, r);
+}
+
+__device__ __noinline__ void pair_exact(const DevProblem &p, int ia, double cx, double cy, double cz,
+                                        int ch, PairQ<double> &o)
+{
+    double d0, d1, d2, r;
+    dist_exact(p, ia, cx, cy, cz, o, d0, d1, d2, r);
     o.racc = 1.0; o.rdon = 1.0; o.Hramp = 1.0;
     const double inv_r = __ddiv_rn(1.0, r);
     const double dn0 = __dmul_rn(d0, inv_r), dn1 = __dmul_rn(d1, inv_r), dn2 = __dmul_rn(d2, inv_r);
@@ -151,11 +172,11 @@ constexpr int META_DIS = 1 << 11;           // disorder flag
 constexpr int META_RVZERO = 1 << 12;        // bond vector exactly zero
 constexpr int META_SKIP_AD4 = 1 << 13;      // disordered hydrogen skipped by LOOP 2 (main.cpp:3052)
 
-// FP32 pair quantities from the canonical frame-relative distance and the
-// atom's staged metadata / bond vectors.  Returns false when any quantity is
-// within its error bound of a discontinuity; the caller then uses pair_exact().
-__device__ __forceinline__ bool pair_fast(int meta, float4 rvA, float4 rvB, int ia, float dX, float dY, float dZ,
-                                          float t, float rs, int ch, float3 rvh, PairQ<float> &o)
+// FP32 distance quantities from the canonical frame-relative distance t (in
+// bins).  Returns false when t (or the disordered-hydrogen row bin) lies
+// within its error bound of a bin edge (the 8 A cutoff is bin 1024); the
+// caller then takes the distance part from dist_exact_f().
+__device__ __forceinline__ bool dist_fast(int meta, float t, float rs, PairQ<float> &o)
 {
     const float tf = floorf(t);
     if (t - tf < GUARD_BIN || (tf + 1.f) - t < GUARD_BIN || t < 1.0f) return false;
@@ -164,11 +185,8 @@ __device__ __forceinline__ bool pair_fast(int meta, float4 rvA, float4 rvB, int 
     o.ad4_in = (t < FAR_T0) && !(meta & META_SKIP_AD4);  // t is not within GUARD_BIN of 1024: equals r <= 8
     o.r = t * (1.0f / AG_A_DIV);
     o.inv_rmax = fminf((float)AG_A_DIV * rs, 2.0f);
-    o.racc = 1.f; o.rdon = 1.f; o.Hramp = 1.f;
     o.ih = 0;
-    if (!o.ad4_in) return true;
-    const bool dis = (meta & META_DIS) != 0;
-    if (dis) {
+    if (o.ad4_in && (meta & META_DIS)) {
         const float xh = t - 140.8f;  // (r - 1.10) * A_DIV
         if (xh > 0.5f) {
             const float xf = floorf(xh);
@@ -176,6 +194,17 @@ __device__ __forceinline__ bool pair_fast(int meta, float4 rvA, float4 rvB, int 
             o.ih = min((int)xf, AG_NEINT - 1);
         }
     }
+    return true;
+}
+
+// FP32 directional factors (racc, rdon, Hramp) from the unit pair vector and
+// the atom's staged bond vectors.  Returns false when cos_theta lies within
+// its error bound of the D1/A2 branch at 0; the caller then uses pair_exact().
+__device__ __forceinline__ bool angular_fast(int meta, float4 rvA, float4 rvB, int ia, float dX, float dY, float dZ,
+                                             float rs, int ch, float3 rvh, PairQ<float> &o)
+{
+    o.racc = 1.f; o.rdon = 1.f; o.Hramp = 1.f;
+    const bool dis = (meta & META_DIS) != 0;
     const int hb = (meta >> META_HB_SHIFT) & 7;
     if (hb != 2 && hb != 4 && hb != 5) return true;
     const float dn0 = dX * rs, dn1 = dY * rs, dn2 = dZ * rs;
@@ -449,7 +478,12 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                     if (t >= FAR_T0 + GUARD_BIN) continue;
                     e_pair = t < FAR_T0;  // the far-field kernel skips exactly these pairs
                     PairQ<float> qf;
-                    if (!pair_fast(meta, S.a[j], S.b[j], ia, dX, dY, dZ, t, rs, ch, rvh, qf)) {
+                    if (!dist_fast(meta, t, rs, qf)) {
+                        dist_exact_f(p, ia, cx, cy, cz, qf);
+                        n_fb++;
+                    }
+                    qf.racc = 1.f; qf.rdon = 1.f; qf.Hramp = 1.f;
+                    if (qf.ad4_in && !angular_fast(meta, S.a[j], S.b[j], ia, dX, dY, dZ, rs, ch, rvh, qf)) {
                         PairQ<double> qd;
                         pair_exact(p, ia, cx, cy, cz, ch, qd);
                         qf.ad4_in = qd.ad4_in; qf.bin = qd.bin; qf.bin_e = qd.bin_e; qf.ih = qd.ih;
@@ -480,6 +514,16 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                 const float4 *Trow = (const float4 *)(ptr.vdwT + ((size_t)ta * AG_NEINT + kn) * ptr.mpad + g.col0);
                 const float4 *Hrow = (g.has_hrow && dis && p.hydrogen_type >= 0)
                     ? (const float4 *)(ptr.vdwT + ((size_t)p.hydrogen_type * AG_NEINT + q.ih) * ptr.mpad + g.col0) : Trow;
+                if ((g.plain_hb >> hb) & 1u) {  // every map a plain sum for this class (most atoms)
+#pragma unroll
+                    for (int m4 = 0; m4 < NG_MAX / 4; m4++) {
+                        if (4 * m4 >= g.ng) break;
+                        const float4 T4 = __ldg(Trow + m4);
+                        E[4 * m4] += (R)T4.x; E[4 * m4 + 1] += (R)T4.y;
+                        E[4 * m4 + 2] += (R)T4.z; E[4 * m4 + 3] += (R)T4.w;
+                    }
+                    continue;
+                }
                 const unsigned long long aw = g.actw[hb];
 #pragma unroll
                 for (int m4 = 0; m4 < NG_MAX / 4; m4++) {

@@ -28,6 +28,8 @@ struct NearGroup {
     int has_hrow;              // some action reads the hydrogen row (disorder_h)
     int col0;                  // first column of this launch's maps in the [type][bin][col] table
     unsigned long long actw[8];  // per receptor hbond class: 3-bit action of kernel map m at bits 3m..3m+2
+    unsigned plain_hb;         // bit hb: every map of this launch is ACT_PLAIN or ACT_SKIP for class hb
+                               // (the table columns of ACT_SKIP maps are zero, so all T can be added)
     int out_map[NG_MAX];       // output map index of kernel map m
     uint8_t cov[NG_MAX];
     double sp[NG_MAX], vp[NG_MAX];  // desolvation factors applied to this map's output
