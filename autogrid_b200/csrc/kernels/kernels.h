@@ -22,6 +22,7 @@ struct NearPtrs {
 struct NearSmem {
     float4 pos[NB_CHUNK_MAX], a[NB_CHUNK_MAX], b[NB_CHUNK_MAX];
     int meta[NB_CHUNK_MAX], idx[NB_CHUNK_MAX];
+    int hl[NB_CHUNK_MAX], nh;  // staged DS/D1 candidates (slots in this chunk), any order
     float etab[NT_SMALL], sol[NT_SMALL];
     int seg_start[NB_SEGS_MAX], seg_off[NB_SEGS_MAX + 1];
     int total;

@@ -344,7 +344,10 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                                    frame_atom_coord(p.z[a] * AG_A_DIV, Z0), (float)p.q[a]);
             S.a[i] = ptr.atomA[a];
             S.b[i] = ptr.atomB[a];
-            S.meta[i] = ptr.meta[a];
+            const int m = ptr.meta[a];
+            S.meta[i] = m;
+            const int hb = (m >> META_HB_SHIFT) & 7;
+            if (hb == 1 || hb == 2) S.hl[atomicAdd(&S.nh, 1)] = i;
         }
     };
     auto layout_segments = [&](int sb, int nseg) {
@@ -361,6 +364,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
             }
             S.seg_off[nseg] = off;
             S.total = off;
+            S.nh = 0;
         }
     };
     // the candidate list fits one chunk in the common case: stage it once
@@ -392,6 +396,8 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                 const int nc = min(NB_CHUNK, total - c0);
                 if (!resident) {
                     __syncthreads();
+                    if (tid == 0) S.nh = 0;
+                    __syncthreads();
                     stage(c0, nc);
                     __syncthreads();
                 }
@@ -403,11 +409,10 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     int ch = -1;
     if (need_h) {
         float best2 = 3.0e38f;
-        for_each_chunk([&](int nc) {
+        for_each_chunk([&](int) {
             if (!valid) return;
-            for (int j = 0; j < nc; j++) {
-                const int hb = (S.meta[j] >> META_HB_SHIFT) & 7;
-                if (hb != 1 && hb != 2) continue;
+            for (int k = 0; k < S.nh; k++) {
+                const int j = S.hl[k];
                 const float4 A = S.pos[j];
                 const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
                 best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
@@ -415,11 +420,10 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
         });
         const float lim = best2 * (1.0f + 2.0e-5f) + 4.0f;
         double rmin = 999999.;
-        for_each_chunk([&](int nc) {
+        for_each_chunk([&](int) {
             if (!valid) return;
-            for (int j = 0; j < nc; j++) {
-                const int hb = (S.meta[j] >> META_HB_SHIFT) & 7;
-                if (hb != 1 && hb != 2) continue;
+            for (int k = 0; k < S.nh; k++) {
+                const int j = S.hl[k];
                 const float4 A = S.pos[j];
                 const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
                 if (dx * dx + dy * dy + dz * dz > lim) continue;
