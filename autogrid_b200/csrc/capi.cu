@@ -608,7 +608,7 @@ struct ag_batch {
     long long *d_far_begin = nullptr, *d_near_begin = nullptr;
     unsigned long long *d_counters = nullptr;  // [0] far units, [1] near units, [2..3] near statistics
     ag_tuning tune{};
-    int far_ctas_per_sm = 3, near_ctas_per_sm = 2;
+    int far_ctas_per_sm = 3, near_ctas_per_sm = 3;  // resident CTAs per SM of the persistent kernels
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     ~ag_batch()

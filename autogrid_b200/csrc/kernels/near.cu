@@ -27,6 +27,9 @@
 namespace agb {
 
 constexpr int NB_THREADS = 256;   // one thread per brick point (brick shape is a template parameter)
+#ifndef NEAR_MIN_CTAS
+#define NEAR_MIN_CTAS 3              // resident CTAs per SM the register allocation targets
+#endif
 constexpr int NB_CHUNK = NB_CHUNK_MAX;   // candidates staged at once (most bricks need one chunk)
 constexpr int NB_SEGS = NB_SEGS_MAX;
 constexpr float GUARD_BIN = 2.0e-3f;   // bins: > 3x the FP32 distance error bound
@@ -210,7 +213,6 @@ __device__ __forceinline__ bool angular_fast(int meta, float4 rvA, float4 rvB, i
     const float dn0 = dX * rs, dn1 = dY * rs, dn2 = dZ * rs;
     const float rv0 = rvA.x, rv1 = rvA.y, rv2 = rvA.z;
     const float cos_theta = ((0.f - dn0 * rv0) - dn1 * rv1) - dn2 * rv2;
-    const float PIH = 1.57079632679489662f;
     // An atom without bonded neighbours keeps a zero bond vector; its cos_theta
     // is exactly 0 in every precision, so the branch at 0 is not ambiguous.
     const bool rv_zero = (meta & META_RVZERO) != 0;
@@ -312,8 +314,10 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                  Z0 = frame_origin_bins(oz, p.nez, sp128);
     const float PX = frame_point_coord(ix - ox, sp128), PY = frame_point_coord(iy - oy, sp128),
                 PZ = frame_point_coord(iz - oz, sp128);
-    const double cx = (double)(ix - p.nex) * p.spacing, cy = (double)(iy - p.ney) * p.spacing,
-                 cz = (double)(iz - p.nez) * p.spacing;
+    // FP64 point coordinates (main.cpp:2815-2859), formed where a pair needs them
+    auto cx = [&]() { return (double)(ix - p.nex) * p.spacing; };
+    auto cy = [&]() { return (double)(iy - p.ney) * p.spacing; };
+    auto cz = [&]() { return (double)(iz - p.nez) * p.spacing; };
 
     const bool need_h = p.n_atom_maps > 0;
     const bool do_e = !EXACT && g.write_special && p.elec_map >= 0;
@@ -428,7 +432,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                 const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
                 if (dx * dx + dy * dy + dz * dz > lim) continue;
                 const int a = S.idx[j];
-                const double r = h_dist(p, a, cx, cy, cz);
+                const double r = h_dist(p, a, cx(), cy(), cz());
                 if (r < rmin || (r == rmin && a < ch)) { rmin = r; ch = a; }
             }
         });
@@ -437,7 +441,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
             ch = -1;
             for (int k = 0; k < p.n_h; k++) {
                 const int a = p.h_index[k];
-                const double r = h_dist(p, a, cx, cy, cz);
+                const double r = h_dist(p, a, cx(), cy(), cz());
                 if (r < rmin) { rmin = r; ch = a; }
             }
         }
@@ -453,7 +457,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     for (int m = 0; m < NG_MM; m++) { hmin[m] = 999999.; hmax[m] = -999999.; }
     uint32_t hflag = 0;
     R D1 = 0, D2 = 0, e_near = 0;
-    unsigned long long n_near = 0, n_fb = 0;
+    unsigned n_near = 0, n_fb = 0;
     if (need_pairs) {
         for_each_chunk([&](int nc) {
             if (!valid) return;
@@ -463,11 +467,11 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                 PairQ<R> q;
                 bool e_pair = false;
                 if (EXACT) {
-                    const double d0 = __dsub_rn(p.x[ia], cx), d1 = __dsub_rn(p.y[ia], cy), d2 = __dsub_rn(p.z[ia], cz);
+                    const double d0 = __dsub_rn(p.x[ia], cx()), d1 = __dsub_rn(p.y[ia], cy()), d2 = __dsub_rn(p.z[ia], cz());
                     const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
                     if (r2 > AG_NBC * AG_NBC * 1.0001) continue;
                     PairQ<double> qd;
-                    pair_exact(p, ia, cx, cy, cz, ch, qd);
+                    pair_exact(p, ia, cx(), cy(), cz(), ch, qd);
                     if (!qd.ad4_in) continue;
                     q.ad4_in = 1; q.bin = qd.bin; q.bin_e = qd.bin_e; q.ih = qd.ih;
                     q.r = (R)qd.r; q.inv_rmax = (R)qd.inv_rmax; q.racc = (R)qd.racc; q.rdon = (R)qd.rdon; q.Hramp = (R)qd.Hramp;
@@ -483,13 +487,13 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                     e_pair = t < FAR_T0;  // the far-field kernel skips exactly these pairs
                     PairQ<float> qf;
                     if (!dist_fast(meta, t, rs, qf)) {
-                        dist_exact_f(p, ia, cx, cy, cz, qf);
+                        dist_exact_f(p, ia, cx(), cy(), cz(), qf);
                         n_fb++;
                     }
                     qf.racc = 1.f; qf.rdon = 1.f; qf.Hramp = 1.f;
                     if (qf.ad4_in && !angular_fast(meta, S.a[j], S.b[j], ia, dX, dY, dZ, rs, ch, rvh, qf)) {
                         PairQ<double> qd;
-                        pair_exact(p, ia, cx, cy, cz, ch, qd);
+                        pair_exact(p, ia, cx(), cy(), cz(), ch, qd);
                         qf.ad4_in = qd.ad4_in; qf.bin = qd.bin; qf.bin_e = qd.bin_e; qf.ih = qd.ih;
                         qf.r = (float)qd.r; qf.inv_rmax = (float)qd.inv_rmax; qf.racc = (float)qd.racc;
                         qf.rdon = (float)qd.rdon; qf.Hramp = (float)qd.Hramp;
@@ -594,8 +598,8 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
         }
     }
     if (ptr.counters) {
-        atomicAdd(&S.cnt[0], n_near);
-        atomicAdd(&S.cnt[1], n_fb);
+        atomicAdd(&S.cnt[0], (unsigned long long)n_near);
+        atomicAdd(&S.cnt[1], (unsigned long long)n_fb);
         __syncthreads();
         if (tid == 0) {
             atomicAdd(ptr.counters + 0, S.cnt[0]);
@@ -606,7 +610,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
 
 // Single instance: one CTA per brick.
 template <bool EXACT, int BX, int BY, int BZ>
-__global__ void __launch_bounds__(NB_THREADS, 2) k_near(DevProblem p, NearGroup g, NearPtrs ptr)
+__global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS) k_near(DevProblem p, NearGroup g, NearPtrs ptr)
 {
     __shared__ NearSmem S;
     near_unit<EXACT, BX, BY, BZ>(p, g, ptr, blockIdx.x, S);
@@ -615,7 +619,7 @@ __global__ void __launch_bounds__(NB_THREADS, 2) k_near(DevProblem p, NearGroup 
 // Many instances, persistent: (instance-group, brick) units from an atomic
 // counter; units never wait on each other.
 template <int BX, int BY, int BZ>
-__global__ void __launch_bounds__(NB_THREADS, 2)
+__global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS)
 k_near_batch(const NearInst *__restrict__ insts, const long long *__restrict__ unit_begin, int n_inst,
              unsigned long long *__restrict__ counter)
 {
