@@ -115,6 +115,10 @@ ag_status invalid(const std::string &m)
 struct ag_context {
     int device = 0;
     cudaStream_t stream = nullptr;
+    // the far-field kernel runs on `side`, concurrently with the near-field
+    // kernel, forked from and joined back to the caller's stream by events
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf0 = nullptr, evf1 = nullptr;
     ag_stats stats{};
     BufferSet pool;
@@ -140,6 +144,8 @@ struct ag_plan {
     double *maps64 = nullptr;
     double *cov = nullptr;
     float *far_partial = nullptr;
+    ReduceInst *d_reduce = nullptr;    // e-map reduction of this plan (one instance)
+    long long *d_reduce_begin = nullptr;
     double *x128 = nullptr, *y128 = nullptr, *z128 = nullptr;
     float *qw = nullptr, *far_tab = nullptr, *etab = nullptr, *solf = nullptr, *vdwT = nullptr;
     float4 *atomA = nullptr, *atomB = nullptr;
@@ -492,8 +498,20 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
     } else {
         pl->far_partial = nullptr;
     }
-    d.far_chunks = (pl->opts.precision == AG_PREC_FP64) ? 0 : pl->n_chunks;
-    d.far_partial = pl->far_partial;
+    if (pl->far_partial && d.elec_map >= 0) {
+        const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * P};
+        const long long beg[2] = {0, d.P};
+        AGB_CK(B->ensure("reduce", sizeof r, &v));
+        pl->d_reduce = (ReduceInst *)v;
+        AGB_CK(B->ensure("reduce_begin", sizeof beg, &v));
+        pl->d_reduce_begin = (long long *)v;
+        AGB_CK(cudaMemcpyAsync(pl->d_reduce, &r, sizeof r, cudaMemcpyHostToDevice, s));
+        AGB_CK(cudaMemcpyAsync(pl->d_reduce_begin, beg, sizeof beg, cudaMemcpyHostToDevice, s));
+        AGB_CK(cudaStreamSynchronize(s));  // sources are locals
+    } else {
+        pl->d_reduce = nullptr;
+        pl->d_reduce_begin = nullptr;
+    }
     return AG_OK;
 }
 
@@ -527,16 +545,19 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
     int launches = 0;
     AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
     AGB_CK(cudaEventRecord(c->ev0, s));
-    if (d.elec_map >= 0) {
-        if (exact) {
-            AGB_CK(launch_emap_exact(d, pl->maps64 + (size_t)d.elec_map * d.P, s));
-            launches++;
-        } else if (pl->n_chunks > 0) {
-            AGB_CK(cudaEventRecord(c->evf0, s));
-            AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, s));
-            AGB_CK(cudaEventRecord(c->evf1, s));
-            launches++;
-        }
+    const bool far = !exact && d.elec_map >= 0 && pl->n_chunks > 0;
+    if (d.elec_map >= 0 && exact) {
+        AGB_CK(launch_emap_exact(d, pl->maps64 + (size_t)d.elec_map * d.P, s));
+        launches++;
+    }
+    if (far) {  // far field on the side stream, concurrent with the near-field kernel
+        AGB_CK(cudaEventRecord(c->fork, s));
+        AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
+        AGB_CK(cudaEventRecord(c->evf0, c->side));
+        AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side));
+        AGB_CK(cudaEventRecord(c->evf1, c->side));
+        AGB_CK(cudaEventRecord(c->join, c->side));
+        launches++;
     }
     if (pl->any_cov) {
         AGB_CK(launch_covalent(d, pl->cov, s));
@@ -559,6 +580,11 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
             AGB_CK(launch_near(exact, d, g, near_ptrs(pl, c->d_counters), 0, s));
             launches++;
         }
+    }
+    if (far) {
+        AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
+        AGB_CK(launch_emap_reduce(pl->d_reduce, pl->d_reduce_begin, 1, d.P, s));
+        launches++;
     }
     AGB_CK(cudaEventRecord(c->ev1, s));
     pl->last_launches = launches;
@@ -603,6 +629,10 @@ struct ag_batch {
     std::vector<NearInst> near;       // per (instance, group), in work order
     std::vector<long long> far_begin, near_begin;
     BufferSet bufs;
+    std::vector<ReduceInst> red;       // e-map reduction per instance with a far field
+    std::vector<long long> red_begin;
+    ReduceInst *d_red = nullptr;
+    long long *d_red_begin = nullptr;
     FarArgs *d_far = nullptr;
     NearInst *d_near = nullptr;
     long long *d_far_begin = nullptr, *d_near_begin = nullptr;
@@ -632,12 +662,16 @@ ag_status batch_upload_far(ag_batch *b, bool chunked)
         a.chunk_atoms = chunked ? std::min(2048, std::max(a.n_atoms, 1)) : std::max(a.n_atoms, 1);
         b->far_begin.push_back(b->far_begin.back() + (a.n_atoms > 0 ? far_units(a) : 0));
     }
-    // the near kernel sums the instance's partial chunks
-    for (NearInst &ni : b->near) {
-        const FarArgs *a = nullptr;
-        for (const FarArgs &f : b->far)
-            if (f.partial == ni.p.far_partial) { a = &f; break; }
-        ni.p.far_chunks = (a && a->n_atoms > 0 && ni.p.elec_map >= 0) ? (a->n_atoms + a->chunk_atoms - 1) / a->chunk_atoms : 0;
+    // e-map reduction: each instance's partial chunks, for this chunking
+    for (size_t i = 0; i < b->far.size(); i++) {
+        const FarArgs &a = b->far[i];
+        b->red[i].n_chunks = a.n_atoms > 0 ? (a.n_atoms + a.chunk_atoms - 1) / a.chunk_atoms : 0;
+    }
+    if (!b->red.empty()) {
+        AGB_CK(cudaMemcpyAsync(b->d_red, b->red.data(), sizeof(ReduceInst) * b->red.size(), cudaMemcpyHostToDevice,
+                               b->ctx->stream));
+        AGB_CK(cudaMemcpyAsync(b->d_red_begin, b->red_begin.data(), sizeof(long long) * b->red_begin.size(),
+                               cudaMemcpyHostToDevice, b->ctx->stream));
     }
     AGB_CK(cudaMemcpyAsync(b->d_far, b->far.data(), sizeof(FarArgs) * b->far.size(), cudaMemcpyHostToDevice, b->ctx->stream));
     AGB_CK(cudaMemcpyAsync(b->d_far_begin, b->far_begin.data(), sizeof(long long) * b->far_begin.size(),
@@ -647,17 +681,33 @@ ag_status batch_upload_far(ag_batch *b, bool chunked)
     return AG_OK;
 }
 
-ag_status batch_launch(ag_batch *b, cudaStream_t s, int tile, int shape, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2)
+// One run of the batch on s.  concurrent: the far-field kernel runs on the
+// context's side stream alongside the near-field kernel (fork/join by
+// events); otherwise they run one after the other (the autotuner times each).
+ag_status batch_launch(ag_batch *b, cudaStream_t s, int tile, int shape, cudaEvent_t e0, cudaEvent_t e1, cudaEvent_t e2,
+                       bool concurrent)
 {
+    ag_context *c = b->ctx;
+    const bool far = b->far_begin.back() > 0;
     AGB_CK(cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(unsigned long long), s));
     if (e0) AGB_CK(cudaEventRecord(e0, s));
-    if (b->far_begin.back() > 0)
+    cudaStream_t fs = s;
+    if (far && concurrent) {
+        AGB_CK(cudaEventRecord(c->fork, s));
+        AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
+        fs = c->side;
+    }
+    if (far)
         AGB_CK(launch_emap_far_batch(b->d_far, b->d_far_begin, (int)b->far.size(), b->d_counters, tile,
-                                     b->far_ctas_per_sm, s));
+                                     b->far_ctas_per_sm, fs));
+    if (far && concurrent) AGB_CK(cudaEventRecord(c->join, fs));
     if (e1) AGB_CK(cudaEventRecord(e1, s));
     if (b->near_begin.back() > 0)
         AGB_CK(launch_near_batch(b->d_near, b->d_near_begin, (int)b->near.size(), b->d_counters + 1, shape,
                                  b->near_ctas_per_sm, s));
+    if (far && concurrent) AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
+    if (!b->red.empty())
+        AGB_CK(launch_emap_reduce(b->d_red, b->d_red_begin, (int)b->red.size(), b->red_begin.back(), s));
     if (e2) AGB_CK(cudaEventRecord(e2, s));
     return AG_OK;
 }
@@ -681,7 +731,7 @@ ag_status batch_time(ag_batch *b, int tile, int shape, double *far_ms, double *n
     double bf = 1e30, bn = 1e30;
     ag_status st = AG_OK;
     for (int rep = 0; rep < 2 && st == AG_OK; rep++) {
-        st = batch_launch(b, s, tile, shape, e[0], e[1], e[2]);
+        st = batch_launch(b, s, tile, shape, e[0], e[1], e[2], false);
         if (st != AG_OK) break;
         cudaError_t ce = cudaEventSynchronize(e[2]);
         if (ce != cudaSuccess) { st = cuda_fail(ce, "cudaEventSynchronize"); break; }
@@ -782,6 +832,9 @@ ag_status ag_context_create(int32_t device, ag_context **out)
     c->device = device;
     AGB_CK(cudaSetDevice(device));
     AGB_CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    AGB_CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
+    AGB_CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    AGB_CK(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
     AGB_CK(cudaEventCreate(&c->ev0));
     AGB_CK(cudaEventCreate(&c->ev1));
     AGB_CK(cudaEventCreate(&c->evf0));
@@ -796,7 +849,11 @@ ag_status ag_context_destroy(ag_context *ctx)
     if (!ctx) return AG_OK;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->side) cudaStreamSynchronize(ctx->side);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
+    if (ctx->fork) cudaEventDestroy(ctx->fork);
+    if (ctx->join) cudaEventDestroy(ctx->join);
+    if (ctx->side) cudaStreamDestroy(ctx->side);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->evf0) cudaEventDestroy(ctx->evf0);
@@ -938,6 +995,7 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
         return (double)a.P * (a.n_atoms + 64) > (double)c.P * (c.n_atoms + 64);
     });
     b->near_begin.assign(1, 0);
+    b->red_begin.assign(1, 0);
     for (int i : order) {
         ag_plan *pl = b->plans[i].get();
         // each instance's partial buffer must hold the chunked layout (at most ceil(N/2048) chunks)
@@ -946,8 +1004,9 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
             void *v = nullptr;
             AGB_CK(pl->bufs->ensure("far_partial", (size_t)max_chunks * (size_t)pl->dp.P * sizeof(float), &v));
             pl->far_partial = (float *)v;
-            pl->dp.far_partial = pl->far_partial;
             b->far.push_back(far_args(pl));
+            b->red.push_back(ReduceInst{pl->dp.P, 0, pl->far_partial, pl->maps32 + (size_t)pl->dp.elec_map * pl->dp.P});
+            b->red_begin.push_back(b->red_begin.back() + pl->dp.P);
         }
         const bool need_near = pl->dp.n_atom_maps > 0 || pl->dp.dsolv_map >= 0 || pl->dp.elec_map >= 0;
         if (need_near)
@@ -975,6 +1034,10 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     b->d_near_begin = (long long *)v;
     AGB_CK(b->bufs.ensure("counters", 4 * sizeof(unsigned long long), &v));
     b->d_counters = (unsigned long long *)v;
+    AGB_CK(b->bufs.ensure("reduce", sizeof(ReduceInst) * std::max<size_t>(1, b->red.size()), &v));
+    b->d_red = (ReduceInst *)v;
+    AGB_CK(b->bufs.ensure("reduce_begin", sizeof(long long) * b->red_begin.size(), &v));
+    b->d_red_begin = (long long *)v;
     if (b->far.empty()) b->far_begin.assign(1, 0);
     ag_status st = batch_set_near_shape(b.get(), 0);
     if (st != AG_OK) return st;
@@ -996,7 +1059,7 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     AGB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     AGB_CK(cudaStreamSynchronize(ctx->stream));
     AGB_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    st = batch_launch(b.get(), cs, b->tune.far_tile, b->tune.near_shape, nullptr, nullptr, nullptr);
+    st = batch_launch(b.get(), cs, b->tune.far_tile, b->tune.near_shape, nullptr, nullptr, nullptr, true);
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(cs, &g);
     cudaStreamDestroy(cs);

@@ -110,9 +110,6 @@ struct DevProblem {
     const float *vdw;                  // [types][atom_maps][NEINT]
     const double *sol_fn, *reps;       // [NDIEL]
     const float *far_tab;              // [NDIEL] 0 below FAR_BIN0, energy factor above
-    // far-field partial sums [n_chunks][P]
-    int far_chunks;
-    const float *far_partial;
 };
 
 }  // namespace agb

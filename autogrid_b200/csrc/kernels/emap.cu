@@ -9,13 +9,17 @@
 //                tiles; each thread keeps 8 grid points of one x-row in
 //                registers (two-level summation: per-tile partial + total).
 //                The atom list is split into chunks for load balance; chunk
-//                partial sums land in far_partial[chunk][point] and are added
-//                in fixed chunk order by the near-field kernel (deterministic).
+//                partial sums land in far_partial[chunk][point].
+// k_emap_reduce -- the e map: chunk partials added in fixed chunk order, then
+//                the near-field part the near kernel left in the map
+//                (deterministic; lets the far and near kernels run
+//                concurrently).
 // k_emap_exact -- FP64 twin: every pair, exactly the reference expression
 //                (nested hypot, double table), file order summation.
 #include <algorithm>
 
 #include "agb_device.cuh"
+#include "kernels.h"
 
 namespace agb {
 
@@ -266,6 +270,38 @@ cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_be
     if (tile == 256) return far_batch_t<256>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
     if (tile == 1024) return far_batch_t<1024>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
     return far_batch_t<512>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+}
+
+// One thread per point of every instance: instance i owns points
+// [begin[i], begin[i+1]) of the flattened range.
+__global__ void __launch_bounds__(256) k_emap_reduce(const ReduceInst *__restrict__ insts,
+                                                     const long long *__restrict__ begin, int n)
+{
+    const long long total = begin[n];
+    for (long long u = (long long)blockIdx.x * blockDim.x + threadIdx.x; u < total;
+         u += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (begin[mid] <= u) lo = mid;
+            else hi = mid - 1;
+        }
+        const ReduceInst r = insts[lo];
+        const long long lin = u - begin[lo];
+        float e = 0.f;
+        for (int c = 0; c < r.n_chunks; c++) e += r.partial[(size_t)c * (size_t)r.P + (size_t)lin];
+        r.out[lin] = e + r.out[lin];
+    }
+}
+
+cudaError_t launch_emap_reduce(const ReduceInst *insts, const long long *begin, int n, long long total,
+                               cudaStream_t s)
+{
+    if (n <= 0 || total <= 0) return cudaSuccess;
+    const long long want = (total + 255) / 256;
+    const unsigned nb = (unsigned)std::min<long long>(want, 148LL * 16);
+    k_emap_reduce<<<nb, 256, 0, s>>>(insts, begin, n);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s)

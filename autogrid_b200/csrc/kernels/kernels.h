@@ -40,6 +40,15 @@ size_t far_smem_bytes(int tile);
 cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s);
 cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_begin, int n_inst,
                                   unsigned long long *counter, int tile, int ctas_per_sm, cudaStream_t s);
+// One instance of the e-map reduction: out[lin] = sum_c partial[c][lin] + out[lin].
+struct ReduceInst {
+    long long P;
+    int n_chunks;
+    const float *partial;
+    float *out;
+};
+cudaError_t launch_emap_reduce(const ReduceInst *insts, const long long *begin, int n, long long total,
+                               cudaStream_t s);
 cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s);
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s);
 cudaError_t launch_distance_maps(const DevProblem &p, double cutoff, float *fmap32, float *cmap32, double *fmap64,

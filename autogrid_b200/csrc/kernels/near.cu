@@ -590,11 +590,8 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                 const R d = (R)p.solpar_q * D1;
                 if (EXACT) ptr.out64[o] = (double)d; else ptr.out32[o] = (float)d;
             }
-            if (do_e) {
-                float e = 0.f;
-                for (int c = 0; c < p.far_chunks; c++) e += p.far_partial[(size_t)c * (size_t)p.P + (size_t)lin];
-                ptr.out32[(size_t)p.elec_map * (size_t)p.P + (size_t)lin] = e + (float)e_near;
-            }
+            if (do_e)  // the near part of the e map; k_emap_reduce adds the far-field chunks
+                ptr.out32[(size_t)p.elec_map * (size_t)p.P + (size_t)lin] = (float)e_near;
         }
     }
     if (ptr.counters) {
