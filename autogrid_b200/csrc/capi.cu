@@ -110,6 +110,11 @@ ag_status invalid(const std::string &m)
     return AG_ERR_INVALID;
 }
 
+// One-shot calls: z-slab height of the copy/compute pipeline (whole far-field
+// frames and near-field brick rows) and the most slabs one call uses.
+constexpr int kSlabZ = 32;
+constexpr int kMaxSlabs = 16;
+
 }  // namespace
 
 struct ag_context {
@@ -119,6 +124,11 @@ struct ag_context {
     // kernel, forked from and joined back to the caller's stream by events
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
+    // one-shot calls copy finished z-slabs of the maps back on `copy` while
+    // later slabs compute (per-slab completion events)
+    cudaStream_t copy = nullptr;
+    std::vector<cudaEvent_t> far_done, red_done;
+    cudaEvent_t copy_done = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf0 = nullptr, evf1 = nullptr;
     ag_stats stats{};
     BufferSet pool;
@@ -519,6 +529,7 @@ FarArgs far_args(const ag_plan *pl)
 {
     const DevProblem &d = pl->dp;
     FarArgs a;
+    std::memset(&a, 0, sizeof a);
     a.ax128 = pl->x128; a.ay128 = pl->y128; a.az128 = pl->z128; a.qw = pl->qw;
     a.far_tab = pl->far_tab; a.partial = pl->far_partial;
     a.spacing_adiv = d.spacing * AG_A_DIV; a.P = d.P;
@@ -835,6 +846,14 @@ ag_status ag_context_create(int32_t device, ag_context **out)
     AGB_CK(cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking));
     AGB_CK(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
     AGB_CK(cudaEventCreateWithFlags(&c->join, cudaEventDisableTiming));
+    AGB_CK(cudaStreamCreateWithFlags(&c->copy, cudaStreamNonBlocking));
+    AGB_CK(cudaEventCreateWithFlags(&c->copy_done, cudaEventDisableTiming));
+    c->far_done.resize(kMaxSlabs);
+    c->red_done.resize(kMaxSlabs);
+    for (int k = 0; k < kMaxSlabs; k++) {
+        AGB_CK(cudaEventCreateWithFlags(&c->far_done[k], cudaEventDisableTiming));
+        AGB_CK(cudaEventCreateWithFlags(&c->red_done[k], cudaEventDisableTiming));
+    }
     AGB_CK(cudaEventCreate(&c->ev0));
     AGB_CK(cudaEventCreate(&c->ev1));
     AGB_CK(cudaEventCreate(&c->evf0));
@@ -850,6 +869,11 @@ ag_status ag_context_destroy(ag_context *ctx)
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->side) cudaStreamSynchronize(ctx->side);
+    if (ctx->copy) cudaStreamSynchronize(ctx->copy);
+    for (cudaEvent_t e : ctx->far_done) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->red_done) cudaEventDestroy(e);
+    if (ctx->copy_done) cudaEventDestroy(ctx->copy_done);
+    if (ctx->copy) cudaStreamDestroy(ctx->copy);
     if (ctx->d_counters) cudaFree(ctx->d_counters);
     if (ctx->fork) cudaEventDestroy(ctx->fork);
     if (ctx->join) cudaEventDestroy(ctx->join);
@@ -872,6 +896,79 @@ ag_status ag_context_stats(const ag_context *ctx, ag_stats *out)
     return AG_OK;
 }
 
+// One-shot FP32 run with the maps copied to `out` slab by slab: every
+// far-field slab runs back to back on the side stream; the near-field kernel of
+// slab k runs on the main stream, then waits for far slab k and reduces the e
+// map of slab k; the copy stream brings slab k back while later slabs compute.
+// All kernels are enqueued before the copies, so a pageable destination (whose
+// copies block the host) does not delay the launches.
+static ag_status run_plan_pipelined(ag_plan *pl, void *out, size_t n_out)
+{
+    ag_context *c = pl->ctx;
+    const DevProblem &d = pl->dp;
+    cudaStream_t s = c->stream;
+    const int nslab = std::min(kMaxSlabs, (d.n1z + kSlabZ - 1) / kSlabZ);
+    const long long plane = (long long)d.n1x * d.n1y;
+    const bool far = d.elec_map >= 0 && pl->n_chunks > 0;
+    int launches = 0;
+    AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+    AGB_CK(cudaEventRecord(c->ev0, s));
+    if (pl->any_cov) {
+        AGB_CK(launch_covalent(d, pl->cov, s));
+        launches++;
+    }
+    if (pl->floating || pl->constriction) {
+        const size_t P = (size_t)d.P, f = (size_t)d.n_maps * P, cc = f + (size_t)pl->floating * P;
+        AGB_CK(launch_distance_maps(d, pl->constriction_cutoff, pl->floating ? pl->maps32 + f : nullptr,
+                                    pl->constriction ? pl->maps32 + cc : nullptr, nullptr, nullptr, s));
+        launches++;
+    }
+    if (far) {
+        AGB_CK(cudaEventRecord(c->fork, s));
+        AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
+        AGB_CK(cudaEventRecord(c->evf0, c->side));
+        for (int k = 0; k < nslab; k++) {
+            const int fz0 = k * (kSlabZ / FRAME_Z), fz1 = (k == nslab - 1) ? -1 : fz0 + kSlabZ / FRAME_Z;
+            AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, fz0, fz1));
+            AGB_CK(cudaEventRecord(c->far_done[k], c->side));
+            launches++;
+        }
+        AGB_CK(cudaEventRecord(c->evf1, c->side));
+    }
+    const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || d.elec_map >= 0;
+    for (int k = 0; k < nslab; k++) {
+        const int bz0 = k * (kSlabZ / 4), bz1 = (k == nslab - 1) ? -1 : bz0 + kSlabZ / 4;  // 8x8x4 bricks
+        if (need_near)
+            for (const NearGroup &g : pl->groups) {
+                AGB_CK(launch_near(false, d, g, near_ptrs(pl, c->d_counters), 0, s, bz0, bz1));
+                launches++;
+            }
+        if (far) {
+            const long long z0 = (long long)k * kSlabZ, z1 = std::min<long long>(d.n1z, z0 + kSlabZ);
+            const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * d.P};
+            AGB_CK(cudaStreamWaitEvent(s, c->far_done[k], 0));
+            AGB_CK(launch_emap_reduce_range(r, z0 * plane, z1 * plane, s));
+            launches++;
+        }
+        AGB_CK(cudaEventRecord(c->red_done[k], s));
+    }
+    AGB_CK(cudaEventRecord(c->ev1, s));
+    pl->last_launches = launches;
+    c->pending = true;
+    c->had_far = far;
+    c->last_launches = launches;
+    c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
+    for (int k = 0; k < nslab; k++) {
+        const long long z0 = (long long)k * kSlabZ, z1 = std::min<long long>(d.n1z, z0 + kSlabZ);
+        const size_t off = (size_t)(z0 * plane) * sizeof(float), width = (size_t)((z1 - z0) * plane) * sizeof(float);
+        AGB_CK(cudaStreamWaitEvent(c->copy, c->red_done[k], 0));
+        AGB_CK(cudaMemcpy2DAsync((char *)out + off, (size_t)d.P * sizeof(float), (const char *)pl->maps32 + off,
+                                 (size_t)d.P * sizeof(float), width, n_out, cudaMemcpyDefault, c->copy));
+    }
+    AGB_CK(cudaStreamSynchronize(c->copy));
+    return AG_OK;
+}
+
 static ag_status compute_common(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, void *maps,
                                 size_t elem)
 {
@@ -880,10 +977,16 @@ static ag_status compute_common(ag_context *ctx, const ag_problem *problem, cons
     ag_status st = make_plan(ctx, problem, opts, false, &pl);
     if (st != AG_OK) return st;
     std::unique_ptr<ag_plan> guard(pl);
+    const size_t n_out = (size_t)problem->n_maps + pl->floating + pl->constriction;
+    if (elem == 4 && pl->dp.n1z > kSlabZ) {
+        st = run_plan_pipelined(pl, maps, n_out);
+        if (st != AG_OK) return st;
+        AGB_CK(cudaStreamSynchronize(ctx->stream));
+        return finish_stats(pl);
+    }
     st = run_plan(pl, ctx->stream);
     if (st != AG_OK) return st;
     const void *src = elem == 8 ? (const void *)pl->maps64 : (const void *)pl->maps32;
-    const size_t n_out = (size_t)problem->n_maps + pl->floating + pl->constriction;
     AGB_CK(cudaMemcpyAsync(maps, src, n_out * (size_t)pl->dp.P * elem, cudaMemcpyDefault, ctx->stream));
     AGB_CK(cudaStreamSynchronize(ctx->stream));
     return finish_stats(pl);

@@ -76,6 +76,7 @@ struct FarArgs {
     long long P;
     int n_atoms, chunk_atoms;
     int n1x, n1y, n1z, nex, ney, nez, nfx, nfy, nfz;
+    int frame0;                           // single-instance launches: first frame of the launch
 };
 
 // Device image of one problem instance.

@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
     float4 *s_tab4 = ef_smem;                 // AG_NDIEL floats
     float4 *s_atom = ef_smem + AG_NDIEL / 4;  // TILE entries
     load_far_table(s_tab4, a.far_tab);
-    far_unit<TILE>(a, blockIdx.x, blockIdx.y, s_tab4, s_atom);
+    far_unit<TILE>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
 }
 
 // Many instances, persistent: each CTA takes (instance, frame, chunk) units
@@ -231,10 +231,14 @@ int frames_z(int n1z) { return (n1z + FRAME_Z - 1) / FRAME_Z; }
 
 size_t far_smem_bytes(int tile) { return AG_NDIEL * sizeof(float) + (size_t)tile * sizeof(float4); }
 
-cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s)
+// Frame z-rows [fz0, fz1) of one instance (fz1 < 0: through the last).
+cudaError_t launch_emap_far(const FarArgs &args, int n_chunks, int tile, cudaStream_t s, int fz0, int fz1)
 {
-    const int frames = a.nfx * a.nfy * a.nfz;
-    dim3 grid((unsigned)frames, (unsigned)n_chunks);
+    FarArgs a = args;
+    if (fz1 < 0 || fz1 > a.nfz) fz1 = a.nfz;
+    if (fz0 >= fz1) return cudaSuccess;
+    a.frame0 = fz0 * a.nfx * a.nfy;
+    dim3 grid((unsigned)(a.nfx * a.nfy * (fz1 - fz0)), (unsigned)n_chunks);
     const size_t smem = far_smem_bytes(tile);
     if (tile == 256) k_emap_far<256><<<grid, EF_THREADS, smem, s>>>(a);
     else if (tile == 1024) k_emap_far<1024><<<grid, EF_THREADS, smem, s>>>(a);
@@ -292,6 +296,25 @@ __global__ void __launch_bounds__(256) k_emap_reduce(const ReduceInst *__restric
         for (int c = 0; c < r.n_chunks; c++) e += r.partial[(size_t)c * (size_t)r.P + (size_t)lin];
         r.out[lin] = e + r.out[lin];
     }
+}
+
+// Points [lin0, lin1) of one instance.
+__global__ void __launch_bounds__(256) k_emap_reduce_range(ReduceInst r, long long lin0, long long lin1)
+{
+    for (long long lin = lin0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; lin < lin1;
+         lin += (long long)gridDim.x * blockDim.x) {
+        float e = 0.f;
+        for (int c = 0; c < r.n_chunks; c++) e += r.partial[(size_t)c * (size_t)r.P + (size_t)lin];
+        r.out[lin] = e + r.out[lin];
+    }
+}
+
+cudaError_t launch_emap_reduce_range(const ReduceInst &r, long long lin0, long long lin1, cudaStream_t s)
+{
+    if (lin1 <= lin0) return cudaSuccess;
+    const unsigned nb = (unsigned)std::min<long long>((lin1 - lin0 + 255) / 256, 148LL * 16);
+    k_emap_reduce_range<<<nb, 256, 0, s>>>(r, lin0, lin1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_emap_reduce(const ReduceInst *insts, const long long *begin, int n, long long total,

@@ -37,7 +37,7 @@ struct NearInst {
 
 
 size_t far_smem_bytes(int tile);
-cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s);
+cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s, int fz0 = 0, int fz1 = -1);
 cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_begin, int n_inst,
                                   unsigned long long *counter, int tile, int ctas_per_sm, cudaStream_t s);
 // One instance of the e-map reduction: out[lin] = sum_c partial[c][lin] + out[lin].
@@ -49,13 +49,14 @@ struct ReduceInst {
 };
 cudaError_t launch_emap_reduce(const ReduceInst *insts, const long long *begin, int n, long long total,
                                cudaStream_t s);
+cudaError_t launch_emap_reduce_range(const ReduceInst &r, long long lin0, long long lin1, cudaStream_t s);
 cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s);
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s);
 cudaError_t launch_distance_maps(const DevProblem &p, double cutoff, float *fmap32, float *cmap32, double *fmap64,
                                  double *cmap64, cudaStream_t s);
 int near_bricks(const DevProblem &p, int shape);
 cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int shape,
-                        cudaStream_t s);
+                        cudaStream_t s, int bz0 = 0, int bz1 = -1);
 cudaError_t launch_near_batch(const NearInst *insts, const long long *unit_begin, int n_inst,
                               unsigned long long *counter, int shape, int ctas_per_sm, cudaStream_t s);
 int frames_x(int n1x);

@@ -607,10 +607,11 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
 
 // Single instance: one CTA per brick.
 template <bool EXACT, int BX, int BY, int BZ>
-__global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS) k_near(DevProblem p, NearGroup g, NearPtrs ptr)
+__global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS) k_near(DevProblem p, NearGroup g, NearPtrs ptr,
+                                                                  int brick0)
 {
     __shared__ NearSmem S;
-    near_unit<EXACT, BX, BY, BZ>(p, g, ptr, blockIdx.x, S);
+    near_unit<EXACT, BX, BY, BZ>(p, g, ptr, brick0 + blockIdx.x, S);
 }
 
 // Many instances, persistent: (instance-group, brick) units from an atomic
@@ -680,18 +681,26 @@ cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s)
     return cudaGetLastError();
 }
 
+// Brick z-rows [bz0, bz1) (bz1 < 0: through the last).
 cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int shape,
-                        cudaStream_t s)
+                        cudaStream_t s, int bz0, int bz1)
 {
-    const unsigned nb = (unsigned)near_bricks(p, shape);
+    int bx = 8, by = 8, bz = 4;
+    if (!exact && shape == 1) { by = 4; bz = 8; }
+    else if (!exact && shape == 2) { bx = 4; bz = 8; }
+    const int nbx = (p.n1x + bx - 1) / bx, nby = (p.n1y + by - 1) / by, nbz = (p.n1z + bz - 1) / bz;
+    if (bz1 < 0 || bz1 > nbz) bz1 = nbz;
+    if (bz0 >= bz1) return cudaSuccess;
+    const unsigned nb = (unsigned)(nbx * nby * (bz1 - bz0));
+    const int b0 = bz0 * nbx * nby;
     if (exact) {
-        k_near<true, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+        k_near<true, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     } else if (shape == 1) {
-        k_near<false, 8, 4, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+        k_near<false, 8, 4, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     } else if (shape == 2) {
-        k_near<false, 4, 8, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+        k_near<false, 4, 8, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     } else {
-        k_near<false, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr);
+        k_near<false, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     }
     return cudaGetLastError();
 }
