@@ -112,7 +112,7 @@ ag_status invalid(const std::string &m)
 
 // One-shot calls: z-slab height of the copy/compute pipeline (whole far-field
 // frames and near-field brick rows) and the most slabs one call uses.
-constexpr int kSlabZ = 32;
+constexpr int kSlabZ = 16;
 constexpr int kMaxSlabs = 16;
 
 }  // namespace
@@ -548,6 +548,51 @@ NearPtrs near_ptrs(const ag_plan *pl, unsigned long long *counters)
     return q;
 }
 
+// FP32 run as z-slabs of kSlabZ planes (whole far-field frames and
+// near-field brick rows), submitted slab by slab: far slab k on the side
+// stream; near slab k on s, then (after far slab k) the e-map reduction of
+// slab k, then event red_done[k].  The far and near kernels of neighbouring
+// slabs overlap, and a caller can copy slab k as soon as red_done[k] fires.
+ag_status enqueue_slabs(ag_plan *pl, cudaStream_t s, int nslab, int &launches)
+{
+    ag_context *c = pl->ctx;
+    const DevProblem &d = pl->dp;
+    const long long plane = (long long)d.n1x * d.n1y;
+    const bool far = d.elec_map >= 0 && pl->n_chunks > 0;
+    if (far) {
+        AGB_CK(cudaEventRecord(c->fork, s));
+        AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
+        AGB_CK(cudaEventRecord(c->evf0, c->side));
+    }
+    const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || d.elec_map >= 0;
+    for (int k = 0; k < nslab; k++) {
+        if (far) {
+            const int fz0 = k * (kSlabZ / FRAME_Z), fz1 = (k == nslab - 1) ? -1 : fz0 + kSlabZ / FRAME_Z;
+            AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, fz0, fz1));
+            AGB_CK(cudaEventRecord(c->far_done[k], c->side));
+            if (k == nslab - 1) AGB_CK(cudaEventRecord(c->evf1, c->side));
+            launches++;
+        }
+        const int bz0 = k * (kSlabZ / 4), bz1 = (k == nslab - 1) ? -1 : bz0 + kSlabZ / 4;  // 8x8x4 bricks
+        if (need_near)
+            for (const NearGroup &g : pl->groups) {
+                AGB_CK(launch_near(false, d, g, near_ptrs(pl, c->d_counters), 0, s, bz0, bz1));
+                launches++;
+            }
+        if (far) {
+            const long long z0 = (long long)k * kSlabZ, z1 = (k == nslab - 1) ? d.n1z : z0 + kSlabZ;
+            const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * d.P};
+            AGB_CK(cudaStreamWaitEvent(s, c->far_done[k], 0));
+            AGB_CK(launch_emap_reduce_range(r, z0 * plane, z1 * plane, s));
+            launches++;
+        }
+        AGB_CK(cudaEventRecord(c->red_done[k], s));
+    }
+    return AG_OK;
+}
+
+int slab_count(const DevProblem &d) { return std::min(kMaxSlabs, (d.n1z + kSlabZ - 1) / kSlabZ); }
+
 ag_status run_plan(ag_plan *pl, cudaStream_t s)
 {
     ag_context *c = pl->ctx;
@@ -560,6 +605,27 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
     if (d.elec_map >= 0 && exact) {
         AGB_CK(launch_emap_exact(d, pl->maps64 + (size_t)d.elec_map * d.P, s));
         launches++;
+    }
+    if (!exact && slab_count(d) > 1) {  // interleaved z-slabs (see enqueue_slabs)
+        if (pl->any_cov) {
+            AGB_CK(launch_covalent(d, pl->cov, s));
+            launches++;
+        }
+        if (pl->floating || pl->constriction) {
+            const size_t P = (size_t)d.P, f = (size_t)d.n_maps * P, cc = f + (size_t)pl->floating * P;
+            AGB_CK(launch_distance_maps(d, pl->constriction_cutoff, pl->floating ? pl->maps32 + f : nullptr,
+                                        pl->constriction ? pl->maps32 + cc : nullptr, nullptr, nullptr, s));
+            launches++;
+        }
+        ag_status st = enqueue_slabs(pl, s, slab_count(d), launches);
+        if (st != AG_OK) return st;
+        AGB_CK(cudaEventRecord(c->ev1, s));
+        pl->last_launches = launches;
+        c->pending = true;
+        c->had_far = far;
+        c->last_launches = launches;
+        c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
+        return AG_OK;
     }
     if (far) {  // far field on the side stream, concurrent with the near-field kernel
         AGB_CK(cudaEventRecord(c->fork, s));
@@ -896,20 +962,17 @@ ag_status ag_context_stats(const ag_context *ctx, ag_stats *out)
     return AG_OK;
 }
 
-// One-shot FP32 run with the maps copied to `out` slab by slab: every
-// far-field slab runs back to back on the side stream; the near-field kernel of
-// slab k runs on the main stream, then waits for far slab k and reduces the e
-// map of slab k; the copy stream brings slab k back while later slabs compute.
-// All kernels are enqueued before the copies, so a pageable destination (whose
-// copies block the host) does not delay the launches.
+// One-shot FP32 run with the maps copied to `out` slab by slab on the copy
+// stream while later slabs compute.  All kernels are enqueued before the
+// copies, so a pageable destination (whose copies block the host) does not
+// delay the launches.
 static ag_status run_plan_pipelined(ag_plan *pl, void *out, size_t n_out)
 {
     ag_context *c = pl->ctx;
     const DevProblem &d = pl->dp;
     cudaStream_t s = c->stream;
-    const int nslab = std::min(kMaxSlabs, (d.n1z + kSlabZ - 1) / kSlabZ);
+    const int nslab = slab_count(d);
     const long long plane = (long long)d.n1x * d.n1y;
-    const bool far = d.elec_map >= 0 && pl->n_chunks > 0;
     int launches = 0;
     AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
     AGB_CK(cudaEventRecord(c->ev0, s));
@@ -923,43 +986,17 @@ static ag_status run_plan_pipelined(ag_plan *pl, void *out, size_t n_out)
                                     pl->constriction ? pl->maps32 + cc : nullptr, nullptr, nullptr, s));
         launches++;
     }
-    if (far) {
-        AGB_CK(cudaEventRecord(c->fork, s));
-        AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
-        AGB_CK(cudaEventRecord(c->evf0, c->side));
-        for (int k = 0; k < nslab; k++) {
-            const int fz0 = k * (kSlabZ / FRAME_Z), fz1 = (k == nslab - 1) ? -1 : fz0 + kSlabZ / FRAME_Z;
-            AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, fz0, fz1));
-            AGB_CK(cudaEventRecord(c->far_done[k], c->side));
-            launches++;
-        }
-        AGB_CK(cudaEventRecord(c->evf1, c->side));
-    }
-    const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || d.elec_map >= 0;
-    for (int k = 0; k < nslab; k++) {
-        const int bz0 = k * (kSlabZ / 4), bz1 = (k == nslab - 1) ? -1 : bz0 + kSlabZ / 4;  // 8x8x4 bricks
-        if (need_near)
-            for (const NearGroup &g : pl->groups) {
-                AGB_CK(launch_near(false, d, g, near_ptrs(pl, c->d_counters), 0, s, bz0, bz1));
-                launches++;
-            }
-        if (far) {
-            const long long z0 = (long long)k * kSlabZ, z1 = std::min<long long>(d.n1z, z0 + kSlabZ);
-            const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * d.P};
-            AGB_CK(cudaStreamWaitEvent(s, c->far_done[k], 0));
-            AGB_CK(launch_emap_reduce_range(r, z0 * plane, z1 * plane, s));
-            launches++;
-        }
-        AGB_CK(cudaEventRecord(c->red_done[k], s));
-    }
+    ag_status st = enqueue_slabs(pl, s, nslab, launches);
+    if (st != AG_OK) return st;
     AGB_CK(cudaEventRecord(c->ev1, s));
+    const bool far = d.elec_map >= 0 && pl->n_chunks > 0;
     pl->last_launches = launches;
     c->pending = true;
     c->had_far = far;
     c->last_launches = launches;
     c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
     for (int k = 0; k < nslab; k++) {
-        const long long z0 = (long long)k * kSlabZ, z1 = std::min<long long>(d.n1z, z0 + kSlabZ);
+        const long long z0 = (long long)k * kSlabZ, z1 = (k == nslab - 1) ? d.n1z : z0 + kSlabZ;
         const size_t off = (size_t)(z0 * plane) * sizeof(float), width = (size_t)((z1 - z0) * plane) * sizeof(float);
         AGB_CK(cudaStreamWaitEvent(c->copy, c->red_done[k], 0));
         AGB_CK(cudaMemcpy2DAsync((char *)out + off, (size_t)d.P * sizeof(float), (const char *)pl->maps32 + off,
