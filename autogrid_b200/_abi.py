@@ -60,7 +60,7 @@ class ag_problem(C.Structure):
 
 class ag_opts(C.Structure):
     _fields_ = [("precision", C.c_int32), ("table_mode", C.c_int32), ("autotune", C.c_int32),
-                ("reserved", C.c_int32 * 5)]
+                ("serial", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class ag_stats(C.Structure):

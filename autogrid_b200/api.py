@@ -247,8 +247,10 @@ class Context:
         check(self._lib.ag_context_stats(self._h, C.byref(st)))
         return Stats(st.near_pairs, st.fp64_fallbacks, st.far_pairs, st.gpu_launches, st.kernel_ms, st.far_ms)
 
-    def plan(self, problem: Problem) -> "Plan":
-        return Plan(self, problem)
+    def plan(self, problem: Problem, serial: bool = False) -> "Plan":
+        """Device-resident plan; serial=True runs every kernel in sequence on one
+        stream (same work, for timing kernels alone)."""
+        return Plan(self, problem, serial)
 
     def close(self) -> None:
         if self._h:
@@ -358,12 +360,12 @@ class Diff:
 class Plan:
     """Device-resident problem: upload once, run many times (ag_plan)."""
 
-    def __init__(self, ctx: Context, problem: Problem):
+    def __init__(self, ctx: Context, problem: Problem, serial: bool = False):
         self.ctx = ctx
         self.problem = problem
         self._lib = ctx._lib
         h = C.c_void_p()
-        opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST)
+        opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST, serial=int(bool(serial)))
         s = problem.struct()
         check(self._lib.ag_plan_create(ctx._h, C.byref(s), C.byref(opts), C.byref(h)))
         self._h = h

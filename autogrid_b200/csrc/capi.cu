@@ -242,7 +242,7 @@ cudaError_t upload(BufferSet *b, const char *name, const T *src, size_t n, T **d
 }
 
 // Build the device image of a problem (host work is O(atoms + tables)).
-ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
+ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipelined)
 {
     ag_status st = validate(p);
     if (st != AG_OK) return st;
@@ -414,11 +414,13 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s)
         solf[k] = (float)p->sol_fn[k];
     }
 
-    // far-field chunking: enough CTAs for ~8 waves
-    const long long frames = (long long)frames_x(d.n1x) * frames_y(d.n1y) * frames_z(d.n1z);
+    // far-field chunking: enough CTAs for ~8 waves per launch; a slab-pipelined
+    // one-shot run launches one slab of frames at a time, ~3 waves each
+    const long long frames = pipelined ? (long long)frames_x(d.n1x) * frames_y(d.n1y) * (kSlabZ / FRAME_Z)
+                                       : (long long)frames_x(d.n1x) * frames_y(d.n1y) * frames_z(d.n1z);
     const int tile = 512;
     if (p->elec_map >= 0 && N > 0) {
-        const long long target = 148LL * 3 * 8;
+        const long long target = pipelined ? 148LL * 3 * 3 : 148LL * 3 * 8;
         int nch = (int)std::max(1LL, (target + frames - 1) / frames);
         nch = std::min(nch, (N + tile - 1) / tile);
         pl->chunk_atoms = ((N + nch - 1) / nch + tile - 1) / tile * tile;
@@ -606,34 +608,19 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
         AGB_CK(launch_emap_exact(d, pl->maps64 + (size_t)d.elec_map * d.P, s));
         launches++;
     }
-    if (!exact && slab_count(d) > 1) {  // interleaved z-slabs (see enqueue_slabs)
-        if (pl->any_cov) {
-            AGB_CK(launch_covalent(d, pl->cov, s));
-            launches++;
+    // far field on the side stream, concurrent with the near-field kernel (or,
+    // with opts.serial, before it on s)
+    const bool serial = pl->opts.serial != 0;
+    cudaStream_t fs = serial ? s : c->side;
+    if (far) {
+        if (!serial) {
+            AGB_CK(cudaEventRecord(c->fork, s));
+            AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
         }
-        if (pl->floating || pl->constriction) {
-            const size_t P = (size_t)d.P, f = (size_t)d.n_maps * P, cc = f + (size_t)pl->floating * P;
-            AGB_CK(launch_distance_maps(d, pl->constriction_cutoff, pl->floating ? pl->maps32 + f : nullptr,
-                                        pl->constriction ? pl->maps32 + cc : nullptr, nullptr, nullptr, s));
-            launches++;
-        }
-        ag_status st = enqueue_slabs(pl, s, slab_count(d), launches);
-        if (st != AG_OK) return st;
-        AGB_CK(cudaEventRecord(c->ev1, s));
-        pl->last_launches = launches;
-        c->pending = true;
-        c->had_far = far;
-        c->last_launches = launches;
-        c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
-        return AG_OK;
-    }
-    if (far) {  // far field on the side stream, concurrent with the near-field kernel
-        AGB_CK(cudaEventRecord(c->fork, s));
-        AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
-        AGB_CK(cudaEventRecord(c->evf0, c->side));
-        AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side));
-        AGB_CK(cudaEventRecord(c->evf1, c->side));
-        AGB_CK(cudaEventRecord(c->join, c->side));
+        AGB_CK(cudaEventRecord(c->evf0, fs));
+        AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, fs));
+        AGB_CK(cudaEventRecord(c->evf1, fs));
+        if (!serial) AGB_CK(cudaEventRecord(c->join, fs));
         launches++;
     }
     if (pl->any_cov) {
@@ -659,7 +646,7 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
         }
     }
     if (far) {
-        AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
+        if (!serial) AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
         AGB_CK(launch_emap_reduce(pl->d_reduce, pl->d_reduce_begin, 1, d.P, s));
         launches++;
     }
@@ -694,7 +681,7 @@ ag_status settle_stats(ag_context *c)
 ag_status finish_stats(ag_plan *pl) { return settle_stats(pl->ctx); }
 
 ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out,
-                    Arena *arena = nullptr);
+                    Arena *arena = nullptr, bool pipelined = false);
 
 }  // namespace
 
@@ -863,7 +850,8 @@ ag_status batch_autotune(ag_batch *b)
     return AG_OK;
 }
 
-ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out, Arena *arena)
+ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out, Arena *arena,
+                    bool pipelined)
 {
     if (!ctx || !p || !out) return invalid("null argument");
     ag_opts opts{};
@@ -884,7 +872,7 @@ ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool
     } else {
         pl->bufs = &ctx->pool;
     }
-    ag_status st = build_plan(pl.get(), p, ctx->stream);
+    ag_status st = build_plan(pl.get(), p, ctx->stream, pipelined);
     if (st != AG_OK) return st;
     *out = pl.release();
     return AG_OK;
@@ -1011,11 +999,12 @@ static ag_status compute_common(ag_context *ctx, const ag_problem *problem, cons
 {
     if (!maps) return invalid("null maps");
     ag_plan *pl = nullptr;
-    ag_status st = make_plan(ctx, problem, opts, false, &pl);
+    const bool pipelined = elem == 4 && problem && problem->n1[2] > kSlabZ && !(opts && opts->serial);
+    ag_status st = make_plan(ctx, problem, opts, false, &pl, nullptr, pipelined);
     if (st != AG_OK) return st;
     std::unique_ptr<ag_plan> guard(pl);
     const size_t n_out = (size_t)problem->n_maps + pl->floating + pl->constriction;
-    if (elem == 4 && pl->dp.n1z > kSlabZ) {
+    if (pipelined) {
         st = run_plan_pipelined(pl, maps, n_out);
         if (st != AG_OK) return st;
         AGB_CK(cudaStreamSynchronize(ctx->stream));

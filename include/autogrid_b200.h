@@ -133,7 +133,10 @@ typedef struct ag_opts {
     int32_t table_mode;  /* AG_TABLE_*                                         */
     int32_t autotune;    /* batches: 1 = time tile/brick shapes at creation,   */
                          /* 0 = use the defaults                               */
-    int32_t reserved[5]; /* zero                                               */
+    int32_t serial;      /* plans / one-shot calls: 1 = every kernel in       */
+                         /* sequence on one stream (same work; for timing     */
+                         /* kernels alone), 0 = far and near fields overlap   */
+    int32_t reserved[4]; /* zero                                               */
 } ag_opts;
 
 /* Diagnostics of the last compute or plan run on a context (FP32 path);
