@@ -610,8 +610,14 @@ template <bool EXACT, int BX, int BY, int BZ>
 __global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS) k_near(DevProblem p, NearGroup g, NearPtrs ptr,
                                                                   int brick0)
 {
+    // The problem is read through a shared-memory copy: the FP64 fallbacks
+    // take it by reference, and a reference to the kernel parameter would make
+    // every thread copy it into local memory.
     __shared__ NearSmem S;
-    near_unit<EXACT, BX, BY, BZ>(p, g, ptr, brick0 + blockIdx.x, S);
+    __shared__ DevProblem s_p;
+    if (threadIdx.x == 0) s_p = p;
+    __syncthreads();
+    near_unit<EXACT, BX, BY, BZ>(s_p, g, ptr, brick0 + blockIdx.x, S);
 }
 
 // Many instances, persistent: (instance-group, brick) units from an atomic
