@@ -10,6 +10,6 @@ Public API:
     torch_maps.GridMaps(job)     torch.autograd binding of the differentiable mode
 """
 from ._abi import AutoGridError, load_library  # noqa: F401
-from .api import Batch, Context, Diff, Job, Plan, Problem, Stats, run_gpf  # noqa: F401
+from .api import Batch, Context, Diff, Job, MapText, Plan, Problem, Stats, run_gpf  # noqa: F401
 
-__all__ = ["AutoGridError", "Batch", "Context", "Diff", "Job", "Plan", "Problem", "Stats", "load_library", "run_gpf"]
+__all__ = ["AutoGridError", "Batch", "Context", "Diff", "Job", "MapText", "Plan", "Problem", "Stats", "load_library", "run_gpf"]

@@ -90,6 +90,10 @@ SIGNATURES = {
     "ag_plan_points": (C.c_size_t, [C.c_void_p]),
     "ag_plan_download": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ag_plan_destroy": (C.c_int, [C.c_void_p]),
+    "ag_maps_format": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.c_void_p, C.c_int32,
+                                 C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_maps_compute_text": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts),
+                                       C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_batch_create": (C.c_int, [C.c_void_p, C.POINTER(C.POINTER(ag_problem)), C.c_int32, C.POINTER(ag_opts),
                                   C.POINTER(C.c_void_p)]),
     "ag_batch_run": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -103,6 +107,7 @@ SIGNATURES = {
     "ag_job_problem": (C.POINTER(ag_problem), [C.c_void_p]),
     "ag_job_write_maps_f32": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ag_job_write_maps_f64": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_job_write_text": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_job_fail": (None, [C.c_void_p, C.c_char_p]),
     "ag_job_free": (None, [C.c_void_p]),
     "ag_job_vina_problem": (C.c_int32, [C.c_void_p, C.POINTER(C.POINTER(ag_problem))]),

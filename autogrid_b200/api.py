@@ -165,6 +165,15 @@ class Job:
             m = np.ascontiguousarray(m, dtype=np.float32)
             check(self._lib.ag_job_write_maps_f32(self._h, m.ctypes.data_as(C.c_void_p)))
 
+    def write_text(self, mt: "MapText") -> None:
+        """Write the map files and GLG summary from device-formatted bodies
+        (ag_job_write_text)."""
+        b = np.ascontiguousarray(mt.map_bytes, dtype=np.uint64)
+        lo = np.ascontiguousarray(mt.emin, dtype=np.float64)
+        hi = np.ascontiguousarray(mt.emax, dtype=np.float64)
+        check(self._lib.ag_job_write_text(self._h, C.c_void_p(mt.ptr), b.ctypes.data_as(C.c_void_p),
+                                          lo.ctypes.data_as(C.c_void_p), hi.ctypes.data_as(C.c_void_p)))
+
     def vina_problem(self) -> Problem:
         """The job with Vina-potential tables (ag_job_vina_problem): atom maps
         only, plain sums, no desolvation."""
@@ -210,6 +219,37 @@ class Job:
 
 
 @dataclass
+class MapText:
+    """Map-file bodies formatted on the device (ag_maps_format).  `ptr` is the
+    context's pinned host buffer: valid until the context's next text call."""
+    ptr: int
+    map_bytes: np.ndarray  # uint64, one entry per output map
+    emin: np.ndarray       # extrema of each energy map
+    emax: np.ndarray
+
+    @property
+    def total(self) -> int:
+        return int(self.map_bytes.sum())
+
+    def body(self, k: int) -> bytes:
+        off = int(self.map_bytes[:k].sum())
+        return C.string_at(self.ptr + off, int(self.map_bytes[k]))
+
+    def tobytes(self) -> bytes:
+        return C.string_at(self.ptr, self.total)
+
+
+def _text_call(fn, problem: Problem, *head) -> MapText:
+    s = problem.struct()
+    ptr = C.c_void_p()
+    nb = np.zeros(problem.n_out, dtype=np.uint64)
+    lo = np.zeros(max(1, problem.n_maps)); hi = np.zeros(max(1, problem.n_maps))
+    check(fn(head[0], C.byref(s), *head[1:], C.byref(ptr), nb.ctypes.data_as(C.c_void_p),
+             lo.ctypes.data_as(C.c_void_p), hi.ctypes.data_as(C.c_void_p)))
+    return MapText(int(ptr.value or 0), nb, lo[:problem.n_maps], hi[:problem.n_maps])
+
+
+@dataclass
 class Stats:
     near_pairs: int
     fp64_fallbacks: int
@@ -241,6 +281,17 @@ class Context:
         fn = self._lib.ag_maps_compute_f64 if prec == _abi.AG_PREC_FP64 else self._lib.ag_maps_compute
         check(fn(self._h, C.byref(s), C.byref(opts), out.ctypes.data_as(C.c_void_p)))
         return out
+
+    def compute_text(self, problem: Problem, precision: str = "fp32") -> MapText:
+        """Compute the maps and format their map-file bodies on the device
+        (ag_maps_compute_text)."""
+        opts = ag_opts(precision=_PREC[precision], table_mode=_abi.AG_TABLE_NEAREST)
+        return _text_call(self._lib.ag_maps_compute_text, problem, self._h, C.byref(opts))
+
+    def format(self, problem: Problem, device_ptr: int, elem_size: int = 4) -> MapText:
+        """Format device-resident maps of `problem`'s layout (ag_maps_format)."""
+        return _text_call(self._lib.ag_maps_format, problem, self._h, C.c_void_p(int(device_ptr)),
+                          C.c_int32(int(elem_size)))
 
     def stats(self) -> Stats:
         st = ag_stats()
@@ -375,6 +426,10 @@ class Plan:
 
     def device_maps_ptr(self) -> int:
         return int(self._lib.ag_plan_device_maps(self._h) or 0)
+
+    def format(self) -> MapText:
+        """Map-file bodies of the plan's device maps (ag_maps_format)."""
+        return self.ctx.format(self.problem, self.device_maps_ptr(), 4)
 
     def download(self, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:

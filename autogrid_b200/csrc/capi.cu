@@ -16,6 +16,7 @@
 
 #include "autogrid_b200.h"
 #include "kernels/kernels.h"
+#include "kernels/maptext.h"
 
 namespace agb {
 void set_last_error(const std::string &m);
@@ -133,6 +134,10 @@ struct ag_context {
     ag_stats stats{};
     BufferSet pool;
     unsigned long long *d_counters = nullptr;
+    // map text (ag_maps_format): device scratch and text, pinned host copy
+    BufferSet text_bufs;
+    char *h_text = nullptr;
+    size_t h_text_cap = 0;
     // the last run, whose statistics ag_context_stats() settles
     bool pending = false, had_far = false;
     int last_launches = 0;
@@ -937,6 +942,7 @@ ag_status ag_context_destroy(ag_context *ctx)
     if (ctx->evf0) cudaEventDestroy(ctx->evf0);
     if (ctx->evf1) cudaEventDestroy(ctx->evf1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->h_text) cudaFreeHost(ctx->h_text);
     delete ctx;
     return AG_OK;
 }
@@ -1062,6 +1068,94 @@ ag_status ag_plan_download(ag_plan *plan, float *host_maps)
                            cudaMemcpyDefault, c->stream));
     AGB_CK(cudaStreamSynchronize(c->stream));
     return finish_stats(plan);
+}
+
+// Map-file text of device-resident maps (kernels/maptext.cu): measure pass,
+// one small read-back of the byte counts, write pass, one copy of the text.
+static ag_status format_maps(ag_context *c, const ag_problem *p, const void *dmaps, int elem, const char **text,
+                             size_t *map_bytes, double *emin, double *emax)
+{
+    if (!c || !p || !dmaps || !text || !map_bytes) return invalid("null argument");
+    if (elem != 4 && elem != 8) return invalid("elem_size must be 4 (FP32 maps) or 8 (FP64 maps)");
+    ag_status st = validate(p);
+    if (st != AG_OK) return st;
+    AGB_CK(cudaSetDevice(c->device));
+    cudaStream_t s = c->stream;
+    const long long P = (long long)p->n1[0] * p->n1[1] * p->n1[2];
+    const int n_out = p->n_maps + (p->floating_grid ? 1 : 0) + (p->constriction_grid ? 1 : 0);
+    TextArgs a{};
+    a.m32 = elem == 4 ? (const float *)dmaps : nullptr;
+    a.m64 = elem == 8 ? (const double *)dmaps : nullptr;
+    a.P = P;
+    a.n_out = n_out;
+    a.n_energy = p->n_maps;
+    a.floating = p->floating_grid ? 1 : 0;
+    a.bpm = text_blocks_per_map(P);
+    const long long nb = (long long)n_out * a.bpm;
+    if (nb > 0x7fffffffll) {
+        set_last_error("ag_maps_format: too many grid points for one call");
+        return AG_ERR_TOO_LARGE;
+    }
+    BufferSet &B = c->text_bufs;
+    void *v;
+    AGB_CK(B.ensure("len8", (size_t)nb * (size_t)text_values_per_block(), &v));
+    a.len8 = (unsigned char *)v;
+    AGB_CK(B.ensure("blk_len", (size_t)nb * sizeof(unsigned), &v));
+    a.blk_len = (unsigned *)v;
+    AGB_CK(B.ensure("blk_off", (size_t)nb * sizeof(unsigned long long), &v));
+    a.blk_off = (unsigned long long *)v;
+    AGB_CK(B.ensure("ext", (size_t)std::max(1, 2 * p->n_maps) * sizeof(unsigned long long), &v));
+    a.ext = (unsigned long long *)v;
+    AGB_CK(B.ensure("map_bytes", (size_t)(n_out + 1) * sizeof(unsigned long long), &v));
+    a.map_bytes = (unsigned long long *)v;
+    AGB_CK(launch_text_measure(a, s));
+    std::vector<unsigned long long> hb((size_t)n_out + 1), he((size_t)std::max(1, 2 * p->n_maps));
+    AGB_CK(cudaMemcpyAsync(hb.data(), a.map_bytes, hb.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    AGB_CK(cudaMemcpyAsync(he.data(), a.ext, he.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    AGB_CK(cudaStreamSynchronize(s));
+    const size_t total = (size_t)hb[(size_t)n_out];
+    AGB_CK(B.ensure("text", total, &v));
+    a.text = (char *)v;
+    AGB_CK(launch_text_write(a, s));
+    if (c->h_text_cap < total || !c->h_text) {
+        if (c->h_text) cudaFreeHost(c->h_text);
+        c->h_text = nullptr;
+        c->h_text_cap = 0;
+        AGB_CK(cudaHostAlloc((void **)&c->h_text, std::max<size_t>(total, 16), cudaHostAllocDefault));
+        c->h_text_cap = std::max<size_t>(total, 16);
+    }
+    AGB_CK(cudaMemcpyAsync(c->h_text, a.text, total, cudaMemcpyDeviceToHost, s));
+    AGB_CK(cudaStreamSynchronize(s));
+    *text = c->h_text;
+    for (int k = 0; k < n_out; k++) map_bytes[k] = (size_t)hb[(size_t)k];
+    for (int k = 0; k < p->n_maps; k++) {
+        if (emin) emin[k] = text_key_to_double(he[2 * (size_t)k]);
+        if (emax) emax[k] = text_key_to_double(he[2 * (size_t)k + 1]);
+    }
+    return AG_OK;
+}
+
+ag_status ag_maps_format(ag_context *ctx, const ag_problem *problem, const void *device_maps, int32_t elem_size,
+                         const char **text, size_t *map_bytes, double *emin, double *emax)
+{
+    return format_maps(ctx, problem, device_maps, elem_size, text, map_bytes, emin, emax);
+}
+
+ag_status ag_maps_compute_text(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, const char **text,
+                               size_t *map_bytes, double *emin, double *emax)
+{
+    if (!text || !map_bytes) return invalid("null argument");
+    ag_plan *pl = nullptr;
+    ag_status st = make_plan(ctx, problem, opts, false, &pl, nullptr, false);
+    if (st != AG_OK) return st;
+    std::unique_ptr<ag_plan> guard(pl);
+    st = run_plan(pl, ctx->stream);
+    if (st != AG_OK) return st;
+    const bool f64 = pl->opts.precision == AG_PREC_FP64;
+    st = format_maps(ctx, problem, f64 ? (const void *)pl->maps64 : (const void *)pl->maps32, f64 ? 8 : 4, text,
+                     map_bytes, emin, emax);
+    if (st != AG_OK) return st;
+    return finish_stats(pl);
 }
 
 ag_status ag_plan_destroy(ag_plan *plan)

@@ -12,13 +12,14 @@
 static const char *kHelp =
     "\t-p parameter_filename\n\t\t\t-l log_filename\n\t\t\t-d (increment debug level)\n"
     "\t\t\t-h (display this message)\n\t\t\t--version (print version information)\n"
-    "\t\t\t--fp64 (FP64 twin instead of the FP32 production path)\n\t\t\t--device N\n";
+    "\t\t\t--fp64 (FP64 twin instead of the FP32 production path)\n\t\t\t--device N\n"
+    "\t\t\t--host-writer (format the map files on the host instead of the GPU)\n";
 
 int main(int argc, char **argv)
 {
     std::string gpf, glg;
     int device = 0;
-    bool fp64 = false;
+    bool fp64 = false, host_writer = false;
     for (int i = 1; i < argc; i++) {
         std::string a = argv[i];
         if (a == "-p" && i + 1 < argc) gpf = argv[++i];
@@ -30,6 +31,7 @@ int main(int argc, char **argv)
             return 0;
         }
         else if (a == "--fp64") fp64 = true;
+        else if (a == "--host-writer") host_writer = true;
         else if (a == "--device" && i + 1 < argc) device = std::atoi(argv[++i]);
         else { std::fprintf(stderr, "%s: unknown switch %s\n", argv[0], a.c_str()); return 1; }
     }
@@ -51,7 +53,14 @@ int main(int argc, char **argv)
     if (st == AG_OK) {
         ag_opts o{};
         o.precision = fp64 ? AG_PREC_FP64 : AG_PREC_FP32;
-        if (fp64) {
+        if (!host_writer) {
+            // maps stay on the device; their text is formatted there
+            const char *text = nullptr;
+            std::vector<size_t> bytes(n_out);
+            std::vector<double> emin((size_t)p->n_maps + 1), emax((size_t)p->n_maps + 1);
+            st = ag_maps_compute_text(ctx, p, &o, &text, bytes.data(), emin.data(), emax.data());
+            if (st == AG_OK) st = ag_job_write_text(job, text, bytes.data(), emin.data(), emax.data());
+        } else if (fp64) {
             std::vector<double> maps(n_out * P);
             st = ag_maps_compute_f64(ctx, p, &o, maps.data());
             if (st == AG_OK) st = ag_job_write_maps_f64(job, maps.data());

@@ -14,6 +14,7 @@
 #include <ctime>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 #include <strings.h>
 
@@ -298,6 +299,7 @@ struct Job {
     void make_problem();
     void build_vina_problem();
     void write_maps(const double *maps64, const float *maps32);
+    void write_text(const char *text, const size_t *bytes, const double *emin, const double *emax);
 };
 
 // ---------------------------------------------------------------- receptor --
@@ -1252,62 +1254,75 @@ void Job::make_problem()
 }
 
 // ------------------------------------------------------------- map writer --
-// main.cpp:3481-3565
+// main.cpp:3481-3565.  write_maps formats on the host; write_text takes bodies
+// formatted on the device by ag_maps_format (same bytes).
 void Job::write_maps(const double *m64, const float *m32)
 {
     const size_t P = (size_t)num_grid_points_per_map;
-    std::vector<char> buf;
-    buf.reserve(P * 10 + 64);
-    bool problem = false;
-    for (int j = 0; j < num_maps; j++) {
-        buf.clear();
-        MapObj &g = gridmap[j];
+    const size_t n_out = (size_t)num_maps + (floating_grid ? 1 : 0) + (constriction_grid ? 1 : 0);
+    auto val = [&](size_t k, size_t a) { return m64 ? m64[k * P + a] : (double)m32[k * P + a]; };
+    std::vector<char> text;
+    text.reserve(P * n_out * 8 + 64);
+    std::vector<size_t> bytes(n_out, 0);
+    std::vector<double> emin((size_t)num_maps, kBig), emax((size_t)num_maps, -kBig);
+    char tmp[64];
+    for (size_t k = 0; k < n_out; k++) {
+        const size_t before = text.size();
+        const bool energy = k < (size_t)num_maps, count = !energy && !(floating_grid && k == (size_t)num_maps);
         for (size_t a = 0; a < P; a++) {
-            const double e = m64 ? m64[(size_t)j * P + a] : (double)m32[(size_t)j * P + a];
-            char tmp[64];
+            const double e = val(k, a);
             int n;
-            if (std::fabs(e) < kPrecision) {
+            if (count) {
+                n = std::snprintf(tmp, sizeof tmp, "%d\n", (int)e);
+            } else if (energy && std::fabs(e) < kPrecision) {
                 tmp[0] = '0'; tmp[1] = '\n'; n = 2;
             } else {
                 const float v = (float)(std::round((long double)e * 1000.0L) / 1000.0L);  // round3dp, main.cpp:86
                 n = std::snprintf(tmp, sizeof tmp, "%.3f\n", (double)v);
             }
-            buf.insert(buf.end(), tmp, tmp + n);
-            g.emax = std::max(g.emax, e);
-            g.emin = std::min(g.emin, e);
+            text.insert(text.end(), tmp, tmp + n);
+            if (energy) {
+                emax[k] = std::max(emax[k], e);
+                emin[k] = std::min(emin[k], e);
+            }
         }
-        if (std::fwrite(buf.data(), 1, buf.size(), g.fp) != buf.size()) problem = true;
-        std::fclose(g.fp);
-        g.fp = nullptr;
+        bytes[k] = text.size() - before;
     }
-    // distance maps follow the energy maps (main.cpp:3498-3514): fmap as %.3f of
-    // round3dp, cmap as an integer count
-    size_t k = (size_t)num_maps;
-    auto dist = [&](size_t a) { return m64 ? m64[k * P + a] : (double)m32[k * P + a]; };
-    if (floating_grid && floating_fp) {
-        buf.clear();
-        for (size_t a = 0; a < P; a++) {
-            char tmp[64];
-            const float v = (float)(std::round((long double)dist(a) * 1000.0L) / 1000.0L);
-            const int n = std::snprintf(tmp, sizeof tmp, "%.3f\n", (double)v);
-            buf.insert(buf.end(), tmp, tmp + n);
-        }
-        if (std::fwrite(buf.data(), 1, buf.size(), floating_fp) != buf.size()) problem = true;
-        std::fclose(floating_fp);
-        floating_fp = nullptr;
-        k++;
+    write_text(text.data(), bytes.data(), emin.data(), emax.data());
+}
+
+void Job::write_text(const char *text, const size_t *bytes, const double *emin, const double *emax)
+{
+    const size_t n_out = (size_t)num_maps + (floating_grid ? 1 : 0) + (constriction_grid ? 1 : 0);
+    std::vector<std::FILE *> fps;
+    for (int j = 0; j < num_maps; j++) fps.push_back(gridmap[j].fp);
+    if (floating_grid) fps.push_back(floating_fp);
+    if (constriction_grid) fps.push_back(constriction_fp);
+    std::vector<size_t> off(n_out + 1, 0);
+    for (size_t k = 0; k < n_out; k++) off[k + 1] = off[k] + bytes[k];
+    // one file per thread, as the reference's loop over maps is an OpenMP
+    // parallel for (main.cpp:3484)
+    std::vector<char> failed(n_out, 0);
+    const size_t nt = std::min<size_t>(n_out, 16);
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; t++)
+        pool.emplace_back([&, t] {
+            for (size_t k = t; k < n_out; k += nt) {
+                if (!fps[k]) continue;
+                if (std::fwrite(text + off[k], 1, bytes[k], fps[k]) != bytes[k]) failed[k] = 1;
+                if (std::fclose(fps[k]) != 0) failed[k] = 1;
+            }
+        });
+    for (auto &th : pool) th.join();
+    for (int j = 0; j < num_maps; j++) {
+        gridmap[j].fp = nullptr;
+        if (emin) gridmap[j].emin = std::min(gridmap[j].emin, emin[j]);
+        if (emax) gridmap[j].emax = std::max(gridmap[j].emax, emax[j]);
     }
-    if (constriction_grid && constriction_fp) {
-        buf.clear();
-        for (size_t a = 0; a < P; a++) {
-            char tmp[32];
-            const int n = std::snprintf(tmp, sizeof tmp, "%d\n", (int)dist(a));
-            buf.insert(buf.end(), tmp, tmp + n);
-        }
-        if (std::fwrite(buf.data(), 1, buf.size(), constriction_fp) != buf.size()) problem = true;
-        std::fclose(constriction_fp);
-        constriction_fp = nullptr;
-    }
+    if (floating_grid) floating_fp = nullptr;
+    if (constriction_grid) constriction_fp = nullptr;
+    bool problem = false;
+    for (char f : failed) problem = problem || f;
     if (problem) fatal("Problems writing grid maps - there may not be enough disk space.", AG_ERR_IO);
     log("\nGrid\tAtom\tMinimum   \tMaximum\nMap \tType\tEnergy    \tEnergy \n\t\t(kcal/mol)\t(kcal/mol)\n"
         "____\t____\t_____________\t_____________\n");
@@ -1391,6 +1406,20 @@ static ag_status write_common(ag_job *job, const double *m64, const float *m32)
 
 ag_status ag_job_write_maps_f32(ag_job *job, const float *maps) { return write_common(job, nullptr, maps); }
 ag_status ag_job_write_maps_f64(ag_job *job, const double *maps) { return write_common(job, maps, nullptr); }
+
+ag_status ag_job_write_text(ag_job *job, const char *text, const size_t *map_bytes, const double *emin,
+                            const double *emax)
+{
+    if (!job || !text || !map_bytes) { agb::set_last_error("ag_job_write_text: null argument"); return AG_ERR_INVALID; }
+    try {
+        job->job.write_text(text, map_bytes, emin, emax);
+    } catch (const Fatal &f) {
+        ag_job_fail(job, f.what());
+        agb::set_last_error(f.what());
+        return f.status;
+    }
+    return AG_OK;
+}
 
 void ag_job_fail(ag_job *job, const char *message)
 {

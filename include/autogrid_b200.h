@@ -196,6 +196,30 @@ ag_status    ag_plan_download(ag_plan *plan, float *host_maps);
 ag_status    ag_plan_destroy(ag_plan *plan);
 
 /*
+ * Map-file bodies formatted on the device (replaces the text loop of
+ * main.cpp:3481-3519), byte for byte what the reference's fprintf writes:
+ *   energy maps     "0\n" when fabs(e) < 1e-4 (PRECISION, autogrid.h:68),
+ *                   else "%.3f\n" of (float)round3dp(e) (main.cpp:84-86);
+ *   floating grid   "%.3f\n" of (float)round3dp(r_min);
+ *   constriction    "%d\n" of the atom count.
+ * `device_maps` holds the n_out = problem->n_maps (+1 floating, +1
+ * constriction) output maps of ag_maps_compute's layout in DEVICE memory,
+ * FP32 (elem_size 4) or FP64 (8); for example ag_plan_device_maps().  On
+ * return *text points to the bodies, map after map, in pinned host memory
+ * owned by the context (valid until its next text call or
+ * ag_context_destroy); map_bytes[k] (n_out entries) is the length of map k's
+ * body; emin/emax (n_maps entries each, may be NULL) receive each energy
+ * map's extrema over the unrounded values (main.cpp:3494-3495).
+ */
+ag_status ag_maps_format(ag_context *ctx, const ag_problem *problem, const void *device_maps,
+                         int32_t elem_size, const char **text, size_t *map_bytes, double *emin,
+                         double *emax);
+/* ag_maps_compute (FP32) or ag_maps_compute_f64 (opts->precision FP64) and
+ * ag_maps_format in one call, the maps never leaving the device. */
+ag_status ag_maps_compute_text(ag_context *ctx, const ag_problem *problem, const ag_opts *opts,
+                               const char **text, size_t *map_bytes, double *emin, double *emax);
+
+/*
  * Electrostatic map for callers that cannot allocate device memory.  No
  * counterpart in the reference (which has no library interface).  Meant for
  * processes whose device memory is owned by their own pool allocator, or
@@ -333,6 +357,11 @@ const ag_problem  *ag_job_problem(const ag_job *job);
  * completion line (main.cpp:3530-3565) from FP32 or FP64 maps. */
 ag_status          ag_job_write_maps_f32(ag_job *job, const float *maps);
 ag_status          ag_job_write_maps_f64(ag_job *job, const double *maps);
+/* Same files and GLG summary from bodies already formatted by
+ * ag_maps_format / ag_maps_compute_text (map_bytes: one entry per output map;
+ * emin/emax: one per energy map). */
+ag_status          ag_job_write_text(ag_job *job, const char *text, const size_t *map_bytes,
+                                     const double *emin, const double *emax);
 /* Record a fatal error in the job's GLG ("Unsuccessful Completion"). */
 void               ag_job_fail(ag_job *job, const char *message);
 void               ag_job_free(ag_job *job);
