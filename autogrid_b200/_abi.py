@@ -66,7 +66,7 @@ class ag_opts(C.Structure):
 class ag_stats(C.Structure):
     _fields_ = [("near_pairs", C.c_int64), ("fp64_fallbacks", C.c_int64), ("far_pairs", C.c_int64),
                 ("gpu_launches", C.c_int32), ("reserved", C.c_int32), ("kernel_ms", C.c_double),
-                ("far_ms", C.c_double)]
+                ("far_ms", C.c_double), ("text_ms", C.c_double), ("text_bytes", C.c_int64)]
 
 
 class ag_tuning(C.Structure):

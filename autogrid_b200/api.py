@@ -257,6 +257,8 @@ class Stats:
     gpu_launches: int
     kernel_ms: float
     far_ms: float
+    text_ms: float = 0.0
+    text_bytes: int = 0
 
 
 class Context:
@@ -296,7 +298,8 @@ class Context:
     def stats(self) -> Stats:
         st = ag_stats()
         check(self._lib.ag_context_stats(self._h, C.byref(st)))
-        return Stats(st.near_pairs, st.fp64_fallbacks, st.far_pairs, st.gpu_launches, st.kernel_ms, st.far_ms)
+        return Stats(st.near_pairs, st.fp64_fallbacks, st.far_pairs, st.gpu_launches, st.kernel_ms, st.far_ms,
+                     st.text_ms, st.text_bytes)
 
     def plan(self, problem: Problem, serial: bool = False) -> "Plan":
         """Device-resident plan; serial=True runs every kernel in sequence on one

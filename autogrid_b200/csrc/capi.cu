@@ -138,6 +138,7 @@ struct ag_context {
     BufferSet text_bufs;
     char *h_text = nullptr;
     size_t h_text_cap = 0;
+    cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // measure and write passes
     // the last run, whose statistics ag_context_stats() settles
     bool pending = false, had_far = false;
     int last_launches = 0;
@@ -918,6 +919,7 @@ ag_status ag_context_create(int32_t device, ag_context **out)
     AGB_CK(cudaEventCreate(&c->evf0));
     AGB_CK(cudaEventCreate(&c->evf1));
     AGB_CK(cudaMalloc(&c->d_counters, 4 * sizeof(unsigned long long)));
+    for (cudaEvent_t &e : c->tev) AGB_CK(cudaEventCreate(&e));
     *out = c.release();
     return AG_OK;
 }
@@ -943,6 +945,8 @@ ag_status ag_context_destroy(ag_context *ctx)
     if (ctx->evf1) cudaEventDestroy(ctx->evf1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->h_text) cudaFreeHost(ctx->h_text);
+    for (cudaEvent_t e : ctx->tev)
+        if (e) cudaEventDestroy(e);
     delete ctx;
     return AG_OK;
 }
@@ -1108,7 +1112,9 @@ static ag_status format_maps(ag_context *c, const ag_problem *p, const void *dma
     a.ext = (unsigned long long *)v;
     AGB_CK(B.ensure("map_bytes", (size_t)(n_out + 1) * sizeof(unsigned long long), &v));
     a.map_bytes = (unsigned long long *)v;
+    AGB_CK(cudaEventRecord(c->tev[0], s));
     AGB_CK(launch_text_measure(a, s));
+    AGB_CK(cudaEventRecord(c->tev[1], s));
     std::vector<unsigned long long> hb((size_t)n_out + 1), he((size_t)std::max(1, 2 * p->n_maps));
     AGB_CK(cudaMemcpyAsync(hb.data(), a.map_bytes, hb.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     AGB_CK(cudaMemcpyAsync(he.data(), a.ext, he.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -1116,7 +1122,9 @@ static ag_status format_maps(ag_context *c, const ag_problem *p, const void *dma
     const size_t total = (size_t)hb[(size_t)n_out];
     AGB_CK(B.ensure("text", total, &v));
     a.text = (char *)v;
+    AGB_CK(cudaEventRecord(c->tev[2], s));
     AGB_CK(launch_text_write(a, s));
+    AGB_CK(cudaEventRecord(c->tev[3], s));
     if (c->h_text_cap < total || !c->h_text) {
         if (c->h_text) cudaFreeHost(c->h_text);
         c->h_text = nullptr;
@@ -1126,6 +1134,11 @@ static ag_status format_maps(ag_context *c, const ag_problem *p, const void *dma
     }
     AGB_CK(cudaMemcpyAsync(c->h_text, a.text, total, cudaMemcpyDeviceToHost, s));
     AGB_CK(cudaStreamSynchronize(s));
+    float t_measure = 0.f, t_write = 0.f;
+    AGB_CK(cudaEventElapsedTime(&t_measure, c->tev[0], c->tev[1]));
+    AGB_CK(cudaEventElapsedTime(&t_write, c->tev[2], c->tev[3]));
+    c->stats.text_ms = (double)t_measure + (double)t_write;
+    c->stats.text_bytes = (int64_t)total;
     *text = c->h_text;
     for (int k = 0; k < n_out; k++) map_bytes[k] = (size_t)hb[(size_t)k];
     for (int k = 0; k < p->n_maps; k++) {

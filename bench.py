@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--batch-instances", type=int, default=256)
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-mode measurement")
     ap.add_argument("--no-vina", action="store_true", help="skip the batched Vina conformer measurement")
+    ap.add_argument("--no-text", action="store_true", help="skip the device map-text measurement")
     return ap.parse_args()
 
 
@@ -257,6 +258,8 @@ def main():
             "clocks": clk,
             "diagnostics": {"near_pairs_per_step": st.near_pairs, "fp64_fallbacks_per_step": st.fp64_fallbacks},
         }
+        if not args.no_text and world == 1:
+            line["map_text"] = map_text(ctx, plan, prob, rec, spec, work, args.steps)
         if not args.no_batch and world == 1:
             line["batched"] = batched_ensemble(ctx, args.batch_instances, work, stream)
         if not args.no_diff and world == 1:
@@ -276,6 +279,64 @@ def main():
     if world > 1:
         dist.destroy_process_group()
     shutil.rmtree(work, ignore_errors=True)
+
+
+def map_text(ctx, plan, prob, rec, spec, work: Path, steps: int):
+    """The map-file text (main.cpp:3481-3519) of the same map set, formatted on
+    the device from the plan's maps (ag_maps_format: measure, scan and write
+    kernels, then one copy of the text to pinned host memory), and the whole
+    one-shot call from host inputs to host text (ag_maps_compute_text).  The
+    host writer (the reference's fprintf loop restated with snprintf, one
+    thread) formats the same maps once for comparison."""
+    from autogrid_b200 import Job, synth
+    plan.run()
+    for _ in range(2):
+        mt = plan.format()
+    fmt_s, kern_ms = [], []
+    import torch
+    for _ in range(steps):
+        plan.run()
+        torch.cuda.synchronize()  # the maps are done before the clock starts
+        t0 = time.perf_counter()
+        mt = plan.format()
+        fmt_s.append(time.perf_counter() - t0)
+        kern_ms.append(ctx.stats().text_ms)
+    nbytes = mt.total
+    one = []
+    ctx.compute_text(prob)
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ctx.compute_text(prob)
+        one.append(time.perf_counter() - t0)
+    maps = plan.download()
+    d = work / "text_host"
+    d.mkdir(exist_ok=True)
+    g = synth.write_case(d, "bench", rec, spec)
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        j = Job(g.name, None)
+    finally:
+        os.chdir(cwd)
+    t0 = time.perf_counter()
+    j.write_maps(maps)
+    host_s = time.perf_counter() - t0
+    j.close()
+    shutil.rmtree(d, ignore_errors=True)
+    values = prob.points * prob.n_out
+    kms = float(np.median(kern_ms))
+    alg = values * 4 + nbytes  # maps read once, text written once
+    return {
+        "text_bytes": nbytes, "values": values,
+        "format_ms": float(np.median(fmt_s)) * 1e3,
+        "format_kernels_ms": kms,
+        "d2h_gbs": nbytes / (float(np.median(fmt_s)) - kms * 1e-3) / 1e9,
+        "kernels_algorithmic_gbs": alg / (kms * 1e-3) / 1e9,
+        "compute_text_ms": float(np.median(one)) * 1e3,
+        "host_writer_s": host_s,
+        "host_writer_note": "snprintf restatement of main.cpp:3481-3519, 1 thread, same maps",
+        "speedup_vs_host_writer": host_s / (float(np.median(fmt_s))),
+    }
 
 
 def batched_ensemble(ctx, n, work: Path, stream):

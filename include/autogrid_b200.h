@@ -151,6 +151,9 @@ typedef struct ag_stats {
     int32_t reserved;
     double  kernel_ms;         /* device time of the call's kernels (events)    */
     double  far_ms;            /* device time of the far-field e-map kernel      */
+    double  text_ms;           /* device time of the last ag_maps_format's
+                                  kernels (measure, scan and write passes)      */
+    int64_t text_bytes;        /* bytes of map text that call produced          */
 } ag_stats;
 
 typedef struct ag_context ag_context;
