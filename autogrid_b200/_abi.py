@@ -112,6 +112,7 @@ SIGNATURES = {
     "ag_job_free": (None, [C.c_void_p]),
     "ag_job_vina_problem": (C.c_int32, [C.c_void_p, C.POINTER(C.POINTER(ag_problem))]),
     "ag_job_bond_vectors": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_job_bond_topology": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "ag_job_bond_vectors_backward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_diff_create": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),
     "ag_diff_create_batch": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_int32,
@@ -125,6 +126,9 @@ SIGNATURES = {
     "ag_diff_closest_h": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ag_diff_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p]),
+    "ag_diff_set_bonds": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_diff_set_atoms_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_diff_backward_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_diff_timing": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "ag_diff_destroy": (C.c_int, [C.c_void_p]),
     "ag_emap_compute_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),

@@ -203,6 +203,12 @@ class Job:
                                                      out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def bond_topology(self) -> np.ndarray:
+        """int32 [N, 7]: kind (AG_BOND_*), i1, i2, nb, nbr[3] per atom."""
+        out = np.zeros((self.n_atoms, 7), dtype=np.int32)
+        check(self._lib.ag_job_bond_topology(self._h, out.ctypes.data_as(C.c_void_p)))
+        return out
+
     def fail(self, message: str) -> None:
         self._lib.ag_job_fail(self._h, message.encode())
 
@@ -392,6 +398,25 @@ class Diff:
                                          gq.ctypes.data_as(C.c_void_p), g1.ctypes.data_as(C.c_void_p),
                                          g2.ctypes.data_as(C.c_void_p)))
         return {"coord": gc, "charge": gq, "rvector": g1, "rvector2": g2}
+
+    def set_bonds(self, job: "Job") -> None:
+        """Attach the job's bond topology (ag_job_bond_topology) so that
+        device-resident updates rebuild the bond vectors on the device."""
+        topo = job.bond_topology()
+        check(self._lib.ag_diff_set_bonds(self._h, topo.ctypes.data_as(C.c_void_p)))
+
+    def set_atoms_device(self, coord_ptr: int, charge_ptr: int | None = None) -> None:
+        """Every conformer's coordinates [K][N][3] (and charges [K][N]) from
+        device pointers to FP64 arrays (ag_diff_set_atoms_device)."""
+        check(self._lib.ag_diff_set_atoms_device(self._h, C.c_void_p(int(coord_ptr)),
+                                                 None if charge_ptr is None else C.c_void_p(int(charge_ptr))))
+
+    def backward_device(self, grad_ptr: int, g_coord_ptr: int | None, g_charge_ptr: int | None) -> None:
+        """Adjoint with the map gradient and the FP64 outputs [K][N][3], [K][N]
+        in device memory (ag_diff_backward_device)."""
+        ptr = lambda v: None if v is None else C.c_void_p(int(v))  # noqa: E731
+        check(self._lib.ag_diff_backward_device(self._h, C.c_void_p(int(grad_ptr)), ptr(g_coord_ptr),
+                                                ptr(g_charge_ptr)))
 
     def timing(self) -> tuple:
         """(forward_ms, closest_h_ms, backward_ms) of the last calls (device events)."""

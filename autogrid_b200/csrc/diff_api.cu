@@ -79,6 +79,9 @@ struct ag_diff {
     cudaEvent_t ev[6] = {};
     float fwd_ms = 0, ch_ms = 0, bwd_ms = 0;
     bool have_ch = false, have_fwd = false;
+    // device-resident atom updates (ag_diff_set_atoms_device)
+    int *d_topo = nullptr, *d_cell_of = nullptr, *d_cell_count = nullptr, *d_bad = nullptr;
+    bool host_stale = false;  // the host copies lag the device arrays
 
     ~ag_diff()
     {
@@ -99,6 +102,7 @@ struct ag_diff {
     }
     size_t map_bytes() const { return esz * (size_t)P * n_maps * n_conf; }
     ag_status upload_conformer(int k);
+    ag_status refresh_host();
 };
 
 namespace {
@@ -184,6 +188,29 @@ ag_status ag_diff::upload_conformer(int k)
                           cudaMemcpyHostToDevice, stream));
     DF_CK(cudaMemcpyAsync(d_cell_atoms + o1, atoms.data(), (size_t)N * sizeof(int), cudaMemcpyHostToDevice, stream));
     DF_CK(cudaStreamSynchronize(stream));  // host vectors are locals
+    return AG_OK;
+}
+
+// Host copies of every conformer's coordinates, charges and bond vectors from
+// the device arrays (after device-resident updates).
+ag_status ag_diff::refresh_host()
+{
+    if (!host_stale) return AG_OK;
+    const size_t NK = (size_t)N * n_conf;
+    std::vector<double> x(NK), y(NK), z(NK);
+    DF_CK(cudaMemcpyAsync(x.data(), d_x, NK * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DF_CK(cudaMemcpyAsync(y.data(), d_y, NK * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DF_CK(cudaMemcpyAsync(z.data(), d_z, NK * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DF_CK(cudaMemcpyAsync(charge.data(), d_q, NK * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DF_CK(cudaMemcpyAsync(rv.data(), d_rv, 3 * NK * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DF_CK(cudaMemcpyAsync(rv2.data(), d_rv2, 3 * NK * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    DF_CK(cudaStreamSynchronize(stream));
+    for (size_t i = 0; i < NK; i++) {
+        coord[3 * i] = x[i];
+        coord[3 * i + 1] = y[i];
+        coord[3 * i + 2] = z[i];
+    }
+    host_stale = false;
     return AG_OK;
 }
 
@@ -396,6 +423,8 @@ ag_status ag_diff_set_conformer(ag_diff *d, int32_t k, const double *coord, cons
     for (size_t i = 0; charge && i < N; i++)
         if (!std::isfinite(charge[i])) { set_last_error("ag_diff_set_atoms: non-finite charge"); return AG_ERR_INVALID; }
     DF_CK(cudaSetDevice(d->device));
+    const ag_status rs = d->refresh_host();
+    if (rs != AG_OK) return rs;
     if (coord) std::copy(coord, coord + 3 * N, d->coord.begin() + o3);
     if (charge) std::copy(charge, charge + N, d->charge.begin() + o1);
     if (rvector) std::copy(rvector, rvector + 3 * N, d->rv.begin() + o3);
@@ -507,6 +536,80 @@ ag_status ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_de
     }
     DF_CK(cudaStreamSynchronize(s));
     DF_CK(cudaEventElapsedTime(&d->bwd_ms, d->ev[2], d->ev[3]));
+    return AG_OK;
+}
+
+ag_status ag_diff_set_bonds(ag_diff *d, const int32_t *topo)
+{
+    if (!d || !topo) { set_last_error("ag_diff_set_bonds: null argument"); return AG_ERR_INVALID; }
+    const int N = d->N;
+    for (int a = 0; a < N; a++) {
+        const int32_t *t = topo + 7 * (size_t)a;
+        const int kind = t[0];
+        bool ok = kind >= AG_BOND_NONE && kind <= AG_BOND_A1;
+        auto in = [&](int32_t i) { return i >= 0 && i < N; };
+        if (ok && (kind == AG_BOND_D1 || kind == AG_BOND_A2_ONE || kind == AG_BOND_A2_DIS || kind == AG_BOND_A2_TWO))
+            ok = in(t[1]);
+        if (ok && kind == AG_BOND_A2_TWO) ok = in(t[2]);
+        if (ok && kind == AG_BOND_A2_ONE) ok = t[2] == -1 || in(t[2]);
+        if (ok && kind == AG_BOND_A1) {
+            ok = t[3] >= 0 && t[3] <= 3;
+            for (int b = 0; ok && b < t[3]; b++) ok = in(t[4 + b]);
+        }
+        if (!ok) { set_last_error("ag_diff_set_bonds: invalid topology entry"); return AG_ERR_INVALID; }
+    }
+    DF_CK(cudaSetDevice(d->device));
+    if (!d->d_topo) DF_CK(d->alloc(&d->d_topo, 7 * (size_t)std::max(N, 1)));
+    DF_CK(cudaMemcpyAsync(d->d_topo, topo, 7 * (size_t)N * sizeof(int32_t), cudaMemcpyHostToDevice, d->stream));
+    DF_CK(cudaStreamSynchronize(d->stream));
+    return AG_OK;
+}
+
+ag_status ag_diff_set_atoms_device(ag_diff *d, const double *coord, const double *charge)
+{
+    if (!d || !coord) { set_last_error("ag_diff_set_atoms_device: null argument"); return AG_ERR_INVALID; }
+    DF_CK(cudaSetDevice(d->device));
+    cudaStream_t s = d->stream;
+    const int N = d->N, K = d->n_conf;
+    const size_t NK = (size_t)N * K;
+    if (!d->d_bad) {
+        DF_CK(d->alloc(&d->d_bad, 1));
+        DF_CK(d->alloc(&d->d_cell_of, std::max<size_t>(NK, 1)));
+        DF_CK(d->alloc(&d->d_cell_count, std::max<size_t>(d->ncells * K, 1)));
+    }
+    DF_CK(cudaMemsetAsync(d->d_bad, 0, sizeof(int), s));
+    DF_CK(launch_split_atoms((long long)NK, coord, charge, d->d_x, d->d_y, d->d_z, d->d_q, d->d_bad, s));
+    int bad = 0;
+    DF_CK(cudaMemcpyAsync(&bad, d->d_bad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DF_CK(cudaStreamSynchronize(s));
+    d->host_stale = true;  // the split already replaced the device coordinates
+    if (bad) {
+        set_last_error("ag_diff_set_atoms_device: non-finite coordinate or charge");
+        return AG_ERR_INVALID;
+    }
+    if (d->d_topo) DF_CK(launch_bond_vectors(K, N, d->d_topo, d->d_x, d->d_y, d->d_z, d->d_rv, d->d_rv2, s));
+    DF_CK(launch_cell_lists(d->args, d->d_cell_of, d->d_cell_count, s));
+    DF_CK(cudaStreamSynchronize(s));
+    return AG_OK;
+}
+
+ag_status ag_diff_backward_device(ag_diff *d, const void *grad_maps, double *g_coord, double *g_charge)
+{
+    if (!d || !grad_maps) { set_last_error("ag_diff_backward_device: null argument"); return AG_ERR_INVALID; }
+    ag_status st = ag_diff_backward(d, grad_maps, 1, nullptr, nullptr, nullptr, nullptr);
+    if (st != AG_OK) return st;
+    cudaStream_t s = d->stream;
+    const size_t N = d->N, K = d->n_conf;
+    for (size_t k = 0; k < K; k++) {
+        const double *base = d->d_grad + 10 * N * k;
+        if (g_coord)
+            DF_CK(cudaMemcpyAsync(g_coord + 3 * N * k, base, 3 * N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        if (g_charge)
+            DF_CK(cudaMemcpyAsync(g_charge + N * k, base + 3 * N, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    if (g_coord && d->d_topo)
+        DF_CK(launch_bond_vectors_adj((int)K, (int)N, d->d_topo, d->d_x, d->d_y, d->d_z, d->d_grad, g_coord, s));
+    DF_CK(cudaStreamSynchronize(s));
     return AG_OK;
 }
 

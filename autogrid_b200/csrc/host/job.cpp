@@ -1462,6 +1462,25 @@ ag_status ag_job_bond_vectors_backward(const ag_job *job, const double *coord, c
     return AG_OK;
 }
 
+ag_status ag_job_bond_topology(const ag_job *job, int32_t *topo)
+{
+    if (!job || !topo) { agb::set_last_error("ag_job_bond_topology: null argument"); return AG_ERR_INVALID; }
+    static_assert(agb::BondRec::D1 == AG_BOND_D1 && agb::BondRec::A2_ONE == AG_BOND_A2_ONE &&
+                      agb::BondRec::A2_DIS == AG_BOND_A2_DIS && agb::BondRec::A2_TWO == AG_BOND_A2_TWO &&
+                      agb::BondRec::A1 == AG_BOND_A1,
+                  "bond kinds");
+    const auto &br = job->job.bondrec;
+    for (size_t a = 0; a < br.size(); a++) {
+        int32_t *t = topo + 7 * a;
+        t[0] = br[a].kind;
+        t[1] = br[a].i1;
+        t[2] = br[a].i2;
+        t[3] = br[a].nb;
+        for (int b = 0; b < 3; b++) t[4 + b] = br[a].nbr[b];
+    }
+    return AG_OK;
+}
+
 const char *ag_last_error(void) { return agb::last_error(); }
 int32_t ag_abi_version(void) { return AG_ABI_VERSION; }
 

@@ -120,6 +120,14 @@ __host__ __device__ inline ConfView conf_view(const DiffArgs &a, DiffGrads g, in
 }
 
 cudaError_t launch_closest_h(const DiffArgs &a, int *ch, cudaStream_t s);
+// kernels/diff_atoms.cu: atom state rebuilt on the device
+cudaError_t launch_split_atoms(long long KN, const double *coord, const double *charge, double *x, double *y,
+                               double *z, double *q, int *bad, cudaStream_t s);
+cudaError_t launch_bond_vectors(int K, int N, const int *topo, const double *x, const double *y, const double *z,
+                                double *rv, double *rv2, cudaStream_t s);
+cudaError_t launch_bond_vectors_adj(int K, int N, const int *topo, const double *x, const double *y, const double *z,
+                                    const double *grad, double *gx, cudaStream_t s);
+cudaError_t launch_cell_lists(const DiffArgs &a, int *cell_of, int *count, cudaStream_t s);
 cudaError_t launch_emap_lin(bool fp64, const DiffArgs &a, const void *eps, void *emap, cudaStream_t s);
 cudaError_t launch_emap_lin_adj(bool fp64, const DiffArgs &a, const void *eps, const void *g_e, DiffGrads g,
                                 cudaStream_t s);

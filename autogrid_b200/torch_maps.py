@@ -7,17 +7,18 @@
     maps = maps_fn(coords, charges)                    # [n_maps, n1z, n1y, n1x] on cuda
     loss = (w * maps).sum(); loss.backward()           # coords.grad, charges.grad
 
-Coordinates are in the problem's centred frame.  The forward recomputes the
-bond vectors at the given coordinates with the bonded neighbours found at load
-time (ag_job_bond_vectors); the backward runs the hand-written adjoint kernels
-(ag_diff_backward) and chains the bond-vector gradients back to the
-coordinates in FP64 (ag_job_bond_vectors_backward).  The closest DS/D1 atom of
-each grid point is searched at the first forward and kept afterwards
-(keep_closest_h=False searches it at every forward).
+Coordinates are in the problem's centred frame.  Everything stays on the
+device: the forward hands the coordinates and charges to the engine as device
+arrays (ag_diff_set_atoms_device), which rebuilds the bond vectors on the bond
+topology found at load time (ag_job_bond_topology) and the cell lists, then
+computes the maps into the output tensor; the backward runs the hand-written
+adjoint kernels and the bond-vector chain rule on the device
+(ag_diff_backward_device).  The closest DS/D1 atom of each grid point is
+searched at the first forward and kept afterwards (keep_closest_h=False
+searches it at every forward).
 """
 from __future__ import annotations
 
-import numpy as np
 import torch
 
 from .api import Context, Diff, Job
@@ -32,6 +33,7 @@ class GridMaps:
         self.device = torch.device("cuda", device)
         self.ctx = Context(device)
         self.diff = Diff(self.ctx, self.problem, precision)
+        self.diff.set_bonds(job)
         self.dtype = torch.float64 if precision == "fp64" else torch.float32
         self.keep_closest_h = keep_closest_h
         self.generation = 0
@@ -40,10 +42,10 @@ class GridMaps:
     def __call__(self, coords: torch.Tensor, charges: torch.Tensor) -> torch.Tensor:
         return _GridMapsFn.apply(coords, charges, self)
 
-    def _run(self, coord: np.ndarray, charge: np.ndarray, out: torch.Tensor) -> None:
-        rv, rv2 = self.job.bond_vectors(coord)
-        self.diff.set_atoms(coord, charge, rv, rv2)
-        torch.cuda.current_stream(self.device).synchronize()  # out may reuse memory torch just released
+    def _run(self, coord: torch.Tensor, charge: torch.Tensor, out: torch.Tensor) -> None:
+        # the inputs are ready and out may reuse memory torch just released
+        torch.cuda.current_stream(self.device).synchronize()
+        self.diff.set_atoms_device(coord.data_ptr(), charge.data_ptr())
         self.diff.forward(keep_closest_h=self.keep_closest_h and self._searched, device_out=out.data_ptr())
         self._searched = True
         self.generation += 1
@@ -52,8 +54,8 @@ class GridMaps:
 class _GridMapsFn(torch.autograd.Function):
     @staticmethod
     def forward(ctx, coords, charges, engine: GridMaps):
-        coord = coords.detach().to("cpu", torch.float64).numpy().reshape(-1, 3)
-        charge = charges.detach().to("cpu", torch.float64).numpy().reshape(-1)
+        coord = coords.detach().to(engine.device, torch.float64).reshape(-1, 3).contiguous()
+        charge = charges.detach().to(engine.device, torch.float64).reshape(-1).contiguous()
         out = torch.empty(engine.diff.shape, dtype=engine.dtype, device=engine.device)
         engine._run(coord, charge, out)
         ctx.engine = engine
@@ -71,9 +73,9 @@ class _GridMapsFn(torch.autograd.Function):
             engine._run(ctx.coord, ctx.charge, scratch)
             engine.keep_closest_h = keep
         g = grad.to(device=engine.device, dtype=engine.dtype).contiguous()
+        g_coord = torch.empty((engine.problem.n_atoms, 3), dtype=torch.float64, device=engine.device)
+        g_charge = torch.empty((engine.problem.n_atoms,), dtype=torch.float64, device=engine.device)
         torch.cuda.current_stream(engine.device).synchronize()
-        out = engine.diff.backward(device_ptr=g.data_ptr())
-        g_coord = out["coord"] + engine.job.bond_vectors_backward(ctx.coord, out["rvector"], out["rvector2"])
+        engine.diff.backward_device(g.data_ptr(), g_coord.data_ptr(), g_charge.data_ptr())
         cs, cdt, cdev, qs, qdt, qdev = ctx.shapes
-        return (torch.from_numpy(g_coord).reshape(cs).to(device=cdev, dtype=cdt),
-                torch.from_numpy(out["charge"]).reshape(qs).to(device=qdev, dtype=qdt), None)
+        return (g_coord.reshape(cs).to(device=cdev, dtype=cdt), g_charge.reshape(qs).to(device=qdev, dtype=qdt), None)

@@ -550,6 +550,24 @@ def vina_conformers(ctx, work: Path, stream, K: int = 32, reps: int = 5):
         df.forward(keep_closest_h=True)
         df.backward(device_ptr=grad.data_ptr())
         e2e.append(time.perf_counter() - t0)
+    # the same with the coordinates updated on the device: one pinned host
+    # array of all conformers in, cell lists rebuilt by kernels, dL/d(coord)
+    # of all conformers back into a pinned host array
+    host_c = torch.tensor(np.stack(confs), dtype=torch.float64).pin_memory()
+    host_g = torch.empty((K, vp.n_atoms, 3), dtype=torch.float64).pin_memory()
+    dev_c = torch.empty_like(host_c, device="cuda")
+    dev_g = torch.empty_like(host_g, device="cuda")
+    e2e_dev = []
+    for it in range(4):
+        t0 = time.perf_counter()
+        dev_c.copy_(host_c, non_blocking=True)
+        torch.cuda.synchronize()
+        df.set_atoms_device(dev_c.data_ptr())
+        df.forward(keep_closest_h=True)
+        df.backward_device(grad.data_ptr(), dev_g.data_ptr(), None)
+        host_g.copy_(dev_g)
+        if it:
+            e2e_dev.append(time.perf_counter() - t0)
     df.close()
     P, M = vp.points, vp.n_maps
     fwd_ms, bwd_ms = float(np.median(fw)), float(np.median(bw))
@@ -559,6 +577,10 @@ def vina_conformers(ctx, work: Path, stream, K: int = 32, reps: int = 5):
             "forward_evals_per_s": K * P * M / (fwd_ms * 1e-3),
             "forward_backward_evals_per_s": K * P * M / ((fwd_ms + bwd_ms) * 1e-3),
             "e2e_forward_backward_ms": float(np.median(e2e)) * 1e3,
+            "e2e_note": "host coordinates through ag_diff_set_conformer (host cell lists) per conformer",
+            "e2e_device_update_ms": float(np.median(e2e_dev)) * 1e3,
+            "e2e_device_update_note": "all conformers' coordinates H2D, ag_diff_set_atoms_device (cell lists "
+                                      "on the device), forward, ag_diff_backward_device, dL/dcoord D2H",
             "launches": {"forward": 1, "backward": 1},
             "parity": "unpinned against the reference (its Vina path is compiled out); tables pinned to the "
                       "source as written, maps to the C oracle"}

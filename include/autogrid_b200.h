@@ -341,6 +341,19 @@ ag_status   ag_diff_closest_h(ag_diff *d, int32_t *host_out);
 ag_status   ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_device,
                              double *g_coord, double *g_charge, double *g_rvector,
                              double *g_rvector2);
+/* Device-resident atom updates.  ag_diff_set_bonds attaches a bond topology
+ * (ag_job_bond_topology, host memory); ag_diff_set_atoms_device then takes
+ * DEVICE arrays for every conformer at once -- coord [K][3N], charge [K][N]
+ * (NULL keeps the charges) -- and rebuilds on the device the bond vectors (when
+ * a topology is attached; otherwise they are kept) and the cell lists.  The
+ * arrays must be ready when the call is made and may be reused once it
+ * returns.  ag_diff_backward_device is ag_diff_backward with the map gradient
+ * and the outputs in device memory: g_coord [K][3N] includes the bond vectors'
+ * dependence on the coordinates when a topology is attached (the pair terms
+ * only otherwise), g_charge [K][N]; either may be NULL. */
+ag_status   ag_diff_set_bonds(ag_diff *d, const int32_t *topo);
+ag_status   ag_diff_set_atoms_device(ag_diff *d, const double *coord, const double *charge);
+ag_status   ag_diff_backward_device(ag_diff *d, const void *grad_maps, double *g_coord, double *g_charge);
 /* Device times (ms) of the last forward (e map + short-range maps), of the
  * last closest-H search and of the last backward. */
 ag_status   ag_diff_timing(const ag_diff *d, float *forward_ms, float *closest_h_ms,
@@ -368,6 +381,20 @@ ag_status          ag_job_write_text(ag_job *job, const char *text, const size_t
 /* Record a fatal error in the job's GLG ("Unsuccessful Completion"). */
 void               ag_job_fail(ag_job *job, const char *message);
 void               ag_job_free(ag_job *job);
+/* Bond topology behind the bond vectors (frozen at load, main.cpp:2297-2659):
+ * topo [n_atoms][7] = kind (AG_BOND_*), i1, i2, nb, nbr[3] per atom, the
+ * atoms whose coordinates define rvector/rvector2 of that atom:
+ *   AG_BOND_D1      rvector = unit(x - x[i1])                    (donor H)
+ *   AG_BOND_A2_ONE  rvector = unit(x - x[i1]); with i2 >= 0,
+ *                   rvector2 = unit(rvector x unit(x[i1] - x[i2]))
+ *   AG_BOND_A2_DIS  rvector = unit(x - x[i1])
+ *   AG_BOND_A2_TWO  rvector2 = unit(x[i2] - x[i1]), rvector = unit of the
+ *                   component of x - x[i1] normal to rvector2
+ *   AG_BOND_A1      rvector = -unit(mean over nbr[0..nb) of x - x[nbr])
+ * For ag_diff_set_bonds. */
+enum { AG_BOND_NONE = 0, AG_BOND_D1 = 1, AG_BOND_A2_ONE = 2, AG_BOND_A2_DIS = 3, AG_BOND_A2_TWO = 4,
+       AG_BOND_A1 = 5 };
+ag_status          ag_job_bond_topology(const ag_job *job, int32_t *topo);
 /* The job with Vina-potential tables in place of the AD4 ones: the table
  * fill of main.cpp:2081-2126 (compiled out of the reference build,
  * use_vina_potential = FALSE at main.cpp:263) with the xs radii of
