@@ -66,7 +66,17 @@ class ag_opts(C.Structure):
 class ag_stats(C.Structure):
     _fields_ = [("near_pairs", C.c_int64), ("fp64_fallbacks", C.c_int64), ("far_pairs", C.c_int64),
                 ("gpu_launches", C.c_int32), ("reserved", C.c_int32), ("kernel_ms", C.c_double),
-                ("far_ms", C.c_double), ("text_ms", C.c_double), ("text_bytes", C.c_int64)]
+                ("far_ms", C.c_double), ("text_ms", C.c_double), ("text_bytes", C.c_int64),
+                ("table_ms", C.c_double)]
+
+
+class ag_table_params(C.Structure):
+    _fields_ = [("n_rec_types", C.c_int32), ("n_atom_maps", C.c_int32),
+                ("cA", C.POINTER(C.c_double)), ("cB", C.POINTER(C.c_double)),
+                ("Rij", C.POINTER(C.c_double)), ("epsij", C.POINTER(C.c_double)),
+                ("xA", C.POINTER(C.c_int32)), ("xB", C.POINTER(C.c_int32)),
+                ("map_is_covalent", C.POINTER(C.c_int32)),
+                ("r_smooth", C.c_double), ("coeff_desolv", C.c_double), ("dddiel", C.c_int32)]
 
 
 class ag_tuning(C.Structure):
@@ -90,6 +100,7 @@ SIGNATURES = {
     "ag_plan_points": (C.c_size_t, [C.c_void_p]),
     "ag_plan_download": (C.c_int, [C.c_void_p, C.c_void_p]),
     "ag_plan_destroy": (C.c_int, [C.c_void_p]),
+    "ag_tables_build": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_maps_format": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.c_void_p, C.c_int32,
                                  C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_maps_compute_text": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts),
@@ -112,6 +123,7 @@ SIGNATURES = {
     "ag_job_free": (None, [C.c_void_p]),
     "ag_job_vina_problem": (C.c_int32, [C.c_void_p, C.POINTER(C.POINTER(ag_problem))]),
     "ag_job_bond_vectors": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ag_job_table_params": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "ag_job_bond_topology": (C.c_int32, [C.c_void_p, C.c_void_p]),
     "ag_job_bond_vectors_backward": (C.c_int32, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ag_diff_create": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),

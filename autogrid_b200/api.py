@@ -101,6 +101,11 @@ class Problem:
         s.e_vdw_hb = _ptr(a["e_vdw_hb"], C.c_float)
         s.sol_fn = _ptr(a["sol_fn"], C.c_double)
         s.r_epsilon_fn = _ptr(a["r_epsilon_fn"], C.c_double)
+        dt = getattr(self, "device_tables", None)
+        if dt is not None:  # (e_vdw_hb, sol_fn, r_epsilon_fn) device pointers, e.g. from ag_tables_build
+            s.e_vdw_hb = C.cast(C.c_void_p(int(dt[0])), C.POINTER(C.c_float))
+            s.sol_fn = C.cast(C.c_void_p(int(dt[1])), C.POINTER(C.c_double))
+            s.r_epsilon_fn = C.cast(C.c_void_p(int(dt[2])), C.POINTER(C.c_double)) if dt[2] else None
         for k, v in self.scalars.items():
             setattr(s, k, v)
         self._struct = s  # arrays stay alive with self
@@ -203,6 +208,13 @@ class Job:
                                                      out.ctypes.data_as(C.c_void_p)))
         return out
 
+    def table_params(self) -> "_abi.ag_table_params":
+        """The job's table parameters for ag_tables_build (ag_job_table_params;
+        the arrays belong to the job)."""
+        tp = _abi.ag_table_params()
+        check(self._lib.ag_job_table_params(self._h, C.byref(tp)))
+        return tp
+
     def bond_topology(self) -> np.ndarray:
         """int32 [N, 7]: kind (AG_BOND_*), i1, i2, nb, nbr[3] per atom."""
         out = np.zeros((self.n_atoms, 7), dtype=np.int32)
@@ -295,6 +307,15 @@ class Context:
         (ag_maps_compute_text)."""
         opts = ag_opts(precision=_PREC[precision], table_mode=_abi.AG_TABLE_NEAREST)
         return _text_call(self._lib.ag_maps_compute_text, problem, self._h, C.byref(opts))
+
+    def build_tables(self, params, e_vdw_hb: int, sol_fn: int, r_epsilon_fn: int | None) -> float:
+        """Energy tables on the device (ag_tables_build) into the given buffers
+        (host or device addresses); returns the kernels' device time in ms."""
+        check(self._lib.ag_tables_build(self._h, C.byref(params), C.c_void_p(int(e_vdw_hb)), C.c_void_p(int(sol_fn)),
+                                        None if not r_epsilon_fn else C.c_void_p(int(r_epsilon_fn))))
+        st = ag_stats()
+        check(self._lib.ag_context_stats(self._h, C.byref(st)))
+        return st.table_ms
 
     def format(self, problem: Problem, device_ptr: int, elem_size: int = 4) -> MapText:
         """Format device-resident maps of `problem`'s layout (ag_maps_format)."""

@@ -28,7 +28,8 @@ CXX_SOURCES = [CSRC / "host" / "params.cpp", CSRC / "host" / "job.cpp"]
 CU_SOURCES = [CSRC / "capi.cu", CSRC / "kernels" / "emap.cu", CSRC / "kernels" / "near.cu",
               CSRC / "kernels" / "diag.cu", CSRC / "kernels" / "noalloc.cu", CSRC / "diff_api.cu",
               CSRC / "kernels" / "diff_emap.cu", CSRC / "kernels" / "diff_near.cu", CSRC / "kernels" / "distmap.cu",
-              CSRC / "kernels" / "maptext.cu", CSRC / "kernels" / "diff_atoms.cu"]
+              CSRC / "kernels" / "maptext.cu", CSRC / "kernels" / "diff_atoms.cu",
+              CSRC / "kernels" / "tables.cu"]
 CLI_SOURCES = [CSRC / "host" / "cli.cpp"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -17,6 +17,7 @@
 #include "autogrid_b200.h"
 #include "kernels/kernels.h"
 #include "kernels/maptext.h"
+#include "kernels/tables.h"
 
 namespace agb {
 void set_last_error(const std::string &m);
@@ -139,6 +140,7 @@ struct ag_context {
     char *h_text = nullptr;
     size_t h_text_cap = 0;
     cudaEvent_t tev[4] = {nullptr, nullptr, nullptr, nullptr};  // measure and write passes
+    BufferSet table_bufs;  // ag_tables_build
     // the last run, whose statistics ag_context_stats() settles
     bool pending = false, had_far = false;
     int last_launches = 0;
@@ -232,6 +234,19 @@ int context_device(const ag_context *c) { return c->device; }
 }  // namespace agb
 
 namespace {
+
+// True for memory that only the device can read (cudaMalloc'd); host,
+// pinned and managed memory are read on the host.
+bool is_device_memory(const void *ptr)
+{
+    if (!ptr) return false;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice;
+}
 
 template <class T>
 cudaError_t upload(BufferSet *b, const char *name, const T *src, size_t n, T **dst, cudaStream_t s, size_t *acc)
@@ -400,24 +415,35 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     // tables: vdW/H-bond transposed to [type][bin][column], columns in kernel order
     pl->mpad = (int)pl->groups.size() * NG_MAX;
     const int nT = std::max(1, p->n_rec_types);
-    std::vector<float> vdwT((size_t)nT * AG_NEINT * pl->mpad, 0.f);
+    std::vector<int> colmap(pl->mpad, -1);
     for (const NearGroup &g : pl->groups)
-        for (int k = 0; k < g.ng; k++) {
-            const int m = g.out_map[k];
-            if (skip_map[m]) continue;
+        for (int k = 0; k < g.ng; k++)
+            if (!skip_map[g.out_map[k]]) colmap[g.col0 + k] = g.out_map[k];
+    const bool dev_tables = is_device_memory(p->e_vdw_hb);
+    if (dev_tables != is_device_memory(p->sol_fn) || (p->dddiel && dev_tables != is_device_memory(p->r_epsilon_fn)))
+        return invalid("the problem's tables must all be host memory or all device memory");
+    std::vector<float> vdwT, far_tab, etab, solf;
+    std::vector<double> reps;
+    if (!dev_tables) {
+        vdwT.assign((size_t)nT * AG_NEINT * pl->mpad, 0.f);
+        for (int c = 0; c < pl->mpad; c++) {
+            const int m = colmap[c];
+            if (m < 0) continue;
             for (int t = 0; t < p->n_rec_types; t++)
                 for (int b = 0; b < AG_NEINT; b++)
-                    vdwT[((size_t)t * AG_NEINT + b) * pl->mpad + g.col0 + k] =
-                        p->e_vdw_hb[((size_t)t * nAM + m) * AG_NEINT + b];
+                    vdwT[((size_t)t * AG_NEINT + b) * pl->mpad + c] = p->e_vdw_hb[((size_t)t * nAM + m) * AG_NEINT + b];
         }
-    std::vector<float> far_tab(AG_NDIEL, 0.f), etab(AG_NDIEL), solf(AG_NDIEL);
-    std::vector<double> reps(AG_NDIEL, 0.0);
-    for (int k = 0; k < AG_NDIEL; k++) {
-        const double f = p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal;
-        if (p->dddiel) reps[k] = p->r_epsilon_fn[k];
-        far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
-        etab[k] = (float)(f * p->coeff_estat);
-        solf[k] = (float)p->sol_fn[k];
+        far_tab.assign(AG_NDIEL, 0.f);
+        etab.resize(AG_NDIEL);
+        solf.resize(AG_NDIEL);
+        reps.assign(AG_NDIEL, 0.0);
+        for (int k = 0; k < AG_NDIEL; k++) {
+            const double f = p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal;
+            if (p->dddiel) reps[k] = p->r_epsilon_fn[k];
+            far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
+            etab[k] = (float)(f * p->coeff_estat);
+            solf[k] = (float)p->sol_fn[k];
+        }
     }
 
     // far-field chunking: enough CTAs for ~8 waves per launch; a slab-pipelined
@@ -474,12 +500,30 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     AGB_CK(upload(B, "m_hbond", mhb.data(), mhb.size(), &dmhb, s, acc));
     AGB_CK(upload(B, "m_solpar", ms.data(), ms.size(), &dms, s, acc));
     AGB_CK(upload(B, "m_vol", mv.data(), mv.size(), &dmv, s, acc));
-    AGB_CK(upload(B, "vdwT", vdwT.data(), vdwT.size(), &pl->vdwT, s, acc));
-    AGB_CK(upload(B, "far_tab", far_tab.data(), far_tab.size(), &pl->far_tab, s, acc));
-    AGB_CK(upload(B, "etab", etab.data(), etab.size(), &pl->etab, s, acc));
-    AGB_CK(upload(B, "solf", solf.data(), solf.size(), &pl->solf, s, acc));
-    AGB_CK(upload(B, "sol_fn", p->sol_fn, AG_NDIEL, &dsolfn, s, acc));
-    AGB_CK(upload(B, "reps", reps.data(), reps.size(), &dreps, s, acc));
+    if (!dev_tables) {
+        AGB_CK(upload(B, "vdwT", vdwT.data(), vdwT.size(), &pl->vdwT, s, acc));
+        AGB_CK(upload(B, "far_tab", far_tab.data(), far_tab.size(), &pl->far_tab, s, acc));
+        AGB_CK(upload(B, "etab", etab.data(), etab.size(), &pl->etab, s, acc));
+        AGB_CK(upload(B, "solf", solf.data(), solf.size(), &pl->solf, s, acc));
+        AGB_CK(upload(B, "sol_fn", p->sol_fn, AG_NDIEL, &dsolfn, s, acc));
+        AGB_CK(upload(B, "reps", reps.data(), reps.size(), &dreps, s, acc));
+    } else {
+        // tables already on the device (e.g. from ag_tables_build): packed by kernels
+        int *dcol;
+        void *vv;
+        AGB_CK(upload(B, "colmap", colmap.data(), colmap.size(), &dcol, s, acc));
+        AGB_CK(B->ensure("vdwT", (size_t)nT * AG_NEINT * pl->mpad * sizeof(float), &vv)); pl->vdwT = (float *)vv;
+        AGB_CK(B->ensure("far_tab", AG_NDIEL * sizeof(float), &vv)); pl->far_tab = (float *)vv;
+        AGB_CK(B->ensure("etab", AG_NDIEL * sizeof(float), &vv)); pl->etab = (float *)vv;
+        AGB_CK(B->ensure("solf", AG_NDIEL * sizeof(float), &vv)); pl->solf = (float *)vv;
+        AGB_CK(B->ensure("sol_fn", AG_NDIEL * sizeof(double), &vv)); dsolfn = (double *)vv;
+        AGB_CK(B->ensure("reps", AG_NDIEL * sizeof(double), &vv)); dreps = (double *)vv;
+        AGB_CK(cudaMemcpyAsync(dsolfn, p->sol_fn, AG_NDIEL * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        AGB_CK(cudaMemsetAsync(pl->vdwT, 0, (size_t)nT * AG_NEINT * pl->mpad * sizeof(float), s));
+        AGB_CK(launch_pack_tables(p->e_vdw_hb, p->n_rec_types, nAM, dcol, pl->mpad, pl->vdwT, p->sol_fn,
+                                  p->dddiel ? p->r_epsilon_fn : nullptr, p->dddiel, p->invdielcal, p->coeff_estat,
+                                  pl->far_tab, pl->etab, pl->solf, dreps, s));
+    }
 
     d.x = dx; d.y = dy; d.z = dz; d.q = dq; d.vol = dvol; d.solpar = dsol; d.rv = drv; d.rv2 = drv2;
     d.type = dtype; d.hbond = dhb; d.rexp = drexp; d.disorder = ddis;
@@ -1145,6 +1189,61 @@ static ag_status format_maps(ag_context *c, const ag_problem *p, const void *dma
         if (emin) emin[k] = text_key_to_double(he[2 * (size_t)k]);
         if (emax) emax[k] = text_key_to_double(he[2 * (size_t)k + 1]);
     }
+    return AG_OK;
+}
+
+ag_status ag_tables_build(ag_context *ctx, const ag_table_params *tp, float *e_vdw_hb, double *sol_fn,
+                          double *r_epsilon_fn)
+{
+    if (!ctx || !tp || !e_vdw_hb || !sol_fn || (tp->dddiel && !r_epsilon_fn)) return invalid("null argument");
+    const int nT = tp->n_rec_types, nAM = tp->n_atom_maps;
+    if (nT < 0 || nT > AG_MAX_REC_TYPES || nAM < 0 || nAM > AG_MAX_MAPS) return invalid("table sizes out of range");
+    if (nT * nAM > 0 && (!tp->cA || !tp->cB || !tp->Rij || !tp->epsij || !tp->xA || !tp->xB || !tp->map_is_covalent))
+        return invalid("null parameter array");
+    AGB_CK(cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    BufferSet &B = ctx->table_bufs;
+    const size_t np = (size_t)std::max(1, nT * nAM), nv = np * AG_NEINT;
+    TableArgs a{};
+    a.n_rec_types = nT;
+    a.n_atom_maps = nAM;
+    a.i_smooth = (int)(tp->r_smooth * AG_A_DIV / 2.);  // main.cpp:2190
+    a.coeff_desolv = tp->coeff_desolv;
+    const size_t npar = (size_t)nT * nAM;
+    double *dcA, *dcB, *dR, *dE;
+    int *dxA, *dxB, *dcov, *dbad;
+    AGB_CK(upload(&B, "cA", tp->cA, npar, &dcA, s, nullptr));
+    AGB_CK(upload(&B, "cB", tp->cB, npar, &dcB, s, nullptr));
+    AGB_CK(upload(&B, "Rij", tp->Rij, npar, &dR, s, nullptr));
+    AGB_CK(upload(&B, "epsij", tp->epsij, npar, &dE, s, nullptr));
+    AGB_CK(upload(&B, "xA", tp->xA, npar, &dxA, s, nullptr));
+    AGB_CK(upload(&B, "xB", tp->xB, npar, &dxB, s, nullptr));
+    AGB_CK(upload(&B, "cov", tp->map_is_covalent, (size_t)nAM, &dcov, s, nullptr));
+    a.cA = dcA; a.cB = dcB; a.Rij = dR; a.epsij = dE; a.xA = dxA; a.xB = dxB; a.map_is_covalent = dcov;
+    void *v;
+    AGB_CK(B.ensure("bad", sizeof(int), &v)); dbad = (int *)v;
+    AGB_CK(B.ensure("raw", nv * sizeof(float), &v)); float *raw = (float *)v;
+    AGB_CK(B.ensure("vdw", nv * sizeof(float), &v)); float *vdw = (float *)v;
+    AGB_CK(B.ensure("sol", AG_NDIEL * sizeof(double), &v)); double *sol = (double *)v;
+    AGB_CK(B.ensure("eps", AG_NDIEL * sizeof(double), &v)); double *eps = (double *)v;
+    AGB_CK(cudaMemsetAsync(dbad, 0, sizeof(int), s));
+    AGB_CK(cudaEventRecord(ctx->tev[0], s));
+    AGB_CK(launch_tables_build(a, raw, vdw, sol, tp->dddiel ? eps : nullptr, dbad, s));
+    AGB_CK(cudaEventRecord(ctx->tev[1], s));
+    int bad = 0;
+    AGB_CK(cudaMemcpyAsync(&bad, dbad, sizeof(int), cudaMemcpyDeviceToHost, s));
+    AGB_CK(cudaStreamSynchronize(s));
+    if (bad) {
+        set_last_error("Van der Waals coefficient is not a number, or an exponent is 0.  AutoGrid must exit.");
+        return AG_ERR_FATAL_INPUT;
+    }
+    if (npar) AGB_CK(cudaMemcpyAsync(e_vdw_hb, vdw, npar * AG_NEINT * sizeof(float), cudaMemcpyDefault, s));
+    AGB_CK(cudaMemcpyAsync(sol_fn, sol, AG_NDIEL * sizeof(double), cudaMemcpyDefault, s));
+    if (tp->dddiel) AGB_CK(cudaMemcpyAsync(r_epsilon_fn, eps, AG_NDIEL * sizeof(double), cudaMemcpyDefault, s));
+    AGB_CK(cudaStreamSynchronize(s));
+    float ms = 0.f;
+    AGB_CK(cudaEventElapsedTime(&ms, ctx->tev[0], ctx->tev[1]));
+    ctx->stats.table_ms = ms;
     return AG_OK;
 }
 

@@ -242,6 +242,31 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
     const int nAM = p->n_atom_maps;
     ag_status st = validate_problem(&pv);
     if (st != AG_OK && st != AG_ERR_NO_CLOSEST_H) return st;
+    // tables in device memory (ag_tables_build): read them here once; the
+    // interpolation pairs are formed on the host at creation
+    std::vector<float> h_vdw;
+    std::vector<double> h_sol, h_eps;
+    {
+        cudaPointerAttributes at{};
+        const bool dev = cudaPointerGetAttributes(&at, p->e_vdw_hb) == cudaSuccess && at.type == cudaMemoryTypeDevice;
+        cudaGetLastError();
+        if (dev) {
+            DF_CK(cudaSetDevice(context_device(ctx)));
+            h_vdw.resize((size_t)std::max(p->n_rec_types, 1) * std::max(nAM, 1) * AG_NEINT);
+            h_sol.resize(AG_NDIEL);
+            DF_CK(cudaMemcpy(h_vdw.data(), p->e_vdw_hb, (size_t)p->n_rec_types * nAM * AG_NEINT * sizeof(float),
+                             cudaMemcpyDeviceToHost));
+            DF_CK(cudaMemcpy(h_sol.data(), p->sol_fn, AG_NDIEL * sizeof(double), cudaMemcpyDeviceToHost));
+            pv.e_vdw_hb = h_vdw.data();
+            pv.sol_fn = h_sol.data();
+            if (p->dddiel) {
+                h_eps.resize(AG_NDIEL);
+                DF_CK(cudaMemcpy(h_eps.data(), p->r_epsilon_fn, AG_NDIEL * sizeof(double), cudaMemcpyDeviceToHost));
+                pv.r_epsilon_fn = h_eps.data();
+            }
+            p = &pv;
+        }
+    }
     // Slots: every map but the e map.  The atom term of map m and the
     // desolvation target follow the reference's map loop (main.cpp:3286-3390):
     // a covalent map is skipped whole; with separate desolvation maps the

@@ -190,6 +190,9 @@ struct Job {
     std::vector<int> nbonds;
     std::vector<std::array<int, kMaxNBonds>> bonded;
     std::vector<BondRec> bondrec;
+    // ag_job_table_params: [map][type] parameter arrays
+    std::vector<double> tp_cA, tp_cB, tp_R, tp_eps;
+    std::vector<int32_t> tp_xA, tp_xB, tp_cov;
     std::vector<std::string> receptor_types;  // by rec index
     int receptor_types_ct = 0, receptor_types_gpf_ct = 0;
     bool has_receptor_types_in_gpf = false;
@@ -1459,6 +1462,33 @@ ag_status ag_job_bond_vectors_backward(const ag_job *job, const double *coord, c
         return AG_ERR_INVALID;
     }
     job->job.bond_vectors_backward(coord ? coord : job->job.coord.data(), g_rvector, g_rvector2, g_coord);
+    return AG_OK;
+}
+
+ag_status ag_job_table_params(const ag_job *job, ag_table_params *out)
+{
+    if (!job || !out) { agb::set_last_error("ag_job_table_params: null argument"); return AG_ERR_INVALID; }
+    Job &j = const_cast<ag_job *>(job)->job;
+    const int nT = j.receptor_types_ct, nAM = j.num_atom_maps;
+    const size_t n = (size_t)std::max(0, nT) * std::max(0, nAM);
+    j.tp_cA.assign(n, 0.); j.tp_cB.assign(n, 0.); j.tp_R.assign(n, 0.); j.tp_eps.assign(n, 0.);
+    j.tp_xA.assign(n, 0); j.tp_xB.assign(n, 0); j.tp_cov.assign((size_t)std::max(nAM, 0), 0);
+    for (int m = 0; m < nAM; m++) {
+        const auto &g = j.gridmap[m];
+        j.tp_cov[m] = g.is_covalent;
+        for (int t = 0; t < nT; t++) {
+            const size_t k = (size_t)m * nT + t;
+            j.tp_cA[k] = g.cA[t]; j.tp_cB[k] = g.cB[t]; j.tp_R[k] = g.nbp_r[t]; j.tp_eps[k] = g.nbp_eps[t];
+            j.tp_xA[k] = g.xA[t]; j.tp_xB[k] = g.xB[t];
+        }
+    }
+    out->n_rec_types = nT;
+    out->n_atom_maps = nAM;
+    out->cA = j.tp_cA.data(); out->cB = j.tp_cB.data(); out->Rij = j.tp_R.data(); out->epsij = j.tp_eps.data();
+    out->xA = j.tp_xA.data(); out->xB = j.tp_xB.data(); out->map_is_covalent = j.tp_cov.data();
+    out->r_smooth = j.r_smooth;
+    out->coeff_desolv = j.ad4.coeff_desolv;
+    out->dddiel = j.dddiel ? 1 : 0;
     return AG_OK;
 }
 

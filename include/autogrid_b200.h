@@ -154,6 +154,7 @@ typedef struct ag_stats {
     double  text_ms;           /* device time of the last ag_maps_format's
                                   kernels (measure, scan and write passes)      */
     int64_t text_bytes;        /* bytes of map text that call produced          */
+    double  table_ms;          /* device time of the last ag_tables_build        */
 } ag_stats;
 
 typedef struct ag_context ag_context;
@@ -197,6 +198,35 @@ const float *ag_plan_device_maps(const ag_plan *plan);   /* device pointer  */
 size_t       ag_plan_points(const ag_plan *plan);        /* n1x*n1y*n1z     */
 ag_status    ag_plan_download(ag_plan *plan, float *host_maps);
 ag_status    ag_plan_destroy(ag_plan *plan);
+
+/*
+ * Energy tables on the device: the table fill of main.cpp:2040-2276 (LJ 12-6 /
+ * H-bond 12-10 pair tables with the EINTCLAMP clamp and the +-smooth/2 bin
+ * minimum filter, the desolvation table) and the Mehler-Solmajer dielectric
+ * of main.cpp:1607-1639, from the per-(map, receptor type) parameters the
+ * parameter library and the nbp_r_eps / nbp_coeffs keywords produce
+ * (ag_job_table_params).  Outputs as ag_problem stores the tables:
+ * e_vdw_hb [n_rec_types][n_atom_maps][AG_NEINT], sol_fn and r_epsilon_fn
+ * [AG_NDIEL] (r_epsilon_fn may be NULL with a constant dielectric); host or
+ * device memory.  FP64 arithmetic in the reference's order, CUDA pow/exp.
+ * A problem whose three table pointers are device memory is accepted by
+ * ag_maps_compute*, ag_plan_create and ag_batch_create (packed on the device)
+ * and by ag_diff_create* (read once at creation).  AG_ERR_FATAL_INPUT on a NaN
+ * coefficient or a zero exponent (main.cpp:2166-2183).
+ */
+typedef struct ag_table_params {
+    int32_t        n_rec_types;
+    int32_t        n_atom_maps;
+    const double  *cA, *cB;          /* [n_atom_maps][n_rec_types]; both 0: from Rij, epsij */
+    const double  *Rij, *epsij;      /* [n_atom_maps][n_rec_types]                          */
+    const int32_t *xA, *xB;          /* [n_atom_maps][n_rec_types] exponents                */
+    const int32_t *map_is_covalent;  /* [n_atom_maps]: table left zero                     */
+    double         r_smooth;         /* GPF smooth (Angstrom)                               */
+    double         coeff_desolv;     /* AD4.coeff_desolv                                    */
+    int32_t        dddiel;           /* 1: distance-dependent dielectric                    */
+} ag_table_params;
+ag_status ag_tables_build(ag_context *ctx, const ag_table_params *params, float *e_vdw_hb, double *sol_fn,
+                          double *r_epsilon_fn);
 
 /*
  * Map-file bodies formatted on the device (replaces the text loop of
@@ -395,6 +425,8 @@ void               ag_job_free(ag_job *job);
 enum { AG_BOND_NONE = 0, AG_BOND_D1 = 1, AG_BOND_A2_ONE = 2, AG_BOND_A2_DIS = 3, AG_BOND_A2_TWO = 4,
        AG_BOND_A1 = 5 };
 ag_status          ag_job_bond_topology(const ag_job *job, int32_t *topo);
+/* The job's table parameters for ag_tables_build (arrays owned by the job). */
+ag_status          ag_job_table_params(const ag_job *job, ag_table_params *out);
 /* The job with Vina-potential tables in place of the AD4 ones: the table
  * fill of main.cpp:2081-2126 (compiled out of the reference build,
  * use_vina_potential = FALSE at main.cpp:263) with the xs radii of
