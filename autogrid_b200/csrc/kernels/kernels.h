@@ -23,6 +23,9 @@ struct NearSmem {
     float4 pos[NB_CHUNK_MAX], a[NB_CHUNK_MAX], b[NB_CHUNK_MAX];
     int meta[NB_CHUNK_MAX], idx[NB_CHUNK_MAX];
     int hl[NB_CHUNK_MAX], nh;  // staged DS/D1 candidates (slots in this chunk), any order
+    // per warp: slots of the staged atoms near that warp's points, in staged order
+    unsigned short wl[NB_WARPS_MAX][NB_CHUNK_MAX];
+    float wbox[NB_WARPS_MAX][6];  // per warp: its points' box in frame bins (lo xyz, hi xyz)
     float etab[NT_SMALL], sol[NT_SMALL];
     int seg_start[NB_SEGS_MAX], seg_off[NB_SEGS_MAX + 1];
     int total;

@@ -459,9 +459,54 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     R D1 = 0, D2 = 0, e_near = 0;
     unsigned n_near = 0, n_fb = 0;
     if (need_pairs) {
+        // This warp's points as a box in frame bins (lanes outside the grid do
+        // not count).  Per chunk, the warp keeps the staged atoms whose
+        // distance to the box is within the near radius plus 2 bins, in staged
+        // order: every pair a lane evaluates below (FP32 t < 1024 + GUARD_BIN,
+        // or the FP64 twin's r^2 <= 64.0064) lies inside that margin, so the
+        // pairs and their summation order are those of the full staged list.
+        static_assert(NB_THREADS / 32 <= NB_WARPS_MAX, "per-warp candidate lists");
+        const int lane = tid & 31, wid = tid >> 5;
+        {
+            float blo[3] = {valid ? PX : 3.0e38f, valid ? PY : 3.0e38f, valid ? PZ : 3.0e38f};
+            float bhi[3] = {valid ? PX : -3.0e38f, valid ? PY : -3.0e38f, valid ? PZ : -3.0e38f};
+#pragma unroll
+            for (int d = 0; d < 3; d++)
+#pragma unroll
+                for (int o = 16; o; o >>= 1) {
+                    blo[d] = fminf(blo[d], __shfl_xor_sync(0xffffffffu, blo[d], o));
+                    bhi[d] = fmaxf(bhi[d], __shfl_xor_sync(0xffffffffu, bhi[d], o));
+                }
+            if (lane == 0)
+                for (int d = 0; d < 3; d++) {
+                    S.wbox[wid][d] = blo[d];
+                    S.wbox[wid][3 + d] = bhi[d];
+                }
+            __syncwarp();
+        }
+        const float keep2 = (FAR_T0 + 2.0f) * (FAR_T0 + 2.0f);
+        unsigned short *wl = S.wl[wid];
         for_each_chunk([&](int nc) {
+            int cnt = 0;
+            for (int j0 = 0; j0 < nc; j0 += 32) {
+                const int jj = j0 + lane;
+                bool keep = false;
+                if (jj < nc) {
+                    const float4 A = S.pos[jj];
+                    const float *bx = S.wbox[wid];
+                    const float ex = fmaxf(fmaxf(bx[0] - A.x, A.x - bx[3]), 0.f);
+                    const float ey = fmaxf(fmaxf(bx[1] - A.y, A.y - bx[4]), 0.f);
+                    const float ez = fmaxf(fmaxf(bx[2] - A.z, A.z - bx[5]), 0.f);
+                    keep = ex * ex + ey * ey + ez * ez <= keep2;
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) wl[cnt + __popc(m & ((1u << lane) - 1u))] = (unsigned short)jj;
+                cnt += __popc(m);
+            }
+            __syncwarp();
             if (!valid) return;
-            for (int j = 0; j < nc; j++) {
+            for (int k = 0; k < cnt; k++) {
+                const int j = wl[k];
                 const int ia = S.idx[j];
                 const int meta = S.meta[j];
                 PairQ<R> q;
