@@ -24,11 +24,15 @@ namespace {
 
 constexpr int DF_MAXCELLS = 512;
 
+constexpr int DF_WARPS = DF_THREADS / 32;
+
 template <class R> struct NearLinSmem {
     Atom<R> at[DF_STAGE];
     int ok[DF_MAXCELLS];
     int cells[DF_MAXCELLS], off[DF_MAXCELLS + 1];
     int ncell, total;
+    unsigned short wl[DF_WARPS][DF_STAGE];  // per warp: staged slots near its points
+    R wbox[DF_WARPS][6];                    // per warp: its points' box (lo xyz, hi xyz), A
 };
 
 struct Brick {
@@ -55,6 +59,65 @@ __device__ __forceinline__ Brick brick_of(const DiffArgs &a)
     b.valid = b.ix < a.n1x && b.iy < a.n1y && b.iz < a.n1z;
     b.lin = b.valid ? (long long)b.ix + (long long)a.n1x * (b.iy + (long long)a.n1y * b.iz) : 0;
     return b;
+}
+
+// This warp's points as a box (lanes outside the grid do not count), kept in
+// shared memory for warp_candidates.
+template <class R>
+__device__ __forceinline__ void warp_box(const Brick &bk, R px, R py, R pz, NearLinSmem<R> &sm)
+{
+    const R big = (R)3.0e38f;
+    R lo[3] = {bk.valid ? px : big, bk.valid ? py : big, bk.valid ? pz : big};
+    R hi[3] = {bk.valid ? px : -big, bk.valid ? py : -big, bk.valid ? pz : -big};
+#pragma unroll
+    for (int d = 0; d < 3; d++)
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            const R a = __shfl_xor_sync(0xffffffffu, lo[d], o), b = __shfl_xor_sync(0xffffffffu, hi[d], o);
+            lo[d] = a < lo[d] ? a : lo[d];
+            hi[d] = b > hi[d] ? b : hi[d];
+        }
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0)
+        for (int d = 0; d < 3; d++) {
+            sm.wbox[w][d] = lo[d];
+            sm.wbox[w][3 + d] = hi[d];
+        }
+    __syncwarp();
+}
+
+// Slots j < n of the staged chunk whose atom lies within the cutoff + 0.01 A
+// of this warp's box, in staged order (called by all 32 lanes).  Every pair a
+// lane of the warp evaluates (r^2 <= 64 in geom) is on the list, so the pairs
+// and their order are those of the whole chunk.
+template <class R>
+__device__ __forceinline__ int warp_candidates(NearLinSmem<R> &sm, int n)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const R *bx = sm.wbox[w];
+    const R lim2 = (R)((AG_NBC + 0.01) * (AG_NBC + 0.01));
+    int cnt = 0;
+    for (int j0 = 0; j0 < n; j0 += 32) {
+        const int j = j0 + lane;
+        bool keep = false;
+        if (j < n) {
+            const Atom<R> &at = sm.at[j];
+            R e[3];
+            const R c[3] = {at.x, at.y, at.z};
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const R u = bx[d] - c[d], v = c[d] - bx[3 + d];
+                const R m = u > v ? u : v;
+                e[d] = m > (R)0 ? m : (R)0;
+            }
+            keep = e[0] * e[0] + e[1] * e[1] + e[2] * e[2] <= lim2;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) sm.wl[w][cnt + __popc(m & ((1u << lane) - 1u))] = (unsigned short)j;
+        cnt += __popc(m);
+    }
+    __syncwarp();
+    return cnt;
 }
 
 // Cells whose box lies within DF_RADIUS of the brick's box, in cell order,
@@ -168,14 +231,17 @@ k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ 
     for (int s = 0; s < DF_MAXMM; s++) { hmin[s] = (R)999999.; hmax[s] = (R)-999999.; amin[s] = -1; amax[s] = -1; }
 
     brick_cells(a, v, bk, sm);
+    warp_box(bk, px, py, pz, sm);
     for (int c0 = 0; c0 < sm.total; c0 += DF_STAGE) {
         __syncthreads();
         stage_chunk(a, v, sm, c0);
         __syncthreads();
         const int n = min(DF_STAGE, sm.total - c0);
+        const int cnt = warp_candidates(sm, n);
         if (!bk.valid) continue;
-        for (int j = 0; j < n; j++) {
-            const Atom<R> at = sm.at[j];
+        const unsigned short *wl = sm.wl[threadIdx.x >> 5];
+        for (int k = 0; k < cnt; k++) {
+            const Atom<R> at = sm.at[wl[k]];
             Geom<R> g;
             if (!geom(sol, at, px, py, pz, g)) continue;
             const int hb = (at.meta >> DM_HB_SHIFT) & 7;
@@ -241,13 +307,16 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
     const int lane = threadIdx.x & 31;
 
     brick_cells(a, v, bk, sm);
+    warp_box(bk, px, py, pz, sm);
     for (int c0 = 0; c0 < sm.total; c0 += DF_STAGE) {
         __syncthreads();
         stage_chunk(a, v, sm, c0);
         __syncthreads();
         const int n = min(DF_STAGE, sm.total - c0);
-        for (int j = 0; j < n; j++) {
-            const Atom<R> at = sm.at[j];
+        const int cnt = warp_candidates(sm, n);
+        const unsigned short *wl = sm.wl[threadIdx.x >> 5];
+        for (int k = 0; k < cnt; k++) {
+            const Atom<R> at = sm.at[wl[k]];
             Geom<R> g;
             const bool in = bk.valid && geom(sol, at, px, py, pz, g);
             if (!__any_sync(0xffffffffu, in)) continue;
