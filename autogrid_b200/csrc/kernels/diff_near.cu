@@ -206,11 +206,16 @@ template <class R> __device__ __forceinline__ R covalent_value(const DiffArgs &a
     return (R)a.cov_barrier * ((R)1 - exp_((R)-0.69314718055994531 * rc * rc));
 }
 
-template <class R>
-__global__ void __launch_bounds__(DF_THREADS)
+// MS slots and MM min/max registers per point: the general instantiation
+// holds DF_MAXS / DF_MAXMM; map sets of at most DF_LEAN_S slots without
+// H-bond min/max (Vina maps, plain AD4 subsets) take the lean one, whose
+// registers leave room for 3 resident CTAs per SM.
+template <class R, int MS, int MM, int MINB>
+__global__ void __launch_bounds__(DF_THREADS, MINB)
 k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ sol, R *__restrict__ maps,
            const int *__restrict__ chs, int *__restrict__ mmarg)
 {
+    constexpr int MMA = MM > 0 ? MM : 1;
     __shared__ NearLinSmem<R> sm;
     const Brick bk = brick_of(a);
     const ConfView v = conf_view(a, DiffGrads{}, bk.conf);
@@ -223,12 +228,12 @@ k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ 
     R rvh[3] = {0, 0, 0};
     if (ch >= 0)
         for (int i = 0; i < 3; i++) rvh[i] = (R)v.rv[3 * ch + i];
-    R E[DF_MAXS], hmin[DF_MAXMM], hmax[DF_MAXMM];
-    int amin[DF_MAXMM], amax[DF_MAXMM];
+    R E[MS], hmin[MMA], hmax[MMA];
+    int amin[MMA], amax[MMA];
 #pragma unroll
-    for (int s = 0; s < DF_MAXS; s++) E[s] = 0;
+    for (int s = 0; s < MS; s++) E[s] = 0;
 #pragma unroll
-    for (int s = 0; s < DF_MAXMM; s++) { hmin[s] = (R)999999.; hmax[s] = (R)-999999.; amin[s] = -1; amax[s] = -1; }
+    for (int s = 0; s < MMA; s++) { hmin[s] = (R)999999.; hmax[s] = (R)-999999.; amin[s] = -1; amax[s] = -1; }
 
     brick_cells(a, v, bk, sm);
     warp_box(bk, px, py, pz, sm);
@@ -248,15 +253,15 @@ k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ 
             Ang<R> an;
             angular(hb, (at.meta >> DM_REXP_SHIFT) & 7, (at.meta & DM_DIS) != 0, ch >= 0 && at.idx != ch, g.dn,
                     at.rv, at.rv2, rvh, an);
-            pair_fwd(a, vdw, g, at, an, E, hmin, hmax, amin, amax);
+            pair_fwd<R, MS, MM>(a, vdw, g, at, an, E, hmin, hmax, amin, amax);
         }
     }
     if (!bk.valid) return;
 #pragma unroll
-    for (int s = 0; s < DF_MAXS; s++) {
+    for (int s = 0; s < MS; s++) {
         if (s >= a.n_slots) break;
         R v = E[s];
-        if (s < DF_MAXMM && s < a.n_mm) {
+        if (s < MM && s < a.n_mm) {
             // H-bond finaliser, main.cpp:3420-3431
             if (amin[s] >= 0) v += hmin[s] + (hmax[s] > (R)0 ? hmax[s] : (R)0);
             mmarg[(2LL * s) * a.P + bk.lin] = amin[s];
@@ -274,12 +279,13 @@ template <class R> __device__ __forceinline__ R warp_sum(R v)
     return v;
 }
 
-template <class R>
-__global__ void __launch_bounds__(DF_THREADS)
+template <class R, int MS, int MM, int MINB>
+__global__ void __launch_bounds__(DF_THREADS, MINB)
 k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ sol,
                const R *__restrict__ g_maps, const int *__restrict__ chs, const int *__restrict__ mmarg,
                DiffGrads gr_all)
 {
+    constexpr int MMA = MM > 0 ? MM : 1;
     __shared__ NearLinSmem<R> sm;
     const Brick bk = brick_of(a);
     const ConfView v = conf_view(a, gr_all, bk.conf);
@@ -293,14 +299,14 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
     R rvh[3] = {0, 0, 0}, g_rvh[3] = {0, 0, 0};
     if (ch >= 0)
         for (int i = 0; i < 3; i++) rvh[i] = (R)v.rv[3 * ch + i];
-    R gs[DF_MAXS];
-    int amin[DF_MAXMM], amax[DF_MAXMM];
+    R gs[MS];
+    int amin[MMA], amax[MMA];
 #pragma unroll
-    for (int s = 0; s < DF_MAXS; s++)
+    for (int s = 0; s < MS; s++)
         gs[s] = (bk.valid && s < a.n_slots) ? g_maps[(long long)a.slot_map[s] * a.P + bk.lin] : (R)0;
 #pragma unroll
-    for (int s = 0; s < DF_MAXMM; s++) {
-        const bool has = bk.valid && s < a.n_mm;
+    for (int s = 0; s < MMA; s++) {
+        const bool has = bk.valid && s < MM && s < a.n_mm;
         amin[s] = has ? mmarg[(2LL * s) * a.P + bk.lin] : -1;
         amax[s] = has ? mmarg[(2LL * s + 1) * a.P + bk.lin] : -1;
     }
@@ -328,7 +334,7 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
                 angular(hb, (at.meta >> DM_REXP_SHIFT) & 7, dis, ch >= 0 && at.idx != ch, g.dn, at.rv, at.rv2, rvh,
                         an);
                 R G_x = 0, G_racc = 0, G_rdon = 0, G_H = 0;
-                pair_bwd(a, vdw, g, at, an, gs, amin, amax, G_x, G_racc, G_rdon, G_H, G_q);
+                pair_bwd<R, MS, MM>(a, vdw, g, at, an, gs, amin, amax, G_x, G_racc, G_rdon, G_H, G_q);
                 R g_dn[3] = {0, 0, 0};
                 angular_bwd(hb, dis, an, G_racc, G_rdon, G_H, g.dn, at.rv, at.rv2, rvh, g_dn, g_rv, g_rv2, g_rvh);
                 geom_bwd(g, G_x, g_dn, g_d);
@@ -412,12 +418,16 @@ cudaError_t launch_near_lin(bool fp64, const DiffArgs &a, const void *vdw, const
                             const int *ch, int *mmarg, cudaStream_t s)
 {
     if (a.P == 0 || a.n_slots == 0) return cudaSuccess;
+    const bool lean = a.n_slots <= DF_LEAN_S && a.n_mm == 0;
     if (fp64)
-        k_near_lin<double><<<brick_grid(a), DF_THREADS, 0, s>>>(a, (const R2<double> *)vdw, (const R2<double> *)sol,
-                                                               (double *)maps, ch, mmarg);
+        k_near_lin<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<double> *)vdw, (const R2<double> *)sol, (double *)maps, ch, mmarg);
+    else if (lean)
+        k_near_lin<float, DF_LEAN_S, 0, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (float *)maps, ch, mmarg);
     else
-        k_near_lin<float><<<brick_grid(a), DF_THREADS, 0, s>>>(a, (const R2<float> *)vdw, (const R2<float> *)sol,
-                                                              (float *)maps, ch, mmarg);
+        k_near_lin<float, DF_MAXS, DF_MAXMM, 2><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (float *)maps, ch, mmarg);
     return cudaGetLastError();
 }
 
@@ -425,12 +435,16 @@ cudaError_t launch_near_lin_adj(bool fp64, const DiffArgs &a, const void *vdw, c
                                 const int *ch, const int *mmarg, DiffGrads g, cudaStream_t s)
 {
     if (a.P == 0 || a.n_slots == 0) return cudaSuccess;
+    const bool lean = a.n_slots <= DF_LEAN_S && a.n_mm == 0;
     if (fp64)
-        k_near_lin_adj<double><<<brick_grid(a), DF_THREADS, 0, s>>>(
+        k_near_lin_adj<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<double> *)vdw, (const R2<double> *)sol, (const double *)g_maps, ch, mmarg, g);
+    else if (lean)
+        k_near_lin_adj<float, DF_LEAN_S, 0, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (const float *)g_maps, ch, mmarg, g);
     else
-        k_near_lin_adj<float><<<brick_grid(a), DF_THREADS, 0, s>>>(a, (const R2<float> *)vdw, (const R2<float> *)sol,
-                                                                  (const float *)g_maps, ch, mmarg, g);
+        k_near_lin_adj<float, DF_MAXS, DF_MAXMM, 2><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (const float *)g_maps, ch, mmarg, g);
     return cudaGetLastError();
 }
 

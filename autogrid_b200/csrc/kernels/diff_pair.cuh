@@ -295,16 +295,18 @@ DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, int type, int s, c
 DF_HD bool act_is_mm(int act) { return act == DA_MMA || act == DA_MMD; }
 
 // Forward: add one pair to the point's slot energies and min/max registers.
-template <class R>
+// MS, MM: the slots and min/max registers a kernel instantiation holds
+// (at least a.n_slots and a.n_mm).
+template <class R, int MS = DF_MAXS, int MM = DF_MAXMM>
 DF_HD void pair_fwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const Atom<R> &at, const Ang<R> &an,
-                    R E[DF_MAXS], R hmin[DF_MAXMM], R hmax[DF_MAXMM], int amin[DF_MAXMM], int amax[DF_MAXMM])
+                    R *E, R *hmin, R *hmax, int *amin, int *amax)
 {
     const int type = at.meta & DM_TYPE_MASK, hb = (at.meta >> DM_HB_SHIFT) & 7;
     const int cls = hb + ((at.meta & DM_DIS) ? 8 : 0);
     const R qasp = R(a.solpar_q);
     const R solv = at.solpar + qasp * ab(at.q);
 #pragma unroll
-    for (int s = 0; s < DF_MAXS; s++) {
+    for (int s = 0; s < MS; s++) {
         if (s >= a.n_slots) break;
         const int kind = a.slot_kind[s];
         if (kind == DK_D) {  // main.cpp:3393-3404
@@ -319,7 +321,7 @@ DF_HD void pair_fwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
                 term(a, vdw, act, type, s, g, an, t);
                 const R val = g.w * t.v;
                 if (act_is_mm(act)) {
-                    if (s < DF_MAXMM) {  // min/max slots come first
+                    if (s < MM) {  // min/max slots come first
                         if (val <= hmin[s]) { hmin[s] = val; amin[s] = at.idx; }
                         if (val >= hmax[s]) { hmax[s] = val; amax[s] = at.idx; }
                     }
@@ -337,10 +339,9 @@ DF_HD void pair_fwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
 // slots; amin/amax: the atoms that attain the point's min/max (amax < 0 when
 // max(hmax, 0) = 0).  Returns d L / d x (x = A_DIV r), d L / d (racc, rdon,
 // Hramp) and d L / d q.
-template <class R>
+template <class R, int MS = DF_MAXS, int MM = DF_MAXMM>
 DF_HD void pair_bwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const Atom<R> &at, const Ang<R> &an,
-                    const R gs[DF_MAXS], const int amin[DF_MAXMM], const int amax[DF_MAXMM], R &G_x, R &G_racc,
-                    R &G_rdon, R &G_H, R &G_q)
+                    const R *gs, const int *amin, const int *amax, R &G_x, R &G_racc, R &G_rdon, R &G_H, R &G_q)
 {
     const int type = at.meta & DM_TYPE_MASK, hb = (at.meta >> DM_HB_SHIFT) & 7;
     const int cls = hb + ((at.meta & DM_DIS) ? 8 : 0);
@@ -349,7 +350,7 @@ DF_HD void pair_bwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
     const R sgnq = at.q > R(0) ? R(1) : (at.q < R(0) ? R(-1) : R(0));
     const R dsol_x = g.dw * g.sol + g.w * g.dsol;  // d (w sol) / d x
 #pragma unroll
-    for (int s = 0; s < DF_MAXS; s++) {
+    for (int s = 0; s < MS; s++) {
         if (s >= a.n_slots) break;
         const int kind = a.slot_kind[s];
         const R gsl = gs[s];
@@ -364,7 +365,7 @@ DF_HD void pair_bwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
                 R gv = gsl;
                 if (act_is_mm(act)) {
                     gv = R(0);
-                    if (s < DF_MAXMM) {
+                    if (s < MM) {
                         if (amin[s] == at.idx) gv += gsl;
                         if (amax[s] == at.idx) gv += gsl;
                     }
