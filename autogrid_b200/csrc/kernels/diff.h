@@ -29,7 +29,8 @@ namespace agb {
 
 constexpr int DF_MAXS = 16;   // map slots of the short-range kernels (atom maps, desolvation partners, d)
 constexpr int DF_MAXMM = 8;   // slots that keep an H-bond min/max
-constexpr int DF_LEAN_S = 8;  // slots of the lean kernel instantiation (no min/max)
+constexpr int DF_LEAN_S = 8;  // slots of the lean kernel instantiations
+constexpr int DF_MID_MM = 2;  // min/max registers of the middle one (the lean one has none)
 constexpr int DF_BRICK_X = 8, DF_BRICK_Y = 8, DF_BRICK_Z = 4;
 constexpr int DF_THREADS = DF_BRICK_X * DF_BRICK_Y * DF_BRICK_Z;
 constexpr int DF_STAGE = 256;       // candidate atoms staged in shared memory at once

@@ -419,9 +419,13 @@ cudaError_t launch_near_lin(bool fp64, const DiffArgs &a, const void *vdw, const
 {
     if (a.P == 0 || a.n_slots == 0) return cudaSuccess;
     const bool lean = a.n_slots <= DF_LEAN_S && a.n_mm == 0;
+    const bool mid = a.n_slots <= DF_LEAN_S && a.n_mm <= DF_MID_MM;
     if (fp64)
         k_near_lin<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<double> *)vdw, (const R2<double> *)sol, (double *)maps, ch, mmarg);
+    else if (mid && !lean)
+        k_near_lin<float, DF_LEAN_S, DF_MID_MM, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (float *)maps, ch, mmarg);
     else if (lean)
         k_near_lin<float, DF_LEAN_S, 0, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<float> *)vdw, (const R2<float> *)sol, (float *)maps, ch, mmarg);
@@ -436,9 +440,13 @@ cudaError_t launch_near_lin_adj(bool fp64, const DiffArgs &a, const void *vdw, c
 {
     if (a.P == 0 || a.n_slots == 0) return cudaSuccess;
     const bool lean = a.n_slots <= DF_LEAN_S && a.n_mm == 0;
+    const bool mid = a.n_slots <= DF_LEAN_S && a.n_mm <= DF_MID_MM;
     if (fp64)
         k_near_lin_adj<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<double> *)vdw, (const R2<double> *)sol, (const double *)g_maps, ch, mmarg, g);
+    else if (mid && !lean)
+        k_near_lin_adj<float, DF_LEAN_S, DF_MID_MM, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (const float *)g_maps, ch, mmarg, g);
     else if (lean)
         k_near_lin_adj<float, DF_LEAN_S, 0, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<float> *)vdw, (const R2<float> *)sol, (const float *)g_maps, ch, mmarg, g);
