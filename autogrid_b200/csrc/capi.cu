@@ -231,6 +231,19 @@ namespace agb {
 ag_status validate_problem(const ag_problem *p) { return validate(p); }
 cudaStream_t context_stream(const ag_context *c) { return c->stream; }
 int context_device(const ag_context *c) { return c->device; }
+// True when kernels on `device` may dereference ptr: device memory of that
+// GPU or managed memory.  Entry points that hand a caller's pointer to a
+// kernel check it first, so a host pointer is an argument error, not a fault.
+bool device_accessible(const void *ptr, int device)
+{
+    if (!ptr) return false;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeManaged || (at.type == cudaMemoryTypeDevice && at.device == device);
+}
 }  // namespace agb
 
 namespace {
@@ -1125,6 +1138,7 @@ static ag_status format_maps(ag_context *c, const ag_problem *p, const void *dma
 {
     if (!c || !p || !dmaps || !text || !map_bytes) return invalid("null argument");
     if (elem != 4 && elem != 8) return invalid("elem_size must be 4 (FP32 maps) or 8 (FP64 maps)");
+    if (!device_accessible(dmaps, c->device)) return invalid("ag_maps_format: the maps must be device memory of the context's GPU");
     ag_status st = validate(p);
     if (st != AG_OK) return st;
     AGB_CK(cudaSetDevice(c->device));

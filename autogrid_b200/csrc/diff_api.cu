@@ -17,6 +17,7 @@ void set_last_error(const std::string &m);
 ag_status validate_problem(const ag_problem *p);
 cudaStream_t context_stream(const ag_context *c);
 int context_device(const ag_context *c);
+bool device_accessible(const void *ptr, int device);
 }  // namespace agb
 
 using namespace agb;
@@ -466,6 +467,10 @@ ag_status ag_diff_set_atoms(ag_diff *d, const double *coord, const double *charg
 ag_status ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out)
 {
     if (!d) { set_last_error("ag_diff_forward: null argument"); return AG_ERR_INVALID; }
+    if (device_out && !device_accessible(device_out, d->device)) {
+        set_last_error("ag_diff_forward: device_out must be device memory of the object's GPU");
+        return AG_ERR_INVALID;
+    }
     DF_CK(cudaSetDevice(d->device));
     cudaStream_t s = d->stream;
     unsigned char *out = device_out ? (unsigned char *)device_out : (unsigned char *)d->d_maps;
@@ -527,6 +532,10 @@ ag_status ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_de
 {
     if (!d || !grad_maps) { set_last_error("ag_diff_backward: null argument"); return AG_ERR_INVALID; }
     if (!d->have_fwd) { set_last_error("ag_diff_backward: no forward to differentiate"); return AG_ERR_INVALID; }
+    if (grad_on_device && !device_accessible(grad_maps, d->device)) {
+        set_last_error("ag_diff_backward: grad_maps is not device memory of the object's GPU");
+        return AG_ERR_INVALID;
+    }
     DF_CK(cudaSetDevice(d->device));
     cudaStream_t s = d->stream;
     const size_t N = d->N, K = d->n_conf;
@@ -593,6 +602,10 @@ ag_status ag_diff_set_bonds(ag_diff *d, const int32_t *topo)
 ag_status ag_diff_set_atoms_device(ag_diff *d, const double *coord, const double *charge)
 {
     if (!d || !coord) { set_last_error("ag_diff_set_atoms_device: null argument"); return AG_ERR_INVALID; }
+    if (!device_accessible(coord, d->device) || (charge && !device_accessible(charge, d->device))) {
+        set_last_error("ag_diff_set_atoms_device: coord and charge must be device memory of the object's GPU");
+        return AG_ERR_INVALID;
+    }
     DF_CK(cudaSetDevice(d->device));
     cudaStream_t s = d->stream;
     const int N = d->N, K = d->n_conf;
@@ -621,6 +634,10 @@ ag_status ag_diff_set_atoms_device(ag_diff *d, const double *coord, const double
 ag_status ag_diff_backward_device(ag_diff *d, const void *grad_maps, double *g_coord, double *g_charge)
 {
     if (!d || !grad_maps) { set_last_error("ag_diff_backward_device: null argument"); return AG_ERR_INVALID; }
+    if ((g_coord && !device_accessible(g_coord, d->device)) || (g_charge && !device_accessible(g_charge, d->device))) {
+        set_last_error("ag_diff_backward_device: g_coord and g_charge must be device memory of the object's GPU");
+        return AG_ERR_INVALID;
+    }
     ag_status st = ag_diff_backward(d, grad_maps, 1, nullptr, nullptr, nullptr, nullptr);
     if (st != AG_OK) return st;
     cudaStream_t s = d->stream;

@@ -26,6 +26,7 @@
 
 namespace agb {
 void set_last_error(const std::string &m);
+bool device_accessible(const void *ptr, int device);
 
 // 32 MiB, held by every GPU that loads the library until the process exits.
 constexpr size_t NOALLOC_SCRATCH_BYTES = size_t(32) << 20;
@@ -202,6 +203,12 @@ extern "C" ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, co
                        std::to_string(n_atoms) + " atoms exceeds the 32 MiB no-allocation scratch (about " +
                        std::to_string((NOALLOC_SCRATCH_BYTES - fixed) / sizeof(float)) + " points)");
         return AG_ERR_TOO_LARGE;
+    }
+    if (!device_accessible(d_emap, device) || (n_atoms > 0 && (!device_accessible(d_coord, device) ||
+                                                              !device_accessible(d_charge, device))) ||
+        (dddiel && !device_accessible(d_r_epsilon_fn, device))) {
+        set_last_error("ag_emap_compute_noalloc: the buffers must be device memory of the given GPU");
+        return AG_ERR_INVALID;
     }
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
