@@ -157,6 +157,8 @@ struct ag_plan {
     int mpad = 4, n_chunks = 0, chunk_atoms = 0;
     bool any_cov = false;
     int floating = 0, constriction = 0;  // distance maps after the n_maps energy maps
+    int far_mode = FAR_TAB_TABLE;        // how k_emap_far obtains far table values (FarArgs::tab_mode)
+    float far_const = 0.f;
     double constriction_cutoff = 7.5;
     float *maps32 = nullptr;
     double *maps64 = nullptr;
@@ -457,6 +459,11 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
             etab[k] = (float)(f * p->coeff_estat);
             solf[k] = (float)p->sol_fn[k];
         }
+        // a constant dielectric needs no far-field table gather
+        if (!p->dddiel) {
+            pl->far_mode = FAR_TAB_CONST;
+            pl->far_const = (float)p->invdielcal;
+        }
     }
 
     // far-field chunking: enough CTAs for ~8 waves per launch; a slab-pipelined
@@ -601,6 +608,8 @@ FarArgs far_args(const ag_plan *pl)
     a.n_atoms = d.n_atoms; a.chunk_atoms = pl->chunk_atoms;
     a.n1x = d.n1x; a.n1y = d.n1y; a.n1z = d.n1z; a.nex = d.nex; a.ney = d.ney; a.nez = d.nez;
     a.nfx = frames_x(d.n1x); a.nfy = frames_y(d.n1y); a.nfz = frames_z(d.n1z);
+    a.tab_mode = pl->far_mode;
+    a.tab_const = pl->far_const;
     return a;
 }
 

@@ -77,7 +77,13 @@ struct FarArgs {
     int n_atoms, chunk_atoms;
     int n1x, n1y, n1z, nex, ney, nez, nfx, nfy, nfz;
     int frame0;                           // single-instance launches: first frame of the launch
+    // How a pair's table value T[b] (b = floor(t) >= AG_NEINT) is obtained:
+    //   FAR_TAB_TABLE  shared-memory gather from far_tab, every pair;
+    //   FAR_TAB_CONST  far_tab is one constant (constant dielectric): no gather.
+    int tab_mode;
+    float tab_const;
 };
+enum { FAR_TAB_TABLE = 0, FAR_TAB_CONST = 2 };
 
 // Device image of one problem instance.
 struct DevProblem {

@@ -41,7 +41,7 @@ __device__ __forceinline__ void load_far_table(float4 *s_tab4, const float *far_
 // One work unit: frame `f` of one instance against atom chunk `chunk`.
 // The caller has loaded the instance's table into s_tab4 and synchronised.
 // Atom tile entries: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
-template <int TILE>
+template <int TILE, int MODE>
 __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
 {
     const int tid = threadIdx.x;
@@ -114,8 +114,14 @@ __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, con
                 float2 t = __fmul2_rn(t2, rs);
                 t = make_float2(fminf(t.x, tmax.x), fminf(t.y, tmax.y));
                 const float2 mg = __fadd2_rz(t, magic);
-                const float T0 = lds_f32(tab_base + (__float_as_uint(mg.x) << 2));
-                const float T1 = lds_f32(tab_base + (__float_as_uint(mg.y) << 2));
+                float T0, T1;
+                if (MODE == FAR_TAB_CONST) {
+                    T0 = t.x < (float)AG_NEINT ? 0.f : a.tab_const;
+                    T1 = t.y < (float)AG_NEINT ? 0.f : a.tab_const;
+                } else {
+                    T0 = lds_f32(tab_base + (__float_as_uint(mg.x) << 2));
+                    T1 = lds_f32(tab_base + (__float_as_uint(mg.y) << 2));
+                }
                 const float2 wv = __fmul2_rn(q2, rs);
                 acc[j] = __ffma2_rn(wv, make_float2(T0, T1), acc[j]);
             }
@@ -143,8 +149,10 @@ __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
     extern __shared__ float4 ef_smem[];
     float4 *s_tab4 = ef_smem;                 // AG_NDIEL floats
     float4 *s_atom = ef_smem + AG_NDIEL / 4;  // TILE entries
-    load_far_table(s_tab4, a.far_tab);
-    far_unit<TILE>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
+    if (a.tab_mode != FAR_TAB_CONST) load_far_table(s_tab4, a.far_tab);
+    __syncthreads();
+    if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
+    else far_unit<TILE, FAR_TAB_TABLE>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
 }
 
 // Many instances, persistent: each CTA takes (instance, frame, chunk) units
@@ -177,12 +185,14 @@ k_emap_far_batch(const FarArgs *__restrict__ insts, const long long *__restrict_
             __syncthreads();
             if (threadIdx.x == 0) s_a = insts[lo];
             __syncthreads();
-            load_far_table(s_tab4, s_a.far_tab);
+            if (s_a.tab_mode != FAR_TAB_CONST) load_far_table(s_tab4, s_a.far_tab);
             cur = lo;
         }
         const long long lu = u - unit_begin[lo];
         const int frames = s_a.nfx * s_a.nfy * s_a.nfz;
-        far_unit<TILE>(s_a, (int)(lu % frames), (int)(lu / frames), s_tab4, s_atom);
+        const int fr = (int)(lu % frames), ch = (int)(lu / frames);
+        if (s_a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST>(s_a, fr, ch, s_tab4, s_atom);
+        else far_unit<TILE, FAR_TAB_TABLE>(s_a, fr, ch, s_tab4, s_atom);
     }
 }
 
