@@ -24,7 +24,8 @@
 namespace agb {
 
 constexpr int EF_THREADS = 256;
-constexpr int EF_PAIRS = 4;       // float2 pairs of points per thread (8 points)
+// float2 pairs of points per thread: 4 (8 points, frames 32 wide) or 2 (4
+// points, frames 16 wide, for grids that 32-wide frames would pad more)
 
 __device__ __forceinline__ float lds_f32(uint32_t addr)
 {
@@ -41,12 +42,12 @@ __device__ __forceinline__ void load_far_table(float4 *s_tab4, const float *far_
 // One work unit: frame `f` of one instance against atom chunk `chunk`.
 // The caller has loaded the instance's table into s_tab4 and synchronised.
 // Atom tile entries: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
-template <int TILE, int MODE>
+template <int TILE, int MODE, int EF_PAIRS>
 __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
 {
     const int tid = threadIdx.x;
     const int fx = f % a.nfx, fy = (f / a.nfx) % a.nfy, fz = f / (a.nfx * a.nfy);
-    const int ox = fx * FRAME_X, oy = fy * FRAME_Y, oz = fz * FRAME_Z;
+    const int ox = fx * (8 * EF_PAIRS), oy = fy * FRAME_Y, oz = fz * FRAME_Z;
     // frame origin in bins, exactly (ox-nex)*spacing*A_DIV as the reference forms c (main.cpp:2859)
     const double X0 = frame_origin_bins(ox, a.nex, a.spacing_adiv);
     const double Y0 = frame_origin_bins(oy, a.ney, a.spacing_adiv);
@@ -143,6 +144,19 @@ __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, con
 }
 
 // Single instance: one CTA per (frame, chunk) = (blockIdx.x, blockIdx.y).
+// The instantiation for the unit's table mode and frame width.
+template <int TILE>
+__device__ __forceinline__ void far_dispatch(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
+{
+    if (a.frame_x == 16) {
+        if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST, 2>(a, f, chunk, s_tab4, s_atom);
+        else far_unit<TILE, FAR_TAB_TABLE, 2>(a, f, chunk, s_tab4, s_atom);
+    } else {
+        if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST, 4>(a, f, chunk, s_tab4, s_atom);
+        else far_unit<TILE, FAR_TAB_TABLE, 4>(a, f, chunk, s_tab4, s_atom);
+    }
+}
+
 template <int TILE>
 __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
 {
@@ -151,8 +165,7 @@ __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
     float4 *s_atom = ef_smem + AG_NDIEL / 4;  // TILE entries
     if (a.tab_mode != FAR_TAB_CONST) load_far_table(s_tab4, a.far_tab);
     __syncthreads();
-    if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
-    else far_unit<TILE, FAR_TAB_TABLE>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
+    far_dispatch<TILE>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
 }
 
 // Many instances, persistent: each CTA takes (instance, frame, chunk) units
@@ -191,8 +204,7 @@ k_emap_far_batch(const FarArgs *__restrict__ insts, const long long *__restrict_
         const long long lu = u - unit_begin[lo];
         const int frames = s_a.nfx * s_a.nfy * s_a.nfz;
         const int fr = (int)(lu % frames), ch = (int)(lu / frames);
-        if (s_a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST>(s_a, fr, ch, s_tab4, s_atom);
-        else far_unit<TILE, FAR_TAB_TABLE>(s_a, fr, ch, s_tab4, s_atom);
+        far_dispatch<TILE>(s_a, fr, ch, s_tab4, s_atom);
     }
 }
 
@@ -235,7 +247,15 @@ k_emap_exact(DevProblem p, double *__restrict__ emap)
 
 namespace agb {
 
-int frames_x(int n1x) { return (n1x + FRAME_X - 1) / FRAME_X; }
+int frames_x(int n1x, int frame_x) { return (n1x + frame_x - 1) / frame_x; }
+
+// 16-wide frames where they pad the x axis less than 32-wide ones, counting
+// the 16-wide kernel's extra atom loads (one per 4 points instead of 8) as 5%.
+int choose_frame_x(int n1x)
+{
+    const double c32 = (double)frames_x(n1x, 32) * 32, c16 = (double)frames_x(n1x, 16) * 16 * 1.05;
+    return c16 < c32 ? 16 : 32;
+}
 int frames_y(int n1y) { return (n1y + FRAME_Y - 1) / FRAME_Y; }
 int frames_z(int n1z) { return (n1z + FRAME_Z - 1) / FRAME_Z; }
 

@@ -291,7 +291,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                                           NearSmem &S)
 {
     static_assert(BX * BY * BZ == NB_THREADS, "one thread per brick point");
-    static_assert(FRAME_X % BX == 0 && FRAME_Y % BY == 0 && FRAME_Z % BZ == 0, "bricks tile far frames");
+    static_assert(16 % BX == 0 && FRAME_Y % BY == 0 && FRAME_Z % BZ == 0, "bricks tile far frames (16 or 32 wide)");
     using R = typename std::conditional<EXACT, double, float>::type;
     const int tid = threadIdx.x;
     if (tid < 2) S.cnt[tid] = 0ull;
@@ -308,7 +308,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
 
     // far-kernel frame of this brick and the point's canonical coordinates
     const double sp128 = p.spacing * AG_A_DIV;
-    const int ox = ((bx * BX) / FRAME_X) * FRAME_X, oy = ((by * BY) / FRAME_Y) * FRAME_Y,
+    const int ox = ((bx * BX) / p.frame_x) * p.frame_x, oy = ((by * BY) / FRAME_Y) * FRAME_Y,
               oz = ((bz * BZ) / FRAME_Z) * FRAME_Z;
     const double X0 = frame_origin_bins(ox, p.nex, sp128), Y0 = frame_origin_bins(oy, p.ney, sp128),
                  Z0 = frame_origin_bins(oz, p.nez, sp128);
