@@ -32,18 +32,59 @@ struct DevBuf {
     size_t cap = 0;
 };
 
+// Device blocks that finished arenas give back to their context, so that
+// repeated batches reuse memory instead of calling cudaMalloc/cudaFree (which
+// maps and unmaps pages, and synchronises) every time.  Freed with the
+// context.  Thread-safe.
+struct BlockCache {
+    std::vector<std::pair<void *, size_t>> free;
+    std::mutex mu;
+    ~BlockCache()
+    {
+        for (auto &b : free) cudaFree(b.first);
+    }
+    cudaError_t take(size_t bytes, void **out, size_t *got)
+    {
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            size_t best = free.size();
+            for (size_t i = 0; i < free.size(); i++)
+                if (free[i].second >= bytes && (best == free.size() || free[i].second < free[best].second)) best = i;
+            if (best < free.size()) {
+                *out = free[best].first;
+                *got = free[best].second;
+                free.erase(free.begin() + (long)best);
+                return cudaSuccess;
+            }
+        }
+        *got = bytes;
+        return cudaMalloc(out, bytes);
+    }
+    void give(void *p, size_t bytes)
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        free.emplace_back(p, bytes);
+    }
+};
+
 // Bump allocator over a few large device blocks, released together: the
-// buffers of a batch's instance plans (one cudaMalloc per 256 MiB instead of
-// one per buffer per instance).  Thread-safe.
+// buffers of a batch's instance plans (one block per 256 MiB instead of one
+// cudaMalloc per buffer per instance).  Blocks come from and go back to the
+// context's cache when it has one.  Thread-safe.
 struct Arena {
-    std::vector<void *> blocks;
+    std::vector<std::pair<void *, size_t>> blocks;
+    BlockCache *cache = nullptr;
     char *cur = nullptr;
     size_t left = 0;
     std::mutex mu;
     static constexpr size_t kBlock = size_t(256) << 20, kAlign = 256;
+    explicit Arena(BlockCache *c = nullptr) : cache(c) {}
     ~Arena()
     {
-        for (void *b : blocks) cudaFree(b);
+        for (auto &b : blocks) {
+            if (cache) cache->give(b.first, b.second);
+            else cudaFree(b.first);
+        }
     }
     cudaError_t alloc(size_t bytes, void **out)
     {
@@ -51,10 +92,10 @@ struct Arena {
         std::lock_guard<std::mutex> lock(mu);
         if (bytes > left) {
             void *b = nullptr;
-            const size_t sz = std::max(bytes, kBlock);
-            cudaError_t e = cudaMalloc(&b, sz);
+            size_t sz = std::max(bytes, kBlock);
+            cudaError_t e = cache ? cache->take(sz, &b, &sz) : cudaMalloc(&b, sz);
             if (e != cudaSuccess) return e;
-            blocks.push_back(b);
+            blocks.emplace_back(b, sz);
             cur = (char *)b;
             left = sz;
         }
@@ -135,6 +176,8 @@ struct ag_context {
     ag_stats stats{};
     BufferSet pool;
     unsigned long long *d_counters = nullptr;
+    // device blocks of finished batch arenas, reused by later batches
+    BlockCache blocks;
     // map text (ag_maps_format): device scratch and text, pinned host copy
     BufferSet text_bufs;
     char *h_text = nullptr;
@@ -755,12 +798,13 @@ ag_status settle_stats(ag_context *c)
 ag_status finish_stats(ag_plan *pl) { return settle_stats(pl->ctx); }
 
 ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out,
-                    Arena *arena = nullptr, bool pipelined = false);
+                    Arena *arena = nullptr, bool pipelined = false, cudaStream_t stream = nullptr);
 
 }  // namespace
 
 struct ag_batch {
     ag_context *ctx = nullptr;
+    cudaStream_t stream = nullptr;  // uploads of the batch's set-up (the context's stream unless pipelined)
     std::unique_ptr<Arena> arena;  // declared before the plans: released after them
     std::vector<std::unique_ptr<ag_plan>> plans;
     std::vector<FarArgs> far;         // per instance, in work order
@@ -807,15 +851,15 @@ ag_status batch_upload_far(ag_batch *b, bool chunked)
     }
     if (!b->red.empty()) {
         AGB_CK(cudaMemcpyAsync(b->d_red, b->red.data(), sizeof(ReduceInst) * b->red.size(), cudaMemcpyHostToDevice,
-                               b->ctx->stream));
+                               b->stream));
         AGB_CK(cudaMemcpyAsync(b->d_red_begin, b->red_begin.data(), sizeof(long long) * b->red_begin.size(),
-                               cudaMemcpyHostToDevice, b->ctx->stream));
+                               cudaMemcpyHostToDevice, b->stream));
     }
-    AGB_CK(cudaMemcpyAsync(b->d_far, b->far.data(), sizeof(FarArgs) * b->far.size(), cudaMemcpyHostToDevice, b->ctx->stream));
+    AGB_CK(cudaMemcpyAsync(b->d_far, b->far.data(), sizeof(FarArgs) * b->far.size(), cudaMemcpyHostToDevice, b->stream));
     AGB_CK(cudaMemcpyAsync(b->d_far_begin, b->far_begin.data(), sizeof(long long) * b->far_begin.size(),
-                           cudaMemcpyHostToDevice, b->ctx->stream));
+                           cudaMemcpyHostToDevice, b->stream));
     AGB_CK(cudaMemcpyAsync(b->d_near, b->near.data(), sizeof(NearInst) * b->near.size(), cudaMemcpyHostToDevice,
-                           b->ctx->stream));
+                           b->stream));
     return AG_OK;
 }
 
@@ -856,7 +900,7 @@ ag_status batch_set_near_shape(ag_batch *b, int shape)
     b->near_begin.assign(1, 0);
     for (const NearInst &ni : b->near) b->near_begin.push_back(b->near_begin.back() + near_bricks(ni.p, shape));
     AGB_CK(cudaMemcpyAsync(b->d_near_begin, b->near_begin.data(), sizeof(long long) * b->near_begin.size(),
-                           cudaMemcpyHostToDevice, b->ctx->stream));
+                           cudaMemcpyHostToDevice, b->stream));
     return AG_OK;
 }
 
@@ -925,7 +969,7 @@ ag_status batch_autotune(ag_batch *b)
 }
 
 ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out, Arena *arena,
-                    bool pipelined)
+                    bool pipelined, cudaStream_t stream)
 {
     if (!ctx || !p || !out) return invalid("null argument");
     ag_opts opts{};
@@ -946,7 +990,7 @@ ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool
     } else {
         pl->bufs = &ctx->pool;
     }
-    ag_status st = build_plan(pl.get(), p, ctx->stream, pipelined);
+    ag_status st = build_plan(pl.get(), p, stream ? stream : ctx->stream, pipelined);
     if (st != AG_OK) return st;
     *out = pl.release();
     return AG_OK;
@@ -1305,8 +1349,10 @@ ag_status ag_plan_destroy(ag_plan *plan)
 }
 
 
-ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, int32_t n, const ag_opts *opts,
-                          ag_batch **out)
+// A batch whose set-up uploads go on stream `us` (the caller synchronises
+// nothing else: kernels already running on the context's stream go on).
+static ag_status batch_create(ag_context *ctx, const ag_problem *const *problems, int32_t n, const ag_opts *opts,
+                              cudaStream_t us, ag_batch **out)
 {
     if (!ctx || !problems || !out || n < 1) return invalid("ag_batch_create: bad argument");
     *out = nullptr;
@@ -1316,7 +1362,8 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     AGB_CK(cudaSetDevice(ctx->device));
     std::unique_ptr<ag_batch> b(new ag_batch());
     b->ctx = ctx;
-    b->arena.reset(new Arena());
+    b->stream = us;
+    b->arena.reset(new Arena(&ctx->blocks));
     for (int i = 0; i < n; i++)
         if (problems[i] && (problems[i]->floating_grid || problems[i]->constriction_grid)) {
             set_last_error("ag_batch_create: batches compute the energy maps only (no fmap/cmap)");
@@ -1332,7 +1379,7 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
         if (cudaSetDevice(ctx->device) != cudaSuccess) return;
         for (int i; (i = next.fetch_add(1)) < n;) {
             ag_plan *pl = nullptr;
-            sts[i] = make_plan(ctx, problems[i], &o, true, &pl, b->arena.get());
+            sts[i] = make_plan(ctx, problems[i], &o, true, &pl, b->arena.get(), false, us);
             if (sts[i] != AG_OK) errs[i] = ag_last_error();
             b->plans[i].reset(pl);
         }
@@ -1380,7 +1427,7 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
                 b->near_begin.push_back(b->near_begin.back() + near_bricks(pl->dp, 0));
             }
         if (pl->any_cov) {
-            AGB_CK(launch_covalent(pl->dp, pl->cov, ctx->stream));  // geometry only: computed once
+            AGB_CK(launch_covalent(pl->dp, pl->cov, us));  // geometry only: computed once
         }
     }
     void *v = nullptr;
@@ -1417,7 +1464,7 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     // capture the run as a graph on a private stream
     cudaStream_t cs;
     AGB_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-    AGB_CK(cudaStreamSynchronize(ctx->stream));
+    AGB_CK(cudaStreamSynchronize(us));
     AGB_CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     st = batch_launch(b.get(), cs, b->tune.far_tile, b->tune.near_shape, nullptr, nullptr, nullptr, true);
     cudaGraph_t g = nullptr;
@@ -1429,6 +1476,13 @@ ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, in
     AGB_CK(cudaGraphInstantiate(&b->exec, g, 0));
     *out = b.release();
     return AG_OK;
+}
+
+ag_status ag_batch_create(ag_context *ctx, const ag_problem *const *problems, int32_t n, const ag_opts *opts,
+                          ag_batch **out)
+{
+    if (!ctx) return invalid("ag_batch_create: bad argument");
+    return batch_create(ctx, problems, n, opts, ctx->stream, out);
 }
 
 ag_status ag_batch_run(ag_batch *b, void *stream)
@@ -1475,13 +1529,82 @@ ag_status ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *proble
                                 float *const *maps)
 {
     if (!maps) return invalid("null maps");
-    ag_batch *b = nullptr;
-    ag_status st = ag_batch_create(ctx, problems, n, opts, &b);
+    if (!ctx || !problems || n < 1) return invalid("ag_maps_compute_batch: bad argument");
+    for (int i = 0; i < n; i++)
+        if (!problems[i] || !maps[i]) return invalid("ag_maps_compute_batch: null problem or output");
+    const bool pipelined = n >= 8 && !(opts && opts->autotune);
+    if (!pipelined) {
+        ag_batch *b = nullptr;
+        ag_status st = ag_batch_create(ctx, problems, n, opts, &b);
+        if (st != AG_OK) return st;
+        std::unique_ptr<ag_batch, ag_status (*)(ag_batch *)> guard(b, ag_batch_destroy);
+        st = ag_batch_run(b, nullptr);
+        for (int i = 0; st == AG_OK && i < n; i++) st = ag_batch_download(b, i, maps[i]);
+        return st;
+    }
+    // Groups of instances, each a batch of its own: group g+1's plans are
+    // built on the host (uploads on a stream of their own) while group g's
+    // graph runs on the context's stream, and each group's maps are copied
+    // back on the copy stream as soon as its graph is done.  Groups take the
+    // instances round-robin by decreasing work, so they are of similar size.
+    AGB_CK(cudaSetDevice(ctx->device));
+    for (int i = 0; i < n; i++) {  // before any launch, with the caller's instance numbers
+        const ag_status vs = validate(problems[i]);
+        if (vs != AG_OK) {
+            set_last_error("instance " + std::to_string(i) + ": " + ag_last_error());
+            return vs;
+        }
+        if (problems[i]->floating_grid || problems[i]->constriction_grid) {
+            set_last_error("ag_batch_create: batches compute the energy maps only (no fmap/cmap)");
+            return AG_ERR_UNSUPPORTED;
+        }
+    }
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    auto work = [&](int i) {
+        const ag_problem *p = problems[i];
+        return (double)p->n1[0] * p->n1[1] * p->n1[2] * (double)(p->n_atoms + 64);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+    const int G = 4;
+    std::vector<std::vector<int>> groups(G);
+    for (int k = 0; k < n; k++) groups[k % G].push_back(order[k]);
+    cudaStream_t us = nullptr;
+    AGB_CK(cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking));
+    std::vector<cudaEvent_t> done(G, nullptr);
+    std::vector<ag_batch *> batches(G, nullptr);
+    ag_status st = AG_OK;
+    cudaError_t ce = cudaSuccess;
+    for (int g = 0; g < G && st == AG_OK; g++) {
+        std::vector<const ag_problem *> ps;
+        for (int i : groups[g]) ps.push_back(problems[i]);
+        st = batch_create(ctx, ps.data(), (int)ps.size(), opts, us, &batches[g]);
+        if (st != AG_OK) break;
+        st = ag_batch_run(batches[g], ctx->stream);
+        if (st != AG_OK) break;
+        if ((ce = cudaEventCreateWithFlags(&done[g], cudaEventDisableTiming)) != cudaSuccess ||
+            (ce = cudaEventRecord(done[g], ctx->stream)) != cudaSuccess)
+            break;
+    }
+    // copies after every launch: a copy into pageable memory blocks the host,
+    // which must not hold up the building of later groups
+    for (int g = 0; g < G && st == AG_OK && ce == cudaSuccess; g++) {
+        if ((ce = cudaStreamWaitEvent(ctx->copy, done[g], 0)) != cudaSuccess) break;
+        for (size_t k = 0; k < groups[g].size() && ce == cudaSuccess; k++) {
+            const ag_plan *pl = batches[g]->plans[k].get();
+            ce = cudaMemcpyAsync(maps[groups[g][k]], pl->maps32, (size_t)pl->dp.n_maps * (size_t)pl->dp.P * sizeof(float),
+                                 cudaMemcpyDefault, ctx->copy);
+        }
+    }
+    const cudaError_t se = cudaStreamSynchronize(ctx->copy);
+    for (ag_batch *b : batches) ag_batch_destroy(b);
+    for (cudaEvent_t e : done)
+        if (e) cudaEventDestroy(e);
+    cudaStreamDestroy(us);
     if (st != AG_OK) return st;
-    std::unique_ptr<ag_batch, ag_status (*)(ag_batch *)> guard(b, ag_batch_destroy);
-    st = ag_batch_run(b, nullptr);
-    for (int i = 0; st == AG_OK && i < n; i++) st = ag_batch_download(b, i, maps[i]);
-    return st;
+    if (ce != cudaSuccess) return cuda_fail(ce, "ag_maps_compute_batch");
+    if (se != cudaSuccess) return cuda_fail(se, "cudaStreamSynchronize");
+    return AG_OK;
 }
 
 }  // extern "C"

@@ -304,9 +304,16 @@ ag_status    ag_batch_run(ag_batch *batch, void *stream);
 const float *ag_batch_device_maps(const ag_batch *batch, int32_t i);
 ag_status    ag_batch_download(ag_batch *batch, int32_t i, float *host_maps);
 ag_status    ag_batch_tuning(const ag_batch *batch, ag_tuning *out);
+/* Destroy a batch before its context.  Its device memory goes back to the
+ * context, which reuses it for later batches and frees it in
+ * ag_context_destroy. */
 ag_status    ag_batch_destroy(ag_batch *batch);
 /* One-shot: create, run, download every instance's maps (maps[i] host or
- * device, [n_maps_i][P_i] each), destroy. */
+ * device, [n_maps_i][P_i] each), destroy.  From 8 instances on (without
+ * autotuning) the instances run as 4 groups, each its own batch: a group's
+ * plans are built on the host while the previous group computes, and each
+ * group's maps are copied back while later groups compute.  Results are those
+ * of one batch without autotuning. */
 ag_status    ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *problems, int32_t n,
                                    const ag_opts *opts, float *const *maps);
 

@@ -61,3 +61,26 @@ def test_batch_one_shot_and_errors(tmp_path, gpu_ctx):
     check(lib.ag_maps_compute_batch(gpu_ctx._h, arr, 3, C.byref(ag_opts()), ptrs))
     for p, o in zip(probs, outs):
         assert tolerance_ok(o, gpu_ctx.compute(p)).all()
+
+
+def test_batch_one_shot_pipelined(tmp_path, gpu_ctx):
+    """From 8 instances the one-shot call runs groups of instances as separate
+    batches, building the next group while the previous one computes: the maps
+    equal the single batch's bit for bit (same chunking, same summation order)
+    and the per-box path's within the parity bar; errors name the caller's
+    instance."""
+    from autogrid_b200 import AutoGridError, Batch, Problem, synth
+    from autogrid_b200.api import compute_batch
+    gpfs = synth.write_ensemble(tmp_path, 10, seed=13, atoms_range=(150, 1200), npts_range=(4, 30), workers=1)
+    probs = _load(tmp_path, gpfs)
+    outs = compute_batch(gpu_ctx, probs)
+    b = Batch(gpu_ctx, probs, autotune=False)
+    b.run()
+    for i, p in enumerate(probs):
+        np.testing.assert_array_equal(outs[i], b.download(i))
+        assert tolerance_ok(outs[i], gpu_ctx.compute(p)).all(), f"instance {i}"
+    b.close()
+    bad = Problem(**probs[6].arrays, n1=probs[6].n1, ne=(0, 0, 0), cov_pos=probs[6].cov_pos, **probs[6].scalars)
+    with pytest.raises(AutoGridError) as e:
+        compute_batch(gpu_ctx, probs[:6] + [bad] + probs[7:])
+    assert e.value.status == 1 and "instance 6" in e.value.message
