@@ -157,7 +157,8 @@ __device__ __forceinline__ void far_dispatch(const FarArgs &a, int f, int chunk,
     }
 }
 
-template <int TILE>
+// One instance; the frame width (PAIRS = frame_x / 8) is fixed per launch.
+template <int TILE, int PAIRS>
 __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
 {
     extern __shared__ float4 ef_smem[];
@@ -165,7 +166,8 @@ __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
     float4 *s_atom = ef_smem + AG_NDIEL / 4;  // TILE entries
     if (a.tab_mode != FAR_TAB_CONST) load_far_table(s_tab4, a.far_tab);
     __syncthreads();
-    far_dispatch<TILE>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
+    if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST, PAIRS>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
+    else far_unit<TILE, FAR_TAB_TABLE, PAIRS>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
 }
 
 // Many instances, persistent: each CTA takes (instance, frame, chunk) units
@@ -270,9 +272,15 @@ cudaError_t launch_emap_far(const FarArgs &args, int n_chunks, int tile, cudaStr
     a.frame0 = fz0 * a.nfx * a.nfy;
     dim3 grid((unsigned)(a.nfx * a.nfy * (fz1 - fz0)), (unsigned)n_chunks);
     const size_t smem = far_smem_bytes(tile);
-    if (tile == 256) k_emap_far<256><<<grid, EF_THREADS, smem, s>>>(a);
-    else if (tile == 1024) k_emap_far<1024><<<grid, EF_THREADS, smem, s>>>(a);
-    else k_emap_far<512><<<grid, EF_THREADS, smem, s>>>(a);
+    if (a.frame_x == 16) {
+        if (tile == 256) k_emap_far<256, 2><<<grid, EF_THREADS, smem, s>>>(a);
+        else if (tile == 1024) k_emap_far<1024, 2><<<grid, EF_THREADS, smem, s>>>(a);
+        else k_emap_far<512, 2><<<grid, EF_THREADS, smem, s>>>(a);
+    } else {
+        if (tile == 256) k_emap_far<256, 4><<<grid, EF_THREADS, smem, s>>>(a);
+        else if (tile == 1024) k_emap_far<1024, 4><<<grid, EF_THREADS, smem, s>>>(a);
+        else k_emap_far<512, 4><<<grid, EF_THREADS, smem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
