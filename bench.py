@@ -60,6 +60,20 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(values, world: int, device: str) -> list:
+    """Each value's maximum over the ranks (the job's time is its slowest
+    rank's); every rank gets the result.  One all-reduce, the only collective
+    of the timed run; `device` is where the process group's backend reduces
+    ("cuda" for NCCL, "cpu" for gloo)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def dist_info():
     return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
             int(os.environ.get("LOCAL_RANK", "0")))
@@ -224,10 +238,7 @@ def main():
         e2e_t.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_t))
 
-    t = torch.tensor([ms, e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, e2e_s = float(t[0]), float(t[1])
+    ms, e2e_s = max_over_ranks([ms, e2e_s], world, "cuda")
 
     if rank == 0:
         evals = P * M * world
