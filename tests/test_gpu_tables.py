@@ -64,7 +64,8 @@ def test_device_tables_match_host(path, tmp_path, gpu_ctx):
     job.close()
 
 
-@pytest.mark.parametrize("path", [p for p in GOLDEN if p.stem in ("disorder_sep_cov", "types14_600", "distance_maps")],
+@pytest.mark.parametrize("path", [p for p in GOLDEN if p.stem in ("disorder_sep_cov", "types14_600", "distance_maps",
+                                                                   "constdiel_nbp")],
                          ids=lambda p: p.stem)
 def test_maps_from_device_tables(path, tmp_path, gpu_ctx):
     from autogrid_b200 import Diff
