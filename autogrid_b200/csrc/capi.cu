@@ -158,6 +158,14 @@ ag_status invalid(const std::string &m)
 constexpr int kSlabZ = 16;
 constexpr int kMaxSlabs = 16;
 
+int slab_count(const DevProblem &d) { return std::min(kMaxSlabs, (d.n1z + kSlabZ - 1) / kSlabZ); }
+// z planes [z0, z1) of slab k: kSlabZ planes each, the last one to n1z
+void slab_range(const DevProblem &d, int k, int *z0, int *z1)
+{
+    *z0 = kSlabZ * k;
+    *z1 = k == slab_count(d) - 1 ? d.n1z : *z0 + kSlabZ;
+}
+
 }  // namespace
 
 struct ag_context {
@@ -215,6 +223,7 @@ struct ag_plan {
     int *meta = nullptr;
     size_t h2d_bytes = 0;
     int last_launches = 0;
+    int far_early = 0;  // far-field slabs a one-shot call launched while its plan was still being built
 };
 
 namespace {
@@ -321,6 +330,8 @@ cudaError_t upload(BufferSet *b, const char *name, const T *src, size_t n, T **d
 }
 
 // Build the device image of a problem (host work is O(atoms + tables)).
+ag_status launch_far_slab(ag_plan *pl, cudaStream_t s, int k, int nslab);
+
 ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipelined)
 {
     ag_status st = validate(p);
@@ -344,17 +355,75 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     pl->h2d_bytes = 0;
     size_t *acc = &pl->h2d_bytes;
 
-    // atoms: SoA doubles, x*A_DIV copies for the far kernel, and the near
-    // kernel's staged record: bond vectors + vol, lone-pair normal + desolvation
-    // factor, and packed metadata (type, hbond, rexp, flags)
+    const bool dev_tables = is_device_memory(p->e_vdw_hb);
+    if (dev_tables != is_device_memory(p->sol_fn) || (p->dddiel && dev_tables != is_device_memory(p->r_epsilon_fn)))
+        return invalid("the problem's tables must all be host memory or all device memory");
+
+    // far-field inputs first: atoms as x*A_DIV and weighted charges, the far
+    // table, the chunking and the partial sums.  A slab-pipelined one-shot run
+    // launches its first far-field slab from here, so that the GPU computes
+    // while the rest of the plan is built on the host.
     std::vector<double> x(N), y(N), z(N), x128(N), y128(N), z128(N);
     std::vector<float> qw(N);
-    std::vector<float4> atomA(std::max(N, 1)), atomB(std::max(N, 1));
-    std::vector<int> meta(std::max(N, 1), 0);
     for (int a = 0; a < N; a++) {
         x[a] = p->coord[3 * a]; y[a] = p->coord[3 * a + 1]; z[a] = p->coord[3 * a + 2];
         x128[a] = x[a] * AG_A_DIV; y128[a] = y[a] * AG_A_DIV; z128[a] = z[a] * AG_A_DIV;
         qw[a] = (float)(p->charge[a] * p->coeff_estat * AG_A_DIV);
+    }
+    std::vector<float> far_tab;
+    if (!dev_tables) {
+        far_tab.assign(AG_NDIEL, 0.f);
+        for (int k = AG_NEINT; k < AG_NDIEL; k++) far_tab[k] = (float)(p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal);
+        // a constant dielectric needs no far-field table gather
+        if (!p->dddiel) {
+            pl->far_mode = FAR_TAB_CONST;
+            pl->far_const = (float)p->invdielcal;
+        }
+    }
+    // far-field chunking: enough CTAs for ~8 waves per launch; a slab-pipelined
+    // one-shot run launches one slab of frames at a time, ~3 waves each
+    const long long frames = pipelined ? (long long)frames_x(d.n1x, d.frame_x) * frames_y(d.n1y) * (kSlabZ / FRAME_Z)
+                                       : (long long)frames_x(d.n1x, d.frame_x) * frames_y(d.n1y) * frames_z(d.n1z);
+    const int tile = 512;
+    if (p->elec_map >= 0 && N > 0) {
+        const long long target = pipelined ? 148LL * 3 * 3 : 148LL * 3 * 8;
+        int nch = (int)std::max(1LL, (target + frames - 1) / frames);
+        nch = std::min(nch, (N + tile - 1) / tile);
+        pl->chunk_atoms = ((N + nch - 1) / nch + tile - 1) / tile * tile;
+        pl->n_chunks = (N + pl->chunk_atoms - 1) / pl->chunk_atoms;
+    } else {
+        pl->chunk_atoms = 0;
+        pl->n_chunks = 0;
+    }
+    void *v = nullptr;
+    const size_t P = (size_t)d.P;
+    if (pl->n_chunks > 0 && pl->opts.precision != AG_PREC_FP64) {
+        AGB_CK(B->ensure("far_partial", (size_t)pl->n_chunks * P * sizeof(float), &v));
+        pl->far_partial = (float *)v;
+    } else {
+        pl->far_partial = nullptr;
+    }
+    AGB_CK(upload(B, "x128", x128.data(), N, &pl->x128, s, acc));
+    AGB_CK(upload(B, "y128", y128.data(), N, &pl->y128, s, acc));
+    AGB_CK(upload(B, "z128", z128.data(), N, &pl->z128, s, acc));
+    AGB_CK(upload(B, "qw", qw.data(), N, &pl->qw, s, acc));
+    if (!dev_tables) AGB_CK(upload(B, "far_tab", far_tab.data(), far_tab.size(), &pl->far_tab, s, acc));
+    pl->far_early = 0;
+    if (pipelined && !dev_tables && pl->far_partial && d.elec_map >= 0) {
+        // the run's statistics start here: counters cleared, then ev0, then the fork
+        ag_context *c = pl->ctx;
+        AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+        AGB_CK(cudaEventRecord(c->ev0, s));
+        ag_status st = launch_far_slab(pl, s, 0, slab_count(d));
+        if (st != AG_OK) return st;
+        pl->far_early = 1;
+    }
+
+    // the near kernel's staged atom record: bond vectors + vol, lone-pair
+    // normal + desolvation factor, and packed metadata (type, hbond, rexp, flags)
+    std::vector<float4> atomA(std::max(N, 1)), atomB(std::max(N, 1));
+    std::vector<int> meta(std::max(N, 1), 0);
+    for (int a = 0; a < N; a++) {
         const double *rv = p->rvector + 3 * a, *rv2 = p->rvector2 + 3 * a;
         atomA[a] = make_float4((float)rv[0], (float)rv[1], (float)rv[2], (float)p->vol[a]);
         atomB[a] = make_float4((float)rv2[0], (float)rv2[1], (float)rv2[2],
@@ -478,10 +547,7 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     for (const NearGroup &g : pl->groups)
         for (int k = 0; k < g.ng; k++)
             if (!skip_map[g.out_map[k]]) colmap[g.col0 + k] = g.out_map[k];
-    const bool dev_tables = is_device_memory(p->e_vdw_hb);
-    if (dev_tables != is_device_memory(p->sol_fn) || (p->dddiel && dev_tables != is_device_memory(p->r_epsilon_fn)))
-        return invalid("the problem's tables must all be host memory or all device memory");
-    std::vector<float> vdwT, far_tab, etab, solf;
+    std::vector<float> vdwT, etab, solf;
     std::vector<double> reps;
     if (!dev_tables) {
         vdwT.assign((size_t)nT * AG_NEINT * pl->mpad, 0.f);
@@ -492,38 +558,15 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
                 for (int b = 0; b < AG_NEINT; b++)
                     vdwT[((size_t)t * AG_NEINT + b) * pl->mpad + c] = p->e_vdw_hb[((size_t)t * nAM + m) * AG_NEINT + b];
         }
-        far_tab.assign(AG_NDIEL, 0.f);
         etab.resize(AG_NDIEL);
         solf.resize(AG_NDIEL);
         reps.assign(AG_NDIEL, 0.0);
         for (int k = 0; k < AG_NDIEL; k++) {
             const double f = p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal;
             if (p->dddiel) reps[k] = p->r_epsilon_fn[k];
-            far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
             etab[k] = (float)(f * p->coeff_estat);
             solf[k] = (float)p->sol_fn[k];
         }
-        // a constant dielectric needs no far-field table gather
-        if (!p->dddiel) {
-            pl->far_mode = FAR_TAB_CONST;
-            pl->far_const = (float)p->invdielcal;
-        }
-    }
-
-    // far-field chunking: enough CTAs for ~8 waves per launch; a slab-pipelined
-    // one-shot run launches one slab of frames at a time, ~3 waves each
-    const long long frames = pipelined ? (long long)frames_x(d.n1x, d.frame_x) * frames_y(d.n1y) * (kSlabZ / FRAME_Z)
-                                       : (long long)frames_x(d.n1x, d.frame_x) * frames_y(d.n1y) * frames_z(d.n1z);
-    const int tile = 512;
-    if (p->elec_map >= 0 && N > 0) {
-        const long long target = pipelined ? 148LL * 3 * 3 : 148LL * 3 * 8;
-        int nch = (int)std::max(1LL, (target + frames - 1) / frames);
-        nch = std::min(nch, (N + tile - 1) / tile);
-        pl->chunk_atoms = ((N + nch - 1) / nch + tile - 1) / tile * tile;
-        pl->n_chunks = (N + pl->chunk_atoms - 1) / pl->chunk_atoms;
-    } else {
-        pl->chunk_atoms = 0;
-        pl->n_chunks = 0;
     }
 
     // uploads
@@ -534,9 +577,6 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     AGB_CK(upload(B, "x", x.data(), N, &dx, s, acc));
     AGB_CK(upload(B, "y", y.data(), N, &dy, s, acc));
     AGB_CK(upload(B, "z", z.data(), N, &dz, s, acc));
-    AGB_CK(upload(B, "x128", x128.data(), N, &pl->x128, s, acc));
-    AGB_CK(upload(B, "y128", y128.data(), N, &pl->y128, s, acc));
-    AGB_CK(upload(B, "z128", z128.data(), N, &pl->z128, s, acc));
     AGB_CK(upload(B, "q", p->charge, N, &dq, s, acc));
     AGB_CK(upload(B, "vol", p->vol, N, &dvol, s, acc));
     AGB_CK(upload(B, "solpar", p->solpar, N, &dsol, s, acc));
@@ -546,7 +586,6 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     AGB_CK(upload(B, "hbond", p->hbond, N, &dhb, s, acc));
     AGB_CK(upload(B, "rexp", p->rexp, N, &drexp, s, acc));
     AGB_CK(upload(B, "disorder", p->disorder, N, &ddis, s, acc));
-    AGB_CK(upload(B, "qw", qw.data(), N, &pl->qw, s, acc));
     AGB_CK(upload(B, "atomA", atomA.data(), atomA.size(), &pl->atomA, s, acc));
     AGB_CK(upload(B, "atomB", atomB.data(), atomB.size(), &pl->atomB, s, acc));
     AGB_CK(upload(B, "meta", meta.data(), meta.size(), &pl->meta, s, acc));
@@ -566,7 +605,6 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     AGB_CK(upload(B, "m_vol", mv.data(), mv.size(), &dmv, s, acc));
     if (!dev_tables) {
         AGB_CK(upload(B, "vdwT", vdwT.data(), vdwT.size(), &pl->vdwT, s, acc));
-        AGB_CK(upload(B, "far_tab", far_tab.data(), far_tab.size(), &pl->far_tab, s, acc));
         AGB_CK(upload(B, "etab", etab.data(), etab.size(), &pl->etab, s, acc));
         AGB_CK(upload(B, "solf", solf.data(), solf.size(), &pl->solf, s, acc));
         AGB_CK(upload(B, "sol_fn", p->sol_fn, AG_NDIEL, &dsolfn, s, acc));
@@ -597,8 +635,6 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     d.vdw = pl->vdwT; d.sol_fn = dsolfn; d.reps = dreps; d.far_tab = pl->far_tab;
 
     // outputs and scratch
-    void *v = nullptr;
-    const size_t P = (size_t)d.P;
     pl->floating = p->floating_grid ? 1 : 0;
     pl->constriction = p->constriction_grid ? 1 : 0;
     pl->constriction_cutoff = p->constriction_cutoff;
@@ -617,12 +653,6 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
         pl->cov = (double *)v;
     } else {
         pl->cov = nullptr;
-    }
-    if (pl->n_chunks > 0 && pl->opts.precision != AG_PREC_FP64) {
-        AGB_CK(B->ensure("far_partial", (size_t)pl->n_chunks * P * sizeof(float), &v));
-        pl->far_partial = (float *)v;
-    } else {
-        pl->far_partial = nullptr;
     }
     if (pl->far_partial && d.elec_map >= 0) {
         const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * P};
@@ -667,39 +697,56 @@ NearPtrs near_ptrs(const ag_plan *pl, unsigned long long *counters)
     return q;
 }
 
-// FP32 run as z-slabs of kSlabZ planes (whole far-field frames and
-// near-field brick rows), submitted slab by slab: far slab k on the side
-// stream; near slab k on s, then (after far slab k) the e-map reduction of
-// slab k, then event red_done[k].  The far and near kernels of neighbouring
-// slabs overlap, and a caller can copy slab k as soon as red_done[k] fires.
-ag_status enqueue_slabs(ag_plan *pl, cudaStream_t s, int nslab, int &launches)
+// Far-field z-slab k of nslab on the side stream; slab 0 first forks the side
+// stream from s.  far_done[k] marks the slab's end; evf0/evf1 bracket all slabs.
+ag_status launch_far_slab(ag_plan *pl, cudaStream_t s, int k, int nslab)
 {
     ag_context *c = pl->ctx;
-    const DevProblem &d = pl->dp;
-    const long long plane = (long long)d.n1x * d.n1y;
-    const bool far = d.elec_map >= 0 && pl->n_chunks > 0;
-    if (far) {
+    if (k == 0) {
         AGB_CK(cudaEventRecord(c->fork, s));
         AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
         AGB_CK(cudaEventRecord(c->evf0, c->side));
     }
+    int z0, z1;
+    slab_range(pl->dp, k, &z0, &z1);
+    const int fz0 = z0 / FRAME_Z, fz1 = (k == nslab - 1) ? -1 : z1 / FRAME_Z;
+    AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, fz0, fz1));
+    AGB_CK(cudaEventRecord(c->far_done[k], c->side));
+    if (k == nslab - 1) AGB_CK(cudaEventRecord(c->evf1, c->side));
+    return AG_OK;
+}
+
+// FP32 run as z-slabs (slab_range: whole far-field frames and near-field
+// brick rows), submitted slab by slab: far slab k on the side
+// stream (unless the plan launched it already); near slab k on s, then (after
+// far slab k) the e-map reduction of slab k, then event red_done[k].  The far
+// and near kernels of neighbouring slabs overlap, and a caller can copy slab k
+// as soon as red_done[k] fires.
+ag_status enqueue_slabs(ag_plan *pl, cudaStream_t s, int nslab, int &launches)
+{
+    const DevProblem &d = pl->dp;
+    ag_context *c = pl->ctx;
+    const long long plane = (long long)d.n1x * d.n1y;
+    const bool far = d.elec_map >= 0 && pl->n_chunks > 0;
     const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || d.elec_map >= 0;
     for (int k = 0; k < nslab; k++) {
         if (far) {
-            const int fz0 = k * (kSlabZ / FRAME_Z), fz1 = (k == nslab - 1) ? -1 : fz0 + kSlabZ / FRAME_Z;
-            AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, fz0, fz1));
-            AGB_CK(cudaEventRecord(c->far_done[k], c->side));
-            if (k == nslab - 1) AGB_CK(cudaEventRecord(c->evf1, c->side));
+            if (k >= pl->far_early) {
+                ag_status st = launch_far_slab(pl, s, k, nslab);
+                if (st != AG_OK) return st;
+            }
             launches++;
         }
-        const int bz0 = k * (kSlabZ / 4), bz1 = (k == nslab - 1) ? -1 : bz0 + kSlabZ / 4;  // 8x8x4 bricks
+        int sz0, sz1;
+        slab_range(d, k, &sz0, &sz1);
+        const int bz0 = sz0 / 4, bz1 = (k == nslab - 1) ? -1 : sz1 / 4;  // 8x8x4 bricks
         if (need_near)
             for (const NearGroup &g : pl->groups) {
                 AGB_CK(launch_near(false, d, g, near_ptrs(pl, c->d_counters), 0, s, bz0, bz1));
                 launches++;
             }
         if (far) {
-            const long long z0 = (long long)k * kSlabZ, z1 = (k == nslab - 1) ? d.n1z : z0 + kSlabZ;
+            const long long z0 = sz0, z1 = sz1;
             const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * d.P};
             AGB_CK(cudaStreamWaitEvent(s, c->far_done[k], 0));
             AGB_CK(launch_emap_reduce_range(r, z0 * plane, z1 * plane, s));
@@ -710,7 +757,6 @@ ag_status enqueue_slabs(ag_plan *pl, cudaStream_t s, int nslab, int &launches)
     return AG_OK;
 }
 
-int slab_count(const DevProblem &d) { return std::min(kMaxSlabs, (d.n1z + kSlabZ - 1) / kSlabZ); }
 
 ag_status run_plan(ag_plan *pl, cudaStream_t s)
 {
@@ -1084,8 +1130,10 @@ static ag_status run_plan_pipelined(ag_plan *pl, void *out, size_t n_out)
     const int nslab = slab_count(d);
     const long long plane = (long long)d.n1x * d.n1y;
     int launches = 0;
-    AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
-    AGB_CK(cudaEventRecord(c->ev0, s));
+    if (pl->far_early == 0) {  // else the plan cleared them and started the clock
+        AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+        AGB_CK(cudaEventRecord(c->ev0, s));
+    }
     if (pl->any_cov) {
         AGB_CK(launch_covalent(d, pl->cov, s));
         launches++;
@@ -1106,7 +1154,9 @@ static ag_status run_plan_pipelined(ag_plan *pl, void *out, size_t n_out)
     c->last_launches = launches;
     c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
     for (int k = 0; k < nslab; k++) {
-        const long long z0 = (long long)k * kSlabZ, z1 = (k == nslab - 1) ? d.n1z : z0 + kSlabZ;
+        int sz0, sz1;
+        slab_range(d, k, &sz0, &sz1);
+        const long long z0 = sz0, z1 = sz1;
         const size_t off = (size_t)(z0 * plane) * sizeof(float), width = (size_t)((z1 - z0) * plane) * sizeof(float);
         AGB_CK(cudaStreamWaitEvent(c->copy, c->red_done[k], 0));
         AGB_CK(cudaMemcpy2DAsync((char *)out + off, (size_t)d.P * sizeof(float), (const char *)pl->maps32 + off,
