@@ -42,8 +42,11 @@ __device__ __forceinline__ void load_far_table(float4 *s_tab4, const float *far_
 // One work unit: frame `f` of one instance against atom chunk `chunk`.
 // The caller has loaded the instance's table into s_tab4 and synchronised.
 // Atom tile entries: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
-template <int TILE, int MODE, int EF_PAIRS>
-__device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
+// Frames are 8*EF_PAIRS points wide; the first NJ pairs of each thread hold
+// the frame's x columns inside the box (the rest is padding and is skipped),
+// and a warp whose 4 rows or 2 planes all lie past the box skips the pairs.
+template <int TILE, int MODE, int EF_PAIRS, int NJ>
+__device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
 {
     const int tid = threadIdx.x;
     const int fx = f % a.nfx, fy = (f / a.nfx) % a.nfy, fz = f / (a.nfx * a.nfy);
@@ -58,17 +61,18 @@ __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, con
     const int tx = lane & 3;
     const int ty = ((lane >> 2) & 3) + 4 * (w & 1);
     const int tz = (lane >> 4) + 2 * (w >> 1);
+    const bool warp_in = oy + 4 * (w & 1) < a.n1y && oz + 2 * (w >> 1) < a.n1z;
     const float py = frame_point_coord(ty, a.spacing_adiv);
     const float pz = frame_point_coord(tz, a.spacing_adiv);
-    float2 npx[EF_PAIRS];
+    float2 npx[NJ];
 #pragma unroll
-    for (int j = 0; j < EF_PAIRS; j++)
+    for (int j = 0; j < NJ; j++)
         npx[j] = make_float2(-frame_point_coord(tx + 8 * j, a.spacing_adiv),
                              -frame_point_coord(tx + 8 * j + 4, a.spacing_adiv));
     const float2 npyz = make_float2(-py, -pz);
-    float2 tot[EF_PAIRS];
+    float2 tot[NJ];
 #pragma unroll
-    for (int j = 0; j < EF_PAIRS; j++) tot[j] = make_float2(0.f, 0.f);
+    for (int j = 0; j < NJ; j++) tot[j] = make_float2(0.f, 0.f);
 
     // 32-bit shared address of the table, pre-biased so that the bit pattern of
     // (t + 2^23) rounded toward zero indexes it directly:
@@ -96,9 +100,10 @@ __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, con
             s_atom[i] = v;
         }
         __syncthreads();
-        float2 acc[EF_PAIRS];
+        if (!warp_in) continue;
+        float2 acc[NJ];
 #pragma unroll
-        for (int j = 0; j < EF_PAIRS; j++) acc[j] = make_float2(0.f, 0.f);
+        for (int j = 0; j < NJ; j++) acc[j] = make_float2(0.f, 0.f);
 #pragma unroll 2
         for (int i = 0; i < na; i++) {
             const float4 A = s_atom[i];
@@ -108,7 +113,7 @@ __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, con
             const float2 ax2 = make_float2(A.x, A.x);
             const float2 q2 = make_float2(A.w, A.w);
 #pragma unroll
-            for (int j = 0; j < EF_PAIRS; j++) {
+            for (int j = 0; j < NJ; j++) {
                 const float2 dx = __fadd2_rn(ax2, npx[j]);
                 const float2 t2 = __ffma2_rn(dx, dx, s2);
                 const float2 rs = make_float2(rsqrt_approx(t2.x), rsqrt_approx(t2.y));
@@ -128,19 +133,32 @@ __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, con
             }
         }
 #pragma unroll
-        for (int j = 0; j < EF_PAIRS; j++) tot[j] = __fadd2_rn(tot[j], acc[j]);
+        for (int j = 0; j < NJ; j++) tot[j] = __fadd2_rn(tot[j], acc[j]);
     }
 
     const int iy = oy + ty, iz = oz + tz;
     if (iy < a.n1y && iz < a.n1z) {
         float *out = a.partial + (size_t)chunk * (size_t)a.P + ((size_t)iz * a.n1y + iy) * (size_t)a.n1x;
 #pragma unroll
-        for (int j = 0; j < EF_PAIRS; j++) {
+        for (int j = 0; j < NJ; j++) {
             const int ix0 = ox + tx + 8 * j, ix1 = ix0 + 4;
             if (ix0 < a.n1x) out[ix0] = tot[j].x;
             if (ix1 < a.n1x) out[ix1] = tot[j].y;
         }
     }
+}
+
+// The unit with as many x pairs as the frame has columns inside the box
+// (CTA-uniform: only a box's last x frame can be partial).
+template <int TILE, int MODE, int EF_PAIRS>
+__device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
+{
+    const int ox = (f % a.nfx) * (8 * EF_PAIRS);
+    const int nj = (a.n1x - ox + 7) / 8;
+    if (nj >= EF_PAIRS) far_unit_n<TILE, MODE, EF_PAIRS, EF_PAIRS>(a, f, chunk, s_tab4, s_atom);
+    else if (nj == 1) far_unit_n<TILE, MODE, EF_PAIRS, 1>(a, f, chunk, s_tab4, s_atom);
+    else if (EF_PAIRS == 4 && nj == 2) far_unit_n<TILE, MODE, EF_PAIRS, (EF_PAIRS == 4 ? 2 : 1)>(a, f, chunk, s_tab4, s_atom);
+    else far_unit_n<TILE, MODE, EF_PAIRS, (EF_PAIRS == 4 ? 3 : 1)>(a, f, chunk, s_tab4, s_atom);
 }
 
 // Single instance: one CTA per (frame, chunk) = (blockIdx.x, blockIdx.y).
@@ -157,8 +175,10 @@ __device__ __forceinline__ void far_dispatch(const FarArgs &a, int f, int chunk,
     }
 }
 
-// One instance; the frame width (PAIRS = frame_x / 8) is fixed per launch.
-template <int TILE, int PAIRS>
+// One instance; the frame width (PAIRS = frame_x / 8) is fixed per launch, and
+// so is the x-pair count of the box's last x frame (NJ_LAST).  A grid whose
+// last x frame is full compiles to the full-frame unit alone.
+template <int TILE, int PAIRS, int NJ_LAST>
 __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
 {
     extern __shared__ float4 ef_smem[];
@@ -166,8 +186,15 @@ __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
     float4 *s_atom = ef_smem + AG_NDIEL / 4;  // TILE entries
     if (a.tab_mode != FAR_TAB_CONST) load_far_table(s_tab4, a.far_tab);
     __syncthreads();
-    if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST, PAIRS>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
-    else far_unit<TILE, FAR_TAB_TABLE, PAIRS>(a, a.frame0 + blockIdx.x, blockIdx.y, s_tab4, s_atom);
+    const int f = a.frame0 + blockIdx.x;
+    const bool last = NJ_LAST < PAIRS && f % a.nfx == a.nfx - 1;
+    if (a.tab_mode == FAR_TAB_CONST) {
+        if (last) far_unit_n<TILE, FAR_TAB_CONST, PAIRS, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
+        else far_unit_n<TILE, FAR_TAB_CONST, PAIRS, PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
+    } else {
+        if (last) far_unit_n<TILE, FAR_TAB_TABLE, PAIRS, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
+        else far_unit_n<TILE, FAR_TAB_TABLE, PAIRS, PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
+    }
 }
 
 // Many instances, persistent: each CTA takes (instance, frame, chunk) units
@@ -266,20 +293,22 @@ size_t far_smem_bytes(int tile) { return AG_NDIEL * sizeof(float) + (size_t)tile
 // Frame z-rows [fz0, fz1) of one instance (fz1 < 0: through the last).
 cudaError_t launch_emap_far(const FarArgs &args, int n_chunks, int tile, cudaStream_t s, int fz0, int fz1)
 {
+    if (tile != 512) return cudaErrorInvalidValue;  // the single-instance kernel stages 512-atom tiles
     FarArgs a = args;
     if (fz1 < 0 || fz1 > a.nfz) fz1 = a.nfz;
     if (fz0 >= fz1) return cudaSuccess;
     a.frame0 = fz0 * a.nfx * a.nfy;
     dim3 grid((unsigned)(a.nfx * a.nfy * (fz1 - fz0)), (unsigned)n_chunks);
-    const size_t smem = far_smem_bytes(tile);
+    const size_t smem = far_smem_bytes(512);
+    const int nj_last = (a.n1x - (a.nfx - 1) * a.frame_x + 7) / 8;  // x pairs of the last frame inside the box
     if (a.frame_x == 16) {
-        if (tile == 256) k_emap_far<256, 2><<<grid, EF_THREADS, smem, s>>>(a);
-        else if (tile == 1024) k_emap_far<1024, 2><<<grid, EF_THREADS, smem, s>>>(a);
-        else k_emap_far<512, 2><<<grid, EF_THREADS, smem, s>>>(a);
+        if (nj_last >= 2) k_emap_far<512, 2, 2><<<grid, EF_THREADS, smem, s>>>(a);
+        else k_emap_far<512, 2, 1><<<grid, EF_THREADS, smem, s>>>(a);
     } else {
-        if (tile == 256) k_emap_far<256, 4><<<grid, EF_THREADS, smem, s>>>(a);
-        else if (tile == 1024) k_emap_far<1024, 4><<<grid, EF_THREADS, smem, s>>>(a);
-        else k_emap_far<512, 4><<<grid, EF_THREADS, smem, s>>>(a);
+        if (nj_last >= 4) k_emap_far<512, 4, 4><<<grid, EF_THREADS, smem, s>>>(a);
+        else if (nj_last == 3) k_emap_far<512, 4, 3><<<grid, EF_THREADS, smem, s>>>(a);
+        else if (nj_last == 2) k_emap_far<512, 4, 2><<<grid, EF_THREADS, smem, s>>>(a);
+        else k_emap_far<512, 4, 1><<<grid, EF_THREADS, smem, s>>>(a);
     }
     return cudaGetLastError();
 }
