@@ -344,7 +344,6 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     d.elec_map = p->elec_map; d.dsolv_map = p->dsolv_map;
     d.n1x = p->n1[0]; d.n1y = p->n1[1]; d.n1z = p->n1[2];
     d.nex = p->ne[0]; d.ney = p->ne[1]; d.nez = p->ne[2];
-    d.frame_x = choose_frame_x(d.n1x);
     d.P = (long long)d.n1x * d.n1y * d.n1z;
     d.spacing = p->spacing;
     d.dddiel = p->dddiel; d.disorder_h = p->disorder_h; d.hydrogen_type = p->hydrogen_type;
@@ -382,8 +381,8 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     }
     // far-field chunking: enough CTAs for ~8 waves per launch; a slab-pipelined
     // one-shot run launches one slab of frames at a time, ~3 waves each
-    const long long frames = pipelined ? (long long)frames_x(d.n1x, d.frame_x) * frames_y(d.n1y) * (kSlabZ / FRAME_Z)
-                                       : (long long)frames_x(d.n1x, d.frame_x) * frames_y(d.n1y) * frames_z(d.n1z);
+    const long long frames = pipelined ? (long long)frames_x(d.n1x) * frames_y(d.n1y) * (kSlabZ / FRAME_Z)
+                                       : (long long)frames_x(d.n1x) * frames_y(d.n1y) * frames_z(d.n1z);
     const int tile = 512;
     if (p->elec_map >= 0 && N > 0) {
         const long long target = pipelined ? 148LL * 3 * 3 : 148LL * 3 * 8;
@@ -681,8 +680,7 @@ FarArgs far_args(const ag_plan *pl)
     a.spacing_adiv = d.spacing * AG_A_DIV; a.P = d.P;
     a.n_atoms = d.n_atoms; a.chunk_atoms = pl->chunk_atoms;
     a.n1x = d.n1x; a.n1y = d.n1y; a.n1z = d.n1z; a.nex = d.nex; a.ney = d.ney; a.nez = d.nez;
-    a.frame_x = d.frame_x;
-    a.nfx = frames_x(d.n1x, d.frame_x); a.nfy = frames_y(d.n1y); a.nfz = frames_z(d.n1z);
+    a.nfx = frames_x(d.n1x); a.nfy = frames_y(d.n1y); a.nfz = frames_z(d.n1z);
     a.tab_mode = pl->far_mode;
     a.tab_const = pl->far_const;
     return a;

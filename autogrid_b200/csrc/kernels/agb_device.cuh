@@ -77,7 +77,6 @@ struct FarArgs {
     int n_atoms, chunk_atoms;
     int n1x, n1y, n1z, nex, ney, nez, nfx, nfy, nfz;
     int frame0;                           // single-instance launches: first frame of the launch
-    int frame_x;                          // frame width in points: 32 (4 point pairs per thread) or 16 (2)
     // How a pair's table value T[b] (b = floor(t) >= AG_NEINT) is obtained:
     //   FAR_TAB_TABLE  shared-memory gather from far_tab, every pair;
     //   FAR_TAB_CONST  far_tab is one constant (constant dielectric): no gather.
@@ -91,7 +90,6 @@ struct DevProblem {
     int n_atoms, n_maps, n_atom_maps, n_rec_types;
     int elec_map, dsolv_map;
     int n1x, n1y, n1z, nex, ney, nez;
-    int frame_x;                          // far-kernel frame width (16 or 32; the near kernel follows it)
     long long P;
     double spacing;
     int dddiel, disorder_h, hydrogen_type, sep_desolv;

@@ -24,8 +24,8 @@
 namespace agb {
 
 constexpr int EF_THREADS = 256;
-// float2 pairs of points per thread: 4 (8 points, frames 32 wide) or 2 (4
-// points, frames 16 wide, for grids that 32-wide frames would pad more)
+// float2 pairs of points per thread: 8 points of one x-row, FRAME_X wide
+constexpr int EF_PAIRS = FRAME_X / 8;
 
 __device__ __forceinline__ float lds_f32(uint32_t addr)
 {
@@ -42,15 +42,15 @@ __device__ __forceinline__ void load_far_table(float4 *s_tab4, const float *far_
 // One work unit: frame `f` of one instance against atom chunk `chunk`.
 // The caller has loaded the instance's table into s_tab4 and synchronised.
 // Atom tile entries: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
-// Frames are 8*EF_PAIRS points wide; the first NJ pairs of each thread hold
-// the frame's x columns inside the box (the rest is padding and is skipped),
-// and a warp whose 4 rows or 2 planes all lie past the box skips the pairs.
-template <int TILE, int MODE, int EF_PAIRS, int NJ>
+// The first NJ pairs of each thread hold the frame's x columns inside the box
+// (the rest is padding and is skipped), and a warp whose 4 rows or 2 planes
+// all lie past the box skips the pairs.
+template <int TILE, int MODE, int NJ>
 __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
 {
     const int tid = threadIdx.x;
     const int fx = f % a.nfx, fy = (f / a.nfx) % a.nfy, fz = f / (a.nfx * a.nfy);
-    const int ox = fx * (8 * EF_PAIRS), oy = fy * FRAME_Y, oz = fz * FRAME_Z;
+    const int ox = fx * FRAME_X, oy = fy * FRAME_Y, oz = fz * FRAME_Z;
     // frame origin in bins, exactly (ox-nex)*spacing*A_DIV as the reference forms c (main.cpp:2859)
     const double X0 = frame_origin_bins(ox, a.nex, a.spacing_adiv);
     const double Y0 = frame_origin_bins(oy, a.ney, a.spacing_adiv);
@@ -150,35 +150,29 @@ __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, c
 
 // The unit with as many x pairs as the frame has columns inside the box
 // (CTA-uniform: only a box's last x frame can be partial).
-template <int TILE, int MODE, int EF_PAIRS>
+template <int TILE, int MODE>
 __device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
 {
-    const int ox = (f % a.nfx) * (8 * EF_PAIRS);
-    const int nj = (a.n1x - ox + 7) / 8;
-    if (nj >= EF_PAIRS) far_unit_n<TILE, MODE, EF_PAIRS, EF_PAIRS>(a, f, chunk, s_tab4, s_atom);
-    else if (nj == 1) far_unit_n<TILE, MODE, EF_PAIRS, 1>(a, f, chunk, s_tab4, s_atom);
-    else if (EF_PAIRS == 4 && nj == 2) far_unit_n<TILE, MODE, EF_PAIRS, (EF_PAIRS == 4 ? 2 : 1)>(a, f, chunk, s_tab4, s_atom);
-    else far_unit_n<TILE, MODE, EF_PAIRS, (EF_PAIRS == 4 ? 3 : 1)>(a, f, chunk, s_tab4, s_atom);
+    static_assert(EF_PAIRS == 4, "x-pair dispatch below");
+    const int nj = (a.n1x - (f % a.nfx) * FRAME_X + 7) / 8;
+    if (nj >= 4) far_unit_n<TILE, MODE, 4>(a, f, chunk, s_tab4, s_atom);
+    else if (nj == 3) far_unit_n<TILE, MODE, 3>(a, f, chunk, s_tab4, s_atom);
+    else if (nj == 2) far_unit_n<TILE, MODE, 2>(a, f, chunk, s_tab4, s_atom);
+    else far_unit_n<TILE, MODE, 1>(a, f, chunk, s_tab4, s_atom);
 }
 
-// Single instance: one CTA per (frame, chunk) = (blockIdx.x, blockIdx.y).
-// The instantiation for the unit's table mode and frame width.
+// The unit for the instance's table mode (batch kernel).
 template <int TILE>
 __device__ __forceinline__ void far_dispatch(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
 {
-    if (a.frame_x == 16) {
-        if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST, 2>(a, f, chunk, s_tab4, s_atom);
-        else far_unit<TILE, FAR_TAB_TABLE, 2>(a, f, chunk, s_tab4, s_atom);
-    } else {
-        if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST, 4>(a, f, chunk, s_tab4, s_atom);
-        else far_unit<TILE, FAR_TAB_TABLE, 4>(a, f, chunk, s_tab4, s_atom);
-    }
+    if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST>(a, f, chunk, s_tab4, s_atom);
+    else far_unit<TILE, FAR_TAB_TABLE>(a, f, chunk, s_tab4, s_atom);
 }
 
-// One instance; the frame width (PAIRS = frame_x / 8) is fixed per launch, and
-// so is the x-pair count of the box's last x frame (NJ_LAST).  A grid whose
-// last x frame is full compiles to the full-frame unit alone.
-template <int TILE, int PAIRS, int NJ_LAST>
+// Single instance: one CTA per (frame, chunk) = (blockIdx.x, blockIdx.y).  The
+// x-pair count of the box's last x frame (NJ_LAST) is fixed per launch, so a
+// grid whose last x frame is full compiles to the full-frame unit alone.
+template <int TILE, int NJ_LAST>
 __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
 {
     extern __shared__ float4 ef_smem[];
@@ -187,13 +181,13 @@ __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
     if (a.tab_mode != FAR_TAB_CONST) load_far_table(s_tab4, a.far_tab);
     __syncthreads();
     const int f = a.frame0 + blockIdx.x;
-    const bool last = NJ_LAST < PAIRS && f % a.nfx == a.nfx - 1;
+    const bool last = NJ_LAST < EF_PAIRS && f % a.nfx == a.nfx - 1;
     if (a.tab_mode == FAR_TAB_CONST) {
-        if (last) far_unit_n<TILE, FAR_TAB_CONST, PAIRS, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
-        else far_unit_n<TILE, FAR_TAB_CONST, PAIRS, PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
+        if (last) far_unit_n<TILE, FAR_TAB_CONST, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
+        else far_unit_n<TILE, FAR_TAB_CONST, EF_PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
     } else {
-        if (last) far_unit_n<TILE, FAR_TAB_TABLE, PAIRS, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
-        else far_unit_n<TILE, FAR_TAB_TABLE, PAIRS, PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
+        if (last) far_unit_n<TILE, FAR_TAB_TABLE, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
+        else far_unit_n<TILE, FAR_TAB_TABLE, EF_PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
     }
 }
 
@@ -276,15 +270,7 @@ k_emap_exact(DevProblem p, double *__restrict__ emap)
 
 namespace agb {
 
-int frames_x(int n1x, int frame_x) { return (n1x + frame_x - 1) / frame_x; }
-
-// 16-wide frames where they pad the x axis less than 32-wide ones, counting
-// the 16-wide kernel's extra atom loads (one per 4 points instead of 8) as 5%.
-int choose_frame_x(int n1x)
-{
-    const double c32 = (double)frames_x(n1x, 32) * 32, c16 = (double)frames_x(n1x, 16) * 16 * 1.05;
-    return c16 < c32 ? 16 : 32;
-}
+int frames_x(int n1x) { return (n1x + FRAME_X - 1) / FRAME_X; }
 int frames_y(int n1y) { return (n1y + FRAME_Y - 1) / FRAME_Y; }
 int frames_z(int n1z) { return (n1z + FRAME_Z - 1) / FRAME_Z; }
 
@@ -300,16 +286,11 @@ cudaError_t launch_emap_far(const FarArgs &args, int n_chunks, int tile, cudaStr
     a.frame0 = fz0 * a.nfx * a.nfy;
     dim3 grid((unsigned)(a.nfx * a.nfy * (fz1 - fz0)), (unsigned)n_chunks);
     const size_t smem = far_smem_bytes(512);
-    const int nj_last = (a.n1x - (a.nfx - 1) * a.frame_x + 7) / 8;  // x pairs of the last frame inside the box
-    if (a.frame_x == 16) {
-        if (nj_last >= 2) k_emap_far<512, 2, 2><<<grid, EF_THREADS, smem, s>>>(a);
-        else k_emap_far<512, 2, 1><<<grid, EF_THREADS, smem, s>>>(a);
-    } else {
-        if (nj_last >= 4) k_emap_far<512, 4, 4><<<grid, EF_THREADS, smem, s>>>(a);
-        else if (nj_last == 3) k_emap_far<512, 4, 3><<<grid, EF_THREADS, smem, s>>>(a);
-        else if (nj_last == 2) k_emap_far<512, 4, 2><<<grid, EF_THREADS, smem, s>>>(a);
-        else k_emap_far<512, 4, 1><<<grid, EF_THREADS, smem, s>>>(a);
-    }
+    const int nj_last = (a.n1x - (a.nfx - 1) * FRAME_X + 7) / 8;  // x pairs of the last frame inside the box
+    if (nj_last >= 4) k_emap_far<512, 4><<<grid, EF_THREADS, smem, s>>>(a);
+    else if (nj_last == 3) k_emap_far<512, 3><<<grid, EF_THREADS, smem, s>>>(a);
+    else if (nj_last == 2) k_emap_far<512, 2><<<grid, EF_THREADS, smem, s>>>(a);
+    else k_emap_far<512, 1><<<grid, EF_THREADS, smem, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -62,8 +62,7 @@ cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, con
                         cudaStream_t s, int bz0 = 0, int bz1 = -1);
 cudaError_t launch_near_batch(const NearInst *insts, const long long *unit_begin, int n_inst,
                               unsigned long long *counter, int shape, int ctas_per_sm, cudaStream_t s);
-int frames_x(int n1x, int frame_x);
-int choose_frame_x(int n1x);
+int frames_x(int n1x);
 int frames_y(int n1y);
 int frames_z(int n1z);
 

@@ -291,7 +291,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                                           NearSmem &S)
 {
     static_assert(BX * BY * BZ == NB_THREADS, "one thread per brick point");
-    static_assert(16 % BX == 0 && FRAME_Y % BY == 0 && FRAME_Z % BZ == 0, "bricks tile far frames (16 or 32 wide)");
+    static_assert(FRAME_X % BX == 0 && FRAME_Y % BY == 0 && FRAME_Z % BZ == 0, "bricks tile far frames");
     using R = typename std::conditional<EXACT, double, float>::type;
     const int tid = threadIdx.x;
     if (tid < 2) S.cnt[tid] = 0ull;
@@ -302,13 +302,17 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     __syncthreads();
     const int nbx = (p.n1x + BX - 1) / BX, nby = (p.n1y + BY - 1) / BY;
     const int bx = b % nbx, by = (b / nbx) % nby, bz = b / (nbx * nby);
-    const int ix = bx * BX + tid % BX, iy = by * BY + (tid / BX) % BY, iz = bz * BZ + tid / (BX * BY);
-    const bool valid = ix < p.n1x && iy < p.n1y && iz < p.n1z;
+    // the brick's points inside the box, packed into its first wx*wy*wz threads
+    // (x fastest), so that a brick on the box's edge leaves whole warps idle
+    // instead of idle lanes in every warp; interior bricks: tid = x + BX*(y + BY*z)
+    const int wx = min(BX, p.n1x - bx * BX), wy = min(BY, p.n1y - by * BY), wz = min(BZ, p.n1z - bz * BZ);
+    const int ix = bx * BX + tid % wx, iy = by * BY + (tid / wx) % wy, iz = bz * BZ + tid / (wx * wy);
+    const bool valid = tid < wx * wy * wz;
     const long long lin = ((long long)iz * p.n1y + iy) * p.n1x + ix;
 
     // far-kernel frame of this brick and the point's canonical coordinates
     const double sp128 = p.spacing * AG_A_DIV;
-    const int ox = ((bx * BX) / p.frame_x) * p.frame_x, oy = ((by * BY) / FRAME_Y) * FRAME_Y,
+    const int ox = ((bx * BX) / FRAME_X) * FRAME_X, oy = ((by * BY) / FRAME_Y) * FRAME_Y,
               oz = ((bz * BZ) / FRAME_Z) * FRAME_Z;
     const double X0 = frame_origin_bins(ox, p.nex, sp128), Y0 = frame_origin_bins(oy, p.ney, sp128),
                  Z0 = frame_origin_bins(oz, p.nez, sp128);
