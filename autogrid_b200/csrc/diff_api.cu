@@ -384,6 +384,7 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
         A.slot_sp[s] = (sl.kind != DK_D) ? p->map_solpar_probe[sl.map] : 0.0;
         A.slot_vp[s] = (sl.kind != DK_D) ? p->map_vol_probe[sl.map] : 0.0;
         std::memcpy(A.act[s], sl.act, 16);
+        if (sl.kind == DK_D || sl.desolv) A.need_sol = 1;
     }
     // cell list geometry: at most 6 cells per axis around a brick
     const double span = (DF_BRICK_X - 1) * p->spacing + 2 * DF_RADIUS;

@@ -75,6 +75,7 @@ struct DiffArgs {
     // slots: every map except the e map; maps per conformer in the output;
     // slots per (type, bin) row of the vdW table
     int n_slots, n_mm, n_maps_out, tab_stride;
+    int need_sol;                // 1: some slot reads the desolvation table (a d map or a desolvation term)
     int slot_map[DF_MAXS];       // output map index
     int slot_kind[DF_MAXS];      // DK_*
     int slot_tab[DF_MAXS];       // atom-map index of the pair term (-1: none)

@@ -248,7 +248,7 @@ k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ 
         for (int k = 0; k < cnt; k++) {
             const Atom<R> at = sm.at[wl[k]];
             Geom<R> g;
-            if (!geom(sol, at, px, py, pz, g)) continue;
+            if (!geom(a.need_sol ? sol : nullptr, at, px, py, pz, g)) continue;
             const int hb = (at.meta >> DM_HB_SHIFT) & 7;
             Ang<R> an;
             angular(hb, (at.meta >> DM_REXP_SHIFT) & 7, (at.meta & DM_DIS) != 0, ch >= 0 && at.idx != ch, g.dn,
@@ -324,7 +324,7 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
         for (int k = 0; k < cnt; k++) {
             const Atom<R> at = sm.at[wl[k]];
             Geom<R> g;
-            const bool in = bk.valid && geom(sol, at, px, py, pz, g);
+            const bool in = bk.valid && geom(a.need_sol ? sol : nullptr, at, px, py, pz, g);
             if (!__any_sync(0xffffffffu, in)) continue;
             const int hb = (at.meta >> DM_HB_SHIFT) & 7;
             const bool dis = (at.meta & DM_DIS) != 0;
@@ -340,7 +340,9 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
                 geom_bwd(g, G_x, g_dn, g_d);
             }
             // the candidate is the same for the whole warp: reduce, one lane adds
-            const R sx = warp_sum(g_d[0]), sy = warp_sum(g_d[1]), sz = warp_sum(g_d[2]), sq = warp_sum(G_q);
+            // G_q comes from desolvation terms only
+            const R sx = warp_sum(g_d[0]), sy = warp_sum(g_d[1]), sz = warp_sum(g_d[2]);
+            const R sq = a.need_sol ? warp_sum(G_q) : (R)0;
             R sr[3] = {0, 0, 0}, sr2[3] = {0, 0, 0};
             const bool has_rv = hb == 2 || hb == 4 || hb == 5;
             const bool has_rv2 = hb == 5 && !dis;

@@ -182,12 +182,36 @@ template <class R> struct Atom {
 // Geometry of one pair: d = atom - point, x = A_DIV r, switch w(x) and the
 // desolvation factor sol(x).
 template <class R> struct Geom {
-    R d[3], dn[3], r, x, fx, w, dw, sol, dsol;
+    R d[3], dn[3], r, inv, x, fx, w, dw, sol, dsol;
     int b;
 };
 
+// r = max(|d|, DF_TINY) and 1 / r from r^2.  r is the correctly rounded
+// square root everywhere (it picks the table bin, and the adjoint's slopes
+// jump at bin edges); FP32 on the device takes 1 / r from one rsqrt.approx
+// (about 2 ulp) instead of a division.
+DF_HD void dist_inv(double r2, double &r, double &inv)
+{
+    r = sqrt(r2);
+    if (r < DF_TINY) r = DF_TINY;
+    inv = 1.0 / r;
+}
+DF_HD void dist_inv(float r2, float &r, float &inv)
+{
+#ifdef __CUDA_ARCH__
+    r = sqrtf(r2);
+    if (r < float(DF_TINY)) r = float(DF_TINY);
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(inv) : "f"(r * r));
+#else
+    r = sqrtf(r2);
+    if (r < float(DF_TINY)) r = float(DF_TINY);
+    inv = 1.0f / r;
+#endif
+}
+
 // False when the pair adds nothing: beyond 8 A, or a disordered hydrogen that
-// LOOP 2 skips (main.cpp:3052).
+// LOOP 2 skips (main.cpp:3052).  sol may be null when no slot reads the
+// desolvation table (sol and dsol are then 0).
 template <class R>
 DF_HD bool geom(const R2<R> *sol, const Atom<R> &at, R px, R py, R pz, Geom<R> &g)
 {
@@ -195,10 +219,10 @@ DF_HD bool geom(const R2<R> *sol, const Atom<R> &at, R px, R py, R pz, Geom<R> &
     g.d[0] = at.x - px; g.d[1] = at.y - py; g.d[2] = at.z - pz;
     const R r2 = g.d[0] * g.d[0] + g.d[1] * g.d[1] + g.d[2] * g.d[2];
     if (r2 > R(AG_NBC * AG_NBC)) return false;
-    R r = sqrt_(r2);
-    if (r < R(DF_TINY)) r = R(DF_TINY);
+    R r, inv;
+    dist_inv(r2, r, inv);
     g.r = r;
-    const R inv = R(1) / r;
+    g.inv = inv;
     for (int i = 0; i < 3; i++) g.dn[i] = g.d[i] * inv;
     g.x = r * R(AG_A_DIV);
     int b = (int)g.x;
@@ -208,8 +232,13 @@ DF_HD bool geom(const R2<R> *sol, const Atom<R> &at, R px, R py, R pz, Geom<R> &
     const R room = R(AG_NEINT) - g.x;
     g.w = room < R(1) ? room : R(1);
     g.dw = room < R(1) ? R(-1) : R(0);
-    g.sol = lerp(sol[b], g.fx);
-    g.dsol = sol[b].d;
+    if (sol) {
+        g.sol = lerp(sol[b], g.fx);
+        g.dsol = sol[b].d;
+    } else {
+        g.sol = R(0);
+        g.dsol = R(0);
+    }
     return true;
 }
 
@@ -234,11 +263,11 @@ template <class R> struct Term {
     R v, dT, dTH, dracc, drdon, dH, dx;  // dx: total d v / d x through both tables
 };
 
+// te: the pair's table entry (value, slope) for slot s.
 template <class R>
-DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, int type, int s, const Geom<R> &g, const Ang<R> &an,
-                Term<R> &t)
+DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, const R2<R> &te, int s, const Geom<R> &g,
+                const Ang<R> &an, Term<R> &t)
 {
-    const R2<R> te = vdw[((size_t)type * AG_NEINT + g.b) * a.tab_stride + s];
     const R T = lerp(te, g.fx);
     R drs;
     const R rs = rsph(T, drs);
@@ -294,6 +323,30 @@ DF_HD void term(const DiffArgs &a, const R2<R> *vdw, int act, int type, int s, c
 
 DF_HD bool act_is_mm(int act) { return act == DA_MMA || act == DA_MMD; }
 
+// The first n (<= MS) entries of a table row.  FP32 on the device reads two
+// slots per 16-byte load: rows hold tab_stride (a multiple of 4) entries of
+// 8 bytes, so every row starts 16-byte aligned.
+template <class R, int MS>
+DF_HD void load_row(const R2<R> *row, int n, R2<R> *out)
+{
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 4 && MS % 2 == 0) {
+        const float4 *r4 = reinterpret_cast<const float4 *>(row);
+#pragma unroll
+        for (int k = 0; k < MS / 2; k++)
+            if (2 * k < n) {
+                const float4 v = __ldg(r4 + k);
+                out[2 * k] = R2<R>{v.x, v.y};
+                out[2 * k + 1] = R2<R>{v.z, v.w};
+            }
+        return;
+    }
+#endif
+#pragma unroll
+    for (int s = 0; s < MS; s++)
+        if (s < n) out[s] = row[s];
+}
+
 // Forward: add one pair to the point's slot energies and min/max registers.
 // MS, MM: the slots and min/max registers a kernel instantiation holds
 // (at least a.n_slots and a.n_mm).
@@ -305,6 +358,8 @@ DF_HD void pair_fwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
     const int cls = hb + ((at.meta & DM_DIS) ? 8 : 0);
     const R qasp = R(a.solpar_q);
     const R solv = at.solpar + qasp * ab(at.q);
+    R2<R> te[MS];
+    load_row<R, MS>(vdw + ((size_t)type * AG_NEINT + g.b) * a.tab_stride, a.n_slots, te);
 #pragma unroll
     for (int s = 0; s < MS; s++) {
         if (s >= a.n_slots) break;
@@ -318,7 +373,7 @@ DF_HD void pair_fwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
             const int act = a.act[s][cls];
             if (act != DA_NONE) {
                 Term<R> t;
-                term(a, vdw, act, type, s, g, an, t);
+                term(a, vdw, act, te[s], s, g, an, t);
                 const R val = g.w * t.v;
                 if (act_is_mm(act)) {
                     if (s < MM) {  // min/max slots come first
@@ -372,7 +427,7 @@ DF_HD void pair_bwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
                 }
                 if (gv != R(0)) {
                     Term<R> t;
-                    term(a, vdw, act, type, s, g, an, t);
+                    term(a, vdw, act, vdw[((size_t)type * AG_NEINT + g.b) * a.tab_stride + s], s, g, an, t);
                     G_x += gv * (g.dw * t.v + g.w * t.dx);
                     G_racc += gv * g.w * t.dracc;
                     G_rdon += gv * g.w * t.drdon;
@@ -394,8 +449,7 @@ DF_HD void geom_bwd(const Geom<R> &g, R G_x, const R g_dn[3], R g_d[3])
 {
     const R gr = G_x * R(AG_A_DIV);
     const R ddot = g.dn[0] * g_dn[0] + g.dn[1] * g_dn[1] + g.dn[2] * g_dn[2];
-    const R inv = R(1) / g.r;
-    for (int i = 0; i < 3; i++) g_d[i] = gr * g.dn[i] + (g_dn[i] - g.dn[i] * ddot) * inv;
+    for (int i = 0; i < 3; i++) g_d[i] = gr * g.dn[i] + (g_dn[i] - g.dn[i] * ddot) * g.inv;
 }
 
 }  // namespace dfm
