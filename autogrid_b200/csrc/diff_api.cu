@@ -354,6 +354,7 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
 
     DiffArgs &A = d->args;
     std::memset(&A, 0, sizeof A);
+    A.need_ang = need_ang ? 1 : 0;
     A.n_atoms = N;
     A.n1x = p->n1[0]; A.n1y = p->n1[1]; A.n1z = p->n1[2];
     A.nex = p->ne[0]; A.ney = p->ne[1]; A.nez = p->ne[2];

@@ -76,6 +76,7 @@ struct DiffArgs {
     // slots per (type, bin) row of the vdW table
     int n_slots, n_mm, n_maps_out, tab_stride;
     int need_sol;                // 1: some slot reads the desolvation table (a d map or a desolvation term)
+    int need_ang;                // 1: some slot's term uses the directional factors
     int slot_map[DF_MAXS];       // output map index
     int slot_kind[DF_MAXS];      // DK_*
     int slot_tab[DF_MAXS];       // atom-map index of the pair term (-1: none)

@@ -209,8 +209,9 @@ template <class R> __device__ __forceinline__ R covalent_value(const DiffArgs &a
 // MS slots and MM min/max registers per point: the general instantiation
 // holds DF_MAXS / DF_MAXMM; map sets of at most DF_LEAN_S slots without
 // H-bond min/max (Vina maps, plain AD4 subsets) take the lean one, whose
-// registers leave room for 3 resident CTAs per SM.
-template <class R, int MS, int MM, int MINB>
+// registers leave room for 3 resident CTAs per SM.  ANG = false: no slot uses
+// the directional factors (DiffArgs::need_ang), so none are evaluated.
+template <class R, int MS, int MM, int MINB, bool ANG = true>
 __global__ void __launch_bounds__(DF_THREADS, MINB)
 k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ sol, R *__restrict__ maps,
            const int *__restrict__ chs, int *__restrict__ mmarg)
@@ -249,10 +250,12 @@ k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ 
             const Atom<R> at = sm.at[wl[k]];
             Geom<R> g;
             if (!geom(a.need_sol ? sol : nullptr, at, px, py, pz, g)) continue;
-            const int hb = (at.meta >> DM_HB_SHIFT) & 7;
             Ang<R> an;
-            angular(hb, (at.meta >> DM_REXP_SHIFT) & 7, (at.meta & DM_DIS) != 0, ch >= 0 && at.idx != ch, g.dn,
-                    at.rv, at.rv2, rvh, an);
+            if (ANG)
+                angular((at.meta >> DM_HB_SHIFT) & 7, (at.meta >> DM_REXP_SHIFT) & 7, (at.meta & DM_DIS) != 0,
+                        ch >= 0 && at.idx != ch, g.dn, at.rv, at.rv2, rvh, an);
+            else
+                ang_plain(an);
             pair_fwd<R, MS, MM>(a, vdw, g, at, an, E, hmin, hmax, amin, amax);
         }
     }
@@ -279,7 +282,7 @@ template <class R> __device__ __forceinline__ R warp_sum(R v)
     return v;
 }
 
-template <class R, int MS, int MM, int MINB>
+template <class R, int MS, int MM, int MINB, bool ANG = true>
 __global__ void __launch_bounds__(DF_THREADS, MINB)
 k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ sol,
                const R *__restrict__ g_maps, const int *__restrict__ chs, const int *__restrict__ mmarg,
@@ -331,12 +334,17 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
             R g_d[3] = {0, 0, 0}, g_rv[3] = {0, 0, 0}, g_rv2[3] = {0, 0, 0}, G_q = 0;
             if (in) {
                 Ang<R> an;
-                angular(hb, (at.meta >> DM_REXP_SHIFT) & 7, dis, ch >= 0 && at.idx != ch, g.dn, at.rv, at.rv2, rvh,
-                        an);
+                if (ANG)
+                    angular(hb, (at.meta >> DM_REXP_SHIFT) & 7, dis, ch >= 0 && at.idx != ch, g.dn, at.rv, at.rv2,
+                            rvh, an);
+                else
+                    ang_plain(an);
                 R G_x = 0, G_racc = 0, G_rdon = 0, G_H = 0;
                 pair_bwd<R, MS, MM>(a, vdw, g, at, an, gs, amin, amax, G_x, G_racc, G_rdon, G_H, G_q);
                 R g_dn[3] = {0, 0, 0};
-                angular_bwd(hb, dis, an, G_racc, G_rdon, G_H, g.dn, at.rv, at.rv2, rvh, g_dn, g_rv, g_rv2, g_rvh);
+                if (ANG)
+                    angular_bwd(hb, dis, an, G_racc, G_rdon, G_H, g.dn, at.rv, at.rv2, rvh, g_dn, g_rv, g_rv2,
+                                g_rvh);
                 geom_bwd(g, G_x, g_dn, g_d);
             }
             // the candidate is the same for the whole warp: reduce, one lane adds
@@ -344,8 +352,8 @@ k_near_lin_adj(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restric
             const R sx = warp_sum(g_d[0]), sy = warp_sum(g_d[1]), sz = warp_sum(g_d[2]);
             const R sq = a.need_sol ? warp_sum(G_q) : (R)0;
             R sr[3] = {0, 0, 0}, sr2[3] = {0, 0, 0};
-            const bool has_rv = hb == 2 || hb == 4 || hb == 5;
-            const bool has_rv2 = hb == 5 && !dis;
+            const bool has_rv = ANG && (hb == 2 || hb == 4 || hb == 5);
+            const bool has_rv2 = ANG && hb == 5 && !dis;
             if (has_rv)
                 for (int i = 0; i < 3; i++) sr[i] = warp_sum(g_rv[i]);
             if (has_rv2)
@@ -425,6 +433,9 @@ cudaError_t launch_near_lin(bool fp64, const DiffArgs &a, const void *vdw, const
     if (fp64)
         k_near_lin<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<double> *)vdw, (const R2<double> *)sol, (double *)maps, ch, mmarg);
+    else if (lean && !a.need_ang)
+        k_near_lin<float, DF_LEAN_S, 0, 3, false><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (float *)maps, ch, mmarg);
     else if (mid && !lean)
         k_near_lin<float, DF_LEAN_S, DF_MID_MM, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<float> *)vdw, (const R2<float> *)sol, (float *)maps, ch, mmarg);
@@ -446,6 +457,9 @@ cudaError_t launch_near_lin_adj(bool fp64, const DiffArgs &a, const void *vdw, c
     if (fp64)
         k_near_lin_adj<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<double> *)vdw, (const R2<double> *)sol, (const double *)g_maps, ch, mmarg, g);
+    else if (lean && !a.need_ang)
+        k_near_lin_adj<float, DF_LEAN_S, 0, 3, false><<<brick_grid(a), DF_THREADS, 0, s>>>(
+            a, (const R2<float> *)vdw, (const R2<float> *)sol, (const float *)g_maps, ch, mmarg, g);
     else if (mid && !lean)
         k_near_lin_adj<float, DF_LEAN_S, DF_MID_MM, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<float> *)vdw, (const R2<float> *)sol, (const float *)g_maps, ch, mmarg, g);

@@ -43,13 +43,20 @@ template <class R> struct Ang {
 // hb: receptor hbond class; dis: disorder flag; ramp: Hramp applies (the
 // point's closest DS/D1 atom exists and is not this atom).
 // dn = (atom - point)/r; rvh = bond vector of the point's closest DS/D1 atom.
+// The factors of a pair without directional terms: all 1, no partials.
 template <class R>
-DF_HD void angular(int hb, int rexp, bool dis, bool ramp, const R dn[3], const R rv[3], const R rv2[3],
-                   const R rvh[3], Ang<R> &o)
+DF_HD void ang_plain(Ang<R> &o)
 {
     o.racc = R(1); o.rdon = R(1); o.H = R(1);
     o.dacc_c = R(0); o.ddon_c = R(0); o.ddon_t0 = R(0); o.ddon_ti = R(0); o.dH_ct = R(0);
     o.cr[0] = o.cr[1] = o.cr[2] = R(0); o.rdi = R(0); o.tin = R(0); o.rd_clamped = true;
+}
+
+template <class R>
+DF_HD void angular(int hb, int rexp, bool dis, bool ramp, const R dn[3], const R rv[3], const R rv2[3],
+                   const R rvh[3], Ang<R> &o)
+{
+    ang_plain(o);
     if (hb != 2 && hb != 4 && hb != 5) return;
     const R c = -(dn[0] * rv[0] + dn[1] * rv[1] + dn[2] * rv[2]);
     if (hb == 2) {  // D1 (main.cpp:3075-3132)
@@ -404,9 +411,12 @@ DF_HD void pair_bwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
     const R solv = at.solpar + qasp * ab(at.q);
     const R sgnq = at.q > R(0) ? R(1) : (at.q < R(0) ? R(-1) : R(0));
     const R dsol_x = g.dw * g.sol + g.w * g.dsol;  // d (w sol) / d x
+    const R2<R> *row = vdw + ((size_t)type * AG_NEINT + g.b) * a.tab_stride;
+    R2<R> tp[2];  // table entries of slots s & ~1 and (s & ~1) + 1
 #pragma unroll
     for (int s = 0; s < MS; s++) {
         if (s >= a.n_slots) break;
+        if ((s & 1) == 0) load_row<R, 2>(row + s, a.n_slots - s, tp);
         const int kind = a.slot_kind[s];
         const R gsl = gs[s];
         if (kind == DK_D) {
@@ -427,7 +437,7 @@ DF_HD void pair_bwd(const DiffArgs &a, const R2<R> *vdw, const Geom<R> &g, const
                 }
                 if (gv != R(0)) {
                     Term<R> t;
-                    term(a, vdw, act, vdw[((size_t)type * AG_NEINT + g.b) * a.tab_stride + s], s, g, an, t);
+                    term(a, vdw, act, tp[s & 1], s, g, an, t);
                     G_x += gv * (g.dw * t.v + g.w * t.dx);
                     G_racc += gv * g.w * t.dracc;
                     G_rdon += gv * g.w * t.drdon;
