@@ -210,7 +210,8 @@ template <class R> __device__ __forceinline__ R covalent_value(const DiffArgs &a
 // holds DF_MAXS / DF_MAXMM; map sets of at most DF_LEAN_S slots without
 // H-bond min/max (Vina maps, plain AD4 subsets) take the lean one, whose
 // registers leave room for 3 resident CTAs per SM.  ANG = false: no slot uses
-// the directional factors (DiffArgs::need_ang), so none are evaluated.
+// the directional factors (DiffArgs::need_ang), so none are evaluated; the
+// lean angle-free kernels fit 64 registers and run 4 CTAs per SM.
 template <class R, int MS, int MM, int MINB, bool ANG = true>
 __global__ void __launch_bounds__(DF_THREADS, MINB)
 k_near_lin(DiffArgs a, const R2<R> *__restrict__ vdw, const R2<R> *__restrict__ sol, R *__restrict__ maps,
@@ -434,7 +435,7 @@ cudaError_t launch_near_lin(bool fp64, const DiffArgs &a, const void *vdw, const
         k_near_lin<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<double> *)vdw, (const R2<double> *)sol, (double *)maps, ch, mmarg);
     else if (lean && !a.need_ang)
-        k_near_lin<float, DF_LEAN_S, 0, 3, false><<<brick_grid(a), DF_THREADS, 0, s>>>(
+        k_near_lin<float, DF_LEAN_S, 0, 4, false><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<float> *)vdw, (const R2<float> *)sol, (float *)maps, ch, mmarg);
     else if (mid && !lean)
         k_near_lin<float, DF_LEAN_S, DF_MID_MM, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
@@ -458,7 +459,7 @@ cudaError_t launch_near_lin_adj(bool fp64, const DiffArgs &a, const void *vdw, c
         k_near_lin_adj<double, DF_MAXS, DF_MAXMM, 1><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<double> *)vdw, (const R2<double> *)sol, (const double *)g_maps, ch, mmarg, g);
     else if (lean && !a.need_ang)
-        k_near_lin_adj<float, DF_LEAN_S, 0, 3, false><<<brick_grid(a), DF_THREADS, 0, s>>>(
+        k_near_lin_adj<float, DF_LEAN_S, 0, 4, false><<<brick_grid(a), DF_THREADS, 0, s>>>(
             a, (const R2<float> *)vdw, (const R2<float> *)sol, (const float *)g_maps, ch, mmarg, g);
     else if (mid && !lean)
         k_near_lin_adj<float, DF_LEAN_S, DF_MID_MM, 3><<<brick_grid(a), DF_THREADS, 0, s>>>(
