@@ -10,43 +10,15 @@ except at points the oracle flags as FP64-ambiguous."""
 import numpy as np
 import pytest
 
-from conftest import make_case, tolerance_ok
+from conftest import fuzz_config, make_case, tolerance_ok
 
 pytestmark = pytest.mark.gpu
-
-LIGANDS = ["A", "C", "HD", "N", "NA", "OA", "SA", "S", "F", "Cl"]
-
-
-def _config(seed):
-    rng = np.random.default_rng(1000 + seed)
-    n_atoms = int(rng.integers(80, 1600))
-    # the generator's density (0.0262 atoms/A^3) or up to 2x sparser
-    radius = 45.0 * (n_atoms / 10000.0) ** (1.0 / 3.0) * float(rng.uniform(1.0, 1.26))
-    npts = tuple(int(v) for v in rng.integers(2, 24, 3))
-    spacing = float(rng.choice([0.2, 0.3, 0.375, 0.5, 0.8]))
-    types = sorted(rng.choice(LIGANDS, int(rng.integers(1, 7)), replace=False).tolist(), key=LIGANDS.index)
-    pre, extra = [], []
-    if rng.random() < 0.4:
-        pre.append("disorder_h")
-    if rng.random() < 0.3:
-        pre.append("separate_desolvation_maps")
-    if rng.random() < 0.3:
-        extra.append(f"qasp {rng.uniform(0.005, 0.02):.4f}")
-    if rng.random() < 0.25:
-        extra.append("covalentmap 1.5 1000.0 1.0 -1.5 2.0")
-    kw = dict(n_atoms=n_atoms, npts=npts, seed=int(seed), radius=radius, spacing=spacing, ligand_types=types,
-              smooth=float(rng.choice([0.0, 0.25, 0.5, 1.0])),
-              dielectric=float(rng.choice([-0.1465, -0.1465, 4.0, 40.0])),
-              elecmap=bool(rng.random() < 0.85), dsolvmap=bool(rng.random() < 0.85),
-              pre_lines=pre, extra_lines=extra)
-    return kw
-
 
 @pytest.mark.parametrize("seed", range(12))
 def test_random_configuration_against_oracle(tmp_path, gpu_ctx, seed):
     from autogrid_b200 import AutoGridError
     from oracle.oracle import oracle_points
-    kw = _config(seed)
+    kw = fuzz_config(seed)
     args = (kw.pop("n_atoms"), kw.pop("npts"))
     common = dict(seed=kw.pop("seed"), radius=kw.pop("radius"))
     try:
@@ -65,7 +37,7 @@ def test_random_configuration_against_oracle(tmp_path, gpu_ctx, seed):
     amb = flags[None, :] != 0
     m32 = gpu_ctx.compute(prob, "fp32").reshape(prob.n_maps, -1)[:, pts].astype(np.float64)
     ok = tolerance_ok(m32, ref) | amb
-    assert ok.all(), f"{int((~ok).sum())} FP32 values off; config {_config(seed)}"
+    assert ok.all(), f"{int((~ok).sum())} FP32 values off; config {fuzz_config(seed)}"
     m64 = gpu_ctx.compute(prob, "fp64").reshape(prob.n_maps, -1)[:, pts]
     ok = (np.abs(m64 - ref) <= 1e-9 * np.maximum(1.0, np.abs(ref))) | amb
-    assert ok.all(), f"{int((~ok).sum())} FP64 values off; config {_config(seed)}"
+    assert ok.all(), f"{int((~ok).sum())} FP64 values off; config {fuzz_config(seed)}"

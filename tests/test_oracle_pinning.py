@@ -7,7 +7,8 @@ that builds its input -- against the reference itself:
     nbp_r_eps / nbp_coeffs overrides, odd npts and a single-point grid;
   * the reference test-suite's golden maps Tests/py_hsg1_sm.*.map, with the
     reference's own comparison rule (test_autogrid4.py:157-186);
-  * live runs of oracle/_ref/autogrid4_fullprec on the reference's test inputs.
+  * live runs of oracle/_ref/autogrid4_fullprec on the reference's test inputs
+    and on seeded random configurations (conftest.fuzz_config).
 """
 import os
 import shutil
@@ -17,7 +18,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from conftest import REFERENCE, ROOT
+from conftest import REFERENCE, ROOT, fuzz_config
 
 GOLDEN = sorted((ROOT / "tests" / "golden").glob("*.npz"))
 
@@ -123,3 +124,57 @@ def test_oracle_vs_live_reference(stem, tmp_path, built):
         ref = read_map(ref_dir / f)
         ok = full_precision_ok(got[i], ref)
         assert ok.all(), f"{stem} {f}: max |d| {np.abs(got[i] - ref).max()}"
+
+
+def _map_files(gpf_text):
+    return [ln.split()[1] for ln in gpf_text.splitlines()
+            if ln.split() and ln.split()[0] in ("map", "elecmap", "dsolvmap")]
+
+
+@needs_reference
+@pytest.mark.parametrize("seed", range(12))
+def test_oracle_vs_live_reference_random(seed, tmp_path, built):
+    """The seeded random configurations of the GPU fuzz test through the
+    reference's full-precision build: front end + oracle equal its maps at
+    every point.  A configuration the reference rejects (a disorder_h bond
+    overflow, bondmanager.cpp:44-88 via main.cpp:2396-2406) must be rejected by
+    the front end with the same message; it is then drawn without disorder_h."""
+    from autogrid_b200 import AutoGridError, Job, synth
+    from oracle.oracle import REF_FULLPREC_BIN, oracle_points, read_map
+    kw = fuzz_config(seed)
+    rec = synth.make_receptor(kw.pop("n_atoms"), seed=kw.pop("seed"), radius=kw.pop("radius"),
+                              center=(1.5, -2.25, 3.0))
+    npts = kw.pop("npts")
+
+    def run(stem):
+        spec = synth.GridSpec(npts=npts, **kw)
+        ref_dir, own_dir = tmp_path / f"{stem}_ref", tmp_path / f"{stem}_own"
+        synth.write_case(ref_dir, stem, rec, spec)
+        synth.write_case(own_dir, stem, rec, spec)
+        r = subprocess.run([str(REF_FULLPREC_BIN), "-p", f"{stem}.gpf", "-l", f"{stem}.glg"], cwd=ref_dir,
+                           capture_output=True, text=True)
+        cwd = os.getcwd()
+        os.chdir(own_dir)
+        try:
+            prob, err = Job(f"{stem}.gpf", f"{stem}.glg").problem(), None
+        except AutoGridError as e:
+            prob, err = None, e
+        finally:
+            os.chdir(cwd)
+        return ref_dir, r, prob, err
+
+    ref_dir, r, prob, err = run("f")
+    if r.returncode != 0:
+        said = r.stdout + r.stderr + (ref_dir / "f.glg").read_text(errors="replace")
+        assert "could not add bond" in said, said[-400:]
+        assert err is not None and "could not add bond" in err.message
+        kw["pre_lines"] = [ln for ln in kw["pre_lines"] if ln != "disorder_h"]
+        ref_dir, r, prob, err = run("g")
+    assert r.returncode == 0 and err is None, (r.stderr[-400:], err)
+    got, _ = oracle_points(prob)
+    files = _map_files(next(ref_dir.glob("*.gpf")).read_text())
+    assert len(files) == prob.n_maps
+    for i, f in enumerate(files):
+        ref = read_map(ref_dir / f)
+        ok = full_precision_ok(got[i], ref)
+        assert ok.all(), f"seed {seed} {f}: {int((~ok).sum())} values off, max |d| {np.abs(got[i] - ref).max()}"
