@@ -6,7 +6,10 @@ included, which the front end truncates as check_size.cpp:79-83 does),
 spacing, the ligand-type subset, smoothing, dielectric (distance-dependent or
 constant), qasp, disorder_h, separate desolvation maps and a covalent map.
 The FP32 path must meet the parity bar and the FP64 twin must agree to 1e-9,
-except at points the oracle flags as FP64-ambiguous."""
+except at points the oracle flags as FP64-ambiguous.  AG_FUZZ_SEEDS sets the
+number of configurations (default 12)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -14,7 +17,7 @@ from conftest import fuzz_config, make_case, tolerance_ok
 
 pytestmark = pytest.mark.gpu
 
-@pytest.mark.parametrize("seed", range(12))
+@pytest.mark.parametrize("seed", range(int(os.environ.get("AG_FUZZ_SEEDS", "12"))))
 def test_random_configuration_against_oracle(tmp_path, gpu_ctx, seed):
     from autogrid_b200 import AutoGridError
     from oracle.oracle import oracle_points

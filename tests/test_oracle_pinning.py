@@ -132,13 +132,14 @@ def _map_files(gpf_text):
 
 
 @needs_reference
-@pytest.mark.parametrize("seed", range(12))
+@pytest.mark.parametrize("seed", range(int(os.environ.get("AG_FUZZ_SEEDS", "12"))))
 def test_oracle_vs_live_reference_random(seed, tmp_path, built):
     """The seeded random configurations of the GPU fuzz test through the
     reference's full-precision build: front end + oracle equal its maps at
     every point.  A configuration the reference rejects (a disorder_h bond
     overflow, bondmanager.cpp:44-88 via main.cpp:2396-2406) must be rejected by
-    the front end with the same message; it is then drawn without disorder_h."""
+    the front end with the same message; it is then drawn without disorder_h.
+    AG_FUZZ_SEEDS sets the number of configurations (default 12; 64 pass)."""
     from autogrid_b200 import AutoGridError, Job, synth
     from oracle.oracle import REF_FULLPREC_BIN, oracle_points, read_map
     kw = fuzz_config(seed)
