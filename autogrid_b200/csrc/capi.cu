@@ -1590,7 +1590,7 @@ ag_status ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *proble
         for (int i = 0; st == AG_OK && i < n; i++) st = ag_batch_download(b, i, maps[i]);
         return st;
     }
-    // Groups of instances, each a batch of its own: group g+1's plans are
+    // Eight groups of instances, each a batch of its own: group g+1's plans are
     // built on the host (uploads on a stream of their own) while group g's
     // graph runs on the context's stream, and each group's maps are copied
     // back on the copy stream as soon as its graph is done.  Groups take the
@@ -1614,7 +1614,7 @@ ag_status ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *proble
         return (double)p->n1[0] * p->n1[1] * p->n1[2] * (double)(p->n_atoms + 64);
     };
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
-    const int G = 4;
+    const int G = std::min(8, n);
     std::vector<std::vector<int>> groups(G);
     for (int k = 0; k < n; k++) groups[k % G].push_back(order[k]);
     cudaStream_t us = nullptr;

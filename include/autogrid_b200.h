@@ -310,7 +310,7 @@ ag_status    ag_batch_tuning(const ag_batch *batch, ag_tuning *out);
 ag_status    ag_batch_destroy(ag_batch *batch);
 /* One-shot: create, run, download every instance's maps (maps[i] host or
  * device, [n_maps_i][P_i] each), destroy.  From 8 instances on (without
- * autotuning) the instances run as 4 groups, each its own batch: a group's
+ * autotuning) the instances run as 8 groups, each its own batch: a group's
  * plans are built on the host while the previous group computes, and each
  * group's maps are copied back while later groups compute.  Results are those
  * of one batch without autotuning. */
