@@ -67,7 +67,8 @@ class ag_stats(C.Structure):
     _fields_ = [("near_pairs", C.c_int64), ("fp64_fallbacks", C.c_int64), ("far_pairs", C.c_int64),
                 ("gpu_launches", C.c_int32), ("reserved", C.c_int32), ("kernel_ms", C.c_double),
                 ("far_ms", C.c_double), ("text_ms", C.c_double), ("text_bytes", C.c_int64),
-                ("table_ms", C.c_double)]
+                ("table_ms", C.c_double), ("far_edge_pairs", C.c_int64), ("far_fp32_bin_errors", C.c_int64),
+                ("far_fp64_ties", C.c_int64)]
 
 
 class ag_table_params(C.Structure):
@@ -96,6 +97,9 @@ SIGNATURES = {
     "ag_maps_compute_f64": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_void_p]),
     "ag_plan_create": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),
     "ag_plan_run": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ag_plan_run_zslab": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_void_p]),
+    "ag_maps_compute_zslab": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_int32, C.c_int32,
+                                        C.c_void_p]),
     "ag_plan_device_maps": (C.c_void_p, [C.c_void_p]),
     "ag_plan_points": (C.c_size_t, [C.c_void_p]),
     "ag_plan_download": (C.c_int, [C.c_void_p, C.c_void_p]),
@@ -146,6 +150,12 @@ SIGNATURES = {
     "ag_emap_compute_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
                                           C.c_double, C.c_int32, C.c_void_p, C.c_double, C.c_double,
                                           C.c_void_p, C.c_void_p]),
+    # measurement and test helpers (include/autogrid_b200_diag.h)
+    "ag_diag_peak_rates": (C.c_int, [C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                     C.POINTER(C.c_double)]),
+    "ag_diag_rsqrt_error": (C.c_int, [C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_double)]),
+    "ag_diag_far_bins": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.c_int32, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
 }
 
 _lib = None

@@ -277,6 +277,9 @@ class Stats:
     far_ms: float
     text_ms: float = 0.0
     text_bytes: int = 0
+    far_edge_pairs: int = 0
+    far_fp32_bin_errors: int = 0
+    far_fp64_ties: int = 0
 
 
 class Context:
@@ -300,6 +303,20 @@ class Context:
         s = problem.struct()
         fn = self._lib.ag_maps_compute_f64 if prec == _abi.AG_PREC_FP64 else self._lib.ag_maps_compute
         check(fn(self._h, C.byref(s), C.byref(opts), out.ctypes.data_as(C.c_void_p)))
+        return out
+
+    def compute_zslab(self, problem: Problem, z0: int, z1: int, out: np.ndarray | None = None) -> np.ndarray:
+        """FP32 maps of grid planes [z0, z1) (ag_maps_compute_zslab); returns
+        [n_out, z1 - z0, n1y, n1x]."""
+        shape = (problem.n_out, int(z1) - int(z0), problem.n1[1], problem.n1[0])
+        if out is None:
+            out = np.empty(shape, dtype=np.float32)
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.shape != shape:
+            raise ValueError(f"out must be a C-contiguous float32 array of shape {shape}")
+        opts = ag_opts(precision=_abi.AG_PREC_FP32, table_mode=_abi.AG_TABLE_NEAREST)
+        s = problem.struct()
+        check(self._lib.ag_maps_compute_zslab(self._h, C.byref(s), C.byref(opts), int(z0), int(z1),
+                                              out.ctypes.data_as(C.c_void_p)))
         return out
 
     def compute_text(self, problem: Problem, precision: str = "fp32") -> MapText:
@@ -326,7 +343,23 @@ class Context:
         st = ag_stats()
         check(self._lib.ag_context_stats(self._h, C.byref(st)))
         return Stats(st.near_pairs, st.fp64_fallbacks, st.far_pairs, st.gpu_launches, st.kernel_ms, st.far_ms,
-                     st.text_ms, st.text_bytes)
+                     st.text_ms, st.text_bytes, st.far_edge_pairs, st.far_fp32_bin_errors, st.far_fp64_ties)
+
+    def far_bins(self, problem: Problem, points) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+        """Far-field table bins of the given grid points (linear indices, X
+        fastest) against every atom, with the far kernel's arithmetic
+        (ag_diag_far_bins): (bin_used, bin_fp32, flags), each [n_points, n_atoms].
+        bin_used is -1 for pairs nearer than 8 A (the near-field kernel's)."""
+        pts = np.ascontiguousarray(points, dtype=np.int64)
+        shape = (pts.size, problem.n_atoms)
+        used = np.empty(shape, np.int32)
+        fp32 = np.empty(shape, np.int32)
+        flags = np.empty(shape, np.int32)
+        s = problem.struct()
+        check(self._lib.ag_diag_far_bins(self._h, C.byref(s), int(pts.size), pts.ctypes.data_as(C.c_void_p),
+                                         used.ctypes.data_as(C.c_void_p), fp32.ctypes.data_as(C.c_void_p),
+                                         flags.ctypes.data_as(C.c_void_p)))
+        return used, fp32, flags
 
     def plan(self, problem: Problem, serial: bool = False) -> "Plan":
         """Device-resident plan; serial=True runs every kernel in sequence on one
@@ -472,6 +505,10 @@ class Plan:
 
     def run(self, stream: int | None = None) -> None:
         check(self._lib.ag_plan_run(self._h, C.c_void_p(stream) if stream else None))
+
+    def run_zslab(self, z0: int, z1: int, stream: int | None = None) -> None:
+        """Run grid planes [z0, z1) only (ag_plan_run_zslab)."""
+        check(self._lib.ag_plan_run_zslab(self._h, int(z0), int(z1), C.c_void_p(stream) if stream else None))
 
     def device_maps_ptr(self) -> int:
         return int(self._lib.ag_plan_device_maps(self._h) or 0)

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "autogrid_b200.h"
+#include "autogrid_b200_diag.h"
 #include "kernels/kernels.h"
 #include "kernels/maptext.h"
 #include "kernels/tables.h"
@@ -135,6 +136,23 @@ struct BufferSet {
     }
 };
 
+// Makes a device current for the scope of an entry point and gives the
+// caller's current device back on return.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit DeviceGuard(int device)
+    {
+        err = cudaGetDevice(&prev);
+        if (err == cudaSuccess && prev != device) err = cudaSetDevice(device);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
 ag_status cuda_fail(cudaError_t e, const char *what)
 {
     set_last_error(std::string(what) + ": " + cudaGetErrorString(e));
@@ -153,6 +171,13 @@ ag_status invalid(const std::string &m)
     return AG_ERR_INVALID;
 }
 
+// Device statistics counters of a context (and of a batch):
+//   context: [0] near pairs, [1] FP64 fallbacks, [2..4] far-field bin guard
+//            (FarArgs::edge_counters);
+//   batch:   [0] far work units, [1] near work units, [2..3] near statistics,
+//            [4..6] far-field bin guard.
+constexpr int kCounters = 8;
+
 // One-shot calls: z-slab height of the copy/compute pipeline (whole far-field
 // frames and near-field brick rows) and the most slabs one call uses.
 constexpr int kSlabZ = 16;
@@ -170,6 +195,7 @@ void slab_range(const DevProblem &d, int k, int *z0, int *z1)
 
 struct ag_context {
     int device = 0;
+    int sms = 148;  // streaming multiprocessors of the device (queried at creation)
     cudaStream_t stream = nullptr;
     // the far-field kernel runs on `side`, concurrently with the near-field
     // kernel, forked from and joined back to the caller's stream by events
@@ -332,7 +358,9 @@ cudaError_t upload(BufferSet *b, const char *name, const T *src, size_t n, T **d
 // Build the device image of a problem (host work is O(atoms + tables)).
 ag_status launch_far_slab(ag_plan *pl, cudaStream_t s, int k, int nslab);
 
-ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipelined)
+// pipelined: far-field chunking sized per 16-plane slab (one-shot calls and
+// z-slab runs); early_far: with pipelined, also launch far slab 0 from here.
+ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipelined, bool early_far = true)
 {
     ag_status st = validate(p);
     if (st != AG_OK) return st;
@@ -371,8 +399,15 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     }
     std::vector<float> far_tab;
     if (!dev_tables) {
-        far_tab.assign(AG_NDIEL, 0.f);
-        for (int k = AG_NEINT; k < AG_NDIEL; k++) far_tab[k] = (float)(p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal);
+        // [0, NDIEL): the far kernel's table, zero below FAR_BIN0 (those pairs
+        // are the near kernel's); [NDIEL, 2 NDIEL): the whole table, for far
+        // pairs whose exact bin the bin guard finds below FAR_BIN0
+        far_tab.assign(2 * AG_NDIEL, 0.f);
+        for (int k = 0; k < AG_NDIEL; k++) {
+            const float f = (float)(p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal);
+            far_tab[AG_NDIEL + k] = f;
+            if (k >= AG_NEINT) far_tab[k] = f;
+        }
         // a constant dielectric needs no far-field table gather
         if (!p->dddiel) {
             pl->far_mode = FAR_TAB_CONST;
@@ -385,7 +420,8 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
                                        : (long long)frames_x(d.n1x) * frames_y(d.n1y) * frames_z(d.n1z);
     const int tile = 512;
     if (p->elec_map >= 0 && N > 0) {
-        const long long target = pipelined ? 148LL * 3 * 3 : 148LL * 3 * 8;
+        const long long sms = pl->ctx ? pl->ctx->sms : 148;
+        const long long target = pipelined ? sms * 3 * 3 : sms * 3 * 8;
         int nch = (int)std::max(1LL, (target + frames - 1) / frames);
         nch = std::min(nch, (N + tile - 1) / tile);
         pl->chunk_atoms = ((N + nch - 1) / nch + tile - 1) / tile * tile;
@@ -408,10 +444,10 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     AGB_CK(upload(B, "qw", qw.data(), N, &pl->qw, s, acc));
     if (!dev_tables) AGB_CK(upload(B, "far_tab", far_tab.data(), far_tab.size(), &pl->far_tab, s, acc));
     pl->far_early = 0;
-    if (pipelined && !dev_tables && pl->far_partial && d.elec_map >= 0) {
+    if (pipelined && early_far && !dev_tables && pl->far_partial && d.elec_map >= 0) {
         // the run's statistics start here: counters cleared, then ev0, then the fork
         ag_context *c = pl->ctx;
-        AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+        AGB_CK(cudaMemsetAsync(c->d_counters, 0, kCounters * sizeof(unsigned long long), s));
         AGB_CK(cudaEventRecord(c->ev0, s));
         ag_status st = launch_far_slab(pl, s, 0, slab_count(d));
         if (st != AG_OK) return st;
@@ -614,7 +650,7 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
         void *vv;
         AGB_CK(upload(B, "colmap", colmap.data(), colmap.size(), &dcol, s, acc));
         AGB_CK(B->ensure("vdwT", (size_t)nT * AG_NEINT * pl->mpad * sizeof(float), &vv)); pl->vdwT = (float *)vv;
-        AGB_CK(B->ensure("far_tab", AG_NDIEL * sizeof(float), &vv)); pl->far_tab = (float *)vv;
+        AGB_CK(B->ensure("far_tab", 2 * AG_NDIEL * sizeof(float), &vv)); pl->far_tab = (float *)vv;
         AGB_CK(B->ensure("etab", AG_NDIEL * sizeof(float), &vv)); pl->etab = (float *)vv;
         AGB_CK(B->ensure("solf", AG_NDIEL * sizeof(float), &vv)); pl->solf = (float *)vv;
         AGB_CK(B->ensure("sol_fn", AG_NDIEL * sizeof(double), &vv)); dsolfn = (double *)vv;
@@ -670,6 +706,22 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     return AG_OK;
 }
 
+// Bin-guard multipliers of the far kernel for a grid spacing (in bins):
+// far_edge_multipliers with the largest frame-relative point coordinate and
+// whether every frame point coordinate il*spacing_adiv is an exact float.
+// rsqrt.approx.f32 is taken at 2.5 * 2^-24 relative error (PTX ISA:
+// 2^-22.9 = 2.14 * 2^-24; checked on the device by ag_diag_rsqrt_error).
+void far_guard(double spacing_adiv, float *lo, float *hi)
+{
+    bool exact = true;
+    for (int il = 0; il < FRAME_X; il++) {
+        const double v = (double)il * spacing_adiv;
+        exact &= std::fma((double)il, spacing_adiv, -v) == 0.0 && (double)(float)v == v;
+    }
+    const double px = (FRAME_X - 1) * spacing_adiv, pyz = (FRAME_Y - 1) * spacing_adiv;
+    far_edge_multipliers(std::sqrt(px * px + 2 * pyz * pyz), exact, 2.5, lo, hi);
+}
+
 FarArgs far_args(const ag_plan *pl)
 {
     const DevProblem &d = pl->dp;
@@ -683,6 +735,9 @@ FarArgs far_args(const ag_plan *pl)
     a.nfx = frames_x(d.n1x); a.nfy = frames_y(d.n1y); a.nfz = frames_z(d.n1z);
     a.tab_mode = pl->far_mode;
     a.tab_const = pl->far_const;
+    a.tab_full = pl->far_tab ? pl->far_tab + AG_NDIEL : nullptr;
+    far_guard(a.spacing_adiv, &a.edge_lo, &a.edge_hi);
+    a.edge_counters = pl->ctx ? pl->ctx->d_counters + 2 : nullptr;
     return a;
 }
 
@@ -756,13 +811,80 @@ ag_status enqueue_slabs(ag_plan *pl, cudaStream_t s, int nslab, int &launches)
 }
 
 
+// A z-slab [z0, z1) of the grid is a shard of the map set: its points need
+// every atom but no other plane.  z0 is a multiple of FRAME_Z (whole far-field
+// frame rows, which hold whole near-field brick rows) and z1 one too or n1z.
+ag_status check_zslab(const ag_problem *p, int z0, int z1)
+{
+    if (!p) return invalid("null problem");
+    const int n1z = p->n1[2];
+    if (z0 < 0 || z1 > n1z || z0 >= z1) return invalid("z-slab outside the grid or empty");
+    if (z0 % FRAME_Z != 0 || (z1 != n1z && z1 % FRAME_Z != 0))
+        return invalid("z-slab bounds must be multiples of 8 planes (or the last plane)");
+    return AG_OK;
+}
+
+// FP32 kernels of planes [z0, z1) only (check_zslab), on s with the far field
+// on the side stream as run_plan; the maps of those planes land at their
+// places in the plan's full-grid buffers.  Each point's work is the one-shot
+// call's, so the planes equal it bit for bit when the plan has its chunking.
+ag_status run_plan_zrange(ag_plan *pl, cudaStream_t s, int z0, int z1)
+{
+    ag_context *c = pl->ctx;
+    const DevProblem &d = pl->dp;
+    int launches = 0;
+    AGB_CK(cudaMemsetAsync(c->d_counters, 0, kCounters * sizeof(unsigned long long), s));
+    AGB_CK(cudaEventRecord(c->ev0, s));
+    const bool far = d.elec_map >= 0 && pl->n_chunks > 0;
+    const bool last = z1 == d.n1z;
+    if (far) {
+        AGB_CK(cudaEventRecord(c->fork, s));
+        AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
+        AGB_CK(cudaEventRecord(c->evf0, c->side));
+        AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, z0 / FRAME_Z, last ? -1 : z1 / FRAME_Z));
+        AGB_CK(cudaEventRecord(c->evf1, c->side));
+        AGB_CK(cudaEventRecord(c->join, c->side));
+        launches++;
+    }
+    if (pl->any_cov) {
+        AGB_CK(launch_covalent(d, pl->cov, s));
+        launches++;
+    }
+    if (pl->floating || pl->constriction) {
+        const size_t P = (size_t)d.P, f = (size_t)d.n_maps * P, cc = f + (size_t)pl->floating * P;
+        AGB_CK(launch_distance_maps(d, pl->constriction_cutoff, pl->floating ? pl->maps32 + f : nullptr,
+                                    pl->constriction ? pl->maps32 + cc : nullptr, nullptr, nullptr, s));
+        launches++;
+    }
+    const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || d.elec_map >= 0;
+    if (need_near)
+        for (const NearGroup &g : pl->groups) {
+            AGB_CK(launch_near(false, d, g, near_ptrs(pl, c->d_counters), 0, s, z0 / 4, last ? -1 : z1 / 4));
+            launches++;
+        }
+    if (far) {
+        const long long plane = (long long)d.n1x * d.n1y;
+        const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * d.P};
+        AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
+        AGB_CK(launch_emap_reduce_range(r, (long long)z0 * plane, (long long)z1 * plane, s));
+        launches++;
+    }
+    AGB_CK(cudaEventRecord(c->ev1, s));
+    pl->last_launches = launches;
+    c->pending = true;
+    c->had_far = far;
+    c->last_launches = launches;
+    c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)(z1 - z0) * d.n1x * d.n1y * d.n_atoms : 0;
+    return AG_OK;
+}
+
 ag_status run_plan(ag_plan *pl, cudaStream_t s)
 {
     ag_context *c = pl->ctx;
     const DevProblem &d = pl->dp;
     const bool exact = pl->opts.precision == AG_PREC_FP64;
     int launches = 0;
-    AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+    AGB_CK(cudaMemsetAsync(c->d_counters, 0, kCounters * sizeof(unsigned long long), s));
     AGB_CK(cudaEventRecord(c->ev0, s));
     const bool far = !exact && d.elec_map >= 0 && pl->n_chunks > 0;
     if (d.elec_map >= 0 && exact) {
@@ -827,10 +949,13 @@ ag_status settle_stats(ag_context *c)
     float ms = 0.f, fms = 0.f;
     AGB_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     if (c->had_far) AGB_CK(cudaEventElapsedTime(&fms, c->evf0, c->evf1));
-    unsigned long long h[4] = {0, 0, 0, 0};
+    unsigned long long h[kCounters] = {};
     AGB_CK(cudaMemcpy(h, c->d_counters, sizeof h, cudaMemcpyDeviceToHost));
     c->stats.near_pairs = (int64_t)h[0];
     c->stats.fp64_fallbacks = (int64_t)h[1];
+    c->stats.far_edge_pairs = (int64_t)h[2];
+    c->stats.far_fp32_bin_errors = (int64_t)h[3];
+    c->stats.far_fp64_ties = (int64_t)h[4];
     c->stats.far_pairs = c->last_far_pairs;
     c->stats.gpu_launches = c->last_launches;
     c->stats.kernel_ms = ms;
@@ -842,7 +967,8 @@ ag_status settle_stats(ag_context *c)
 ag_status finish_stats(ag_plan *pl) { return settle_stats(pl->ctx); }
 
 ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out,
-                    Arena *arena = nullptr, bool pipelined = false, cudaStream_t stream = nullptr);
+                    Arena *arena = nullptr, bool pipelined = false, cudaStream_t stream = nullptr,
+                    bool early_far = true);
 
 }  // namespace
 
@@ -862,7 +988,7 @@ struct ag_batch {
     FarArgs *d_far = nullptr;
     NearInst *d_near = nullptr;
     long long *d_far_begin = nullptr, *d_near_begin = nullptr;
-    unsigned long long *d_counters = nullptr;  // [0] far units, [1] near units, [2..3] near statistics
+    unsigned long long *d_counters = nullptr;  // kCounters: see its definition
     ag_tuning tune{};
     int far_ctas_per_sm = 3, near_ctas_per_sm = 3;  // resident CTAs per SM of the persistent kernels
     cudaGraph_t graph = nullptr;
@@ -915,7 +1041,7 @@ ag_status batch_launch(ag_batch *b, cudaStream_t s, int tile, int shape, cudaEve
 {
     ag_context *c = b->ctx;
     const bool far = b->far_begin.back() > 0;
-    AGB_CK(cudaMemsetAsync(b->d_counters, 0, 4 * sizeof(unsigned long long), s));
+    AGB_CK(cudaMemsetAsync(b->d_counters, 0, kCounters * sizeof(unsigned long long), s));
     if (e0) AGB_CK(cudaEventRecord(e0, s));
     cudaStream_t fs = s;
     if (far && concurrent) {
@@ -1013,7 +1139,7 @@ ag_status batch_autotune(ag_batch *b)
 }
 
 ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool own, ag_plan **out, Arena *arena,
-                    bool pipelined, cudaStream_t stream)
+                    bool pipelined, cudaStream_t stream, bool early_far)
 {
     if (!ctx || !p || !out) return invalid("null argument");
     ag_opts opts{};
@@ -1034,7 +1160,7 @@ ag_status make_plan(ag_context *ctx, const ag_problem *p, const ag_opts *o, bool
     } else {
         pl->bufs = &ctx->pool;
     }
-    ag_status st = build_plan(pl.get(), p, stream ? stream : ctx->stream, pipelined);
+    ag_status st = build_plan(pl.get(), p, stream ? stream : ctx->stream, pipelined, early_far);
     if (st != AG_OK) return st;
     *out = pl.release();
     return AG_OK;
@@ -1074,8 +1200,13 @@ ag_status ag_context_create(int32_t device, ag_context **out)
     AGB_CK(cudaEventCreate(&c->ev1));
     AGB_CK(cudaEventCreate(&c->evf0));
     AGB_CK(cudaEventCreate(&c->evf1));
-    AGB_CK(cudaMalloc(&c->d_counters, 4 * sizeof(unsigned long long)));
+    AGB_CK(cudaMalloc(&c->d_counters, kCounters * sizeof(unsigned long long)));
+    AGB_CK(cudaMemset(c->d_counters, 0, kCounters * sizeof(unsigned long long)));
     for (cudaEvent_t &e : c->tev) AGB_CK(cudaEventCreate(&e));
+    // shared-memory limits of the far kernels on this device, set here (once
+    // per context, outside any stream capture) rather than at launch
+    AGB_CK(prepare_far_kernels());
+    AGB_CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     *out = c.release();
     return AG_OK;
 }
@@ -1129,7 +1260,7 @@ static ag_status run_plan_pipelined(ag_plan *pl, void *out, size_t n_out)
     const long long plane = (long long)d.n1x * d.n1y;
     int launches = 0;
     if (pl->far_early == 0) {  // else the plan cleared them and started the clock
-        AGB_CK(cudaMemsetAsync(c->d_counters, 0, 4 * sizeof(unsigned long long), s));
+        AGB_CK(cudaMemsetAsync(c->d_counters, 0, kCounters * sizeof(unsigned long long), s));
         AGB_CK(cudaEventRecord(c->ev0, s));
     }
     if (pl->any_cov) {
@@ -1200,6 +1331,33 @@ ag_status ag_maps_compute_f64(ag_context *ctx, const ag_problem *problem, const 
     return compute_common(ctx, problem, opts, maps, 8);
 }
 
+ag_status ag_maps_compute_zslab(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, int32_t z0,
+                                int32_t z1, float *maps)
+{
+    if (!maps) return invalid("null maps");
+    if (opts && opts->precision != AG_PREC_FP32) return invalid("ag_maps_compute_zslab runs the FP32 path");
+    ag_status st = check_zslab(problem, z0, z1);
+    if (st != AG_OK) return st;
+    if (!ctx) return invalid("null context");
+    DeviceGuard dg(ctx->device);
+    AGB_CK(dg.err);
+    ag_plan *pl = nullptr;
+    // the one-shot call's far-field chunking (bit-identical planes), no early launch
+    st = make_plan(ctx, problem, opts, false, &pl, nullptr, problem->n1[2] > kSlabZ, nullptr, false);
+    if (st != AG_OK) return st;
+    std::unique_ptr<ag_plan> guard(pl);
+    st = run_plan_zrange(pl, ctx->stream, z0, z1);
+    if (st != AG_OK) return st;
+    const DevProblem &d = pl->dp;
+    const size_t n_out = (size_t)problem->n_maps + pl->floating + pl->constriction;
+    const size_t plane = (size_t)d.n1x * d.n1y, rows = (size_t)(z1 - z0) * plane;
+    AGB_CK(cudaMemcpy2DAsync(maps, rows * sizeof(float), pl->maps32 + (size_t)z0 * plane, (size_t)d.P * sizeof(float),
+                             rows * sizeof(float), n_out, cudaMemcpyDefault, ctx->stream));
+    AGB_CK(cudaStreamSynchronize(ctx->stream));
+    return finish_stats(pl);
+}
+
+
 ag_status ag_plan_create(ag_context *ctx, const ag_problem *problem, const ag_opts *opts, ag_plan **out)
 {
     ag_opts o{};
@@ -1212,11 +1370,72 @@ ag_status ag_plan_create(ag_context *ctx, const ag_problem *problem, const ag_op
     return AG_OK;
 }
 
+// Far-field bins of listed points against every atom (autogrid_b200_diag.h).
+static ag_status far_bins_diag(ag_context *ctx, const ag_problem *problem, int32_t n_points, const int64_t *points,
+                               int32_t *bin_used, int32_t *bin_fp32, int32_t *flags)
+{
+    if (!ctx || !problem || (n_points > 0 && (!points || !bin_used || !bin_fp32 || !flags)))
+        return invalid("null argument");
+    if (n_points < 0) return invalid("negative point count");
+    const long long n = (long long)n_points * std::max(problem->n_atoms, 0);
+    if (n > (1LL << 27)) {
+        set_last_error("ag_diag_far_bins: at most 2^27 (point, atom) pairs per call");
+        return AG_ERR_TOO_LARGE;
+    }
+    const long long P = (long long)problem->n1[0] * problem->n1[1] * problem->n1[2];
+    for (int32_t i = 0; i < n_points; i++)
+        if (points[i] < 0 || points[i] >= P) return invalid("point index outside the grid");
+    ag_opts o{};
+    ag_plan *pl = nullptr;
+    ag_status st = make_plan(ctx, problem, &o, true, &pl);
+    if (st != AG_OK) return st;
+    std::unique_ptr<ag_plan> hold(pl);
+    if (n == 0) return AG_OK;
+    if (pl->far_mode != FAR_TAB_TABLE || !pl->far_tab) {
+        set_last_error("ag_diag_far_bins: the problem has no far-field table (constant dielectric or no e map)");
+        return AG_ERR_UNSUPPORTED;
+    }
+    cudaStream_t s = ctx->stream;
+    long long *dpts = nullptr;
+    int *dout = nullptr;
+    AGB_CK(cudaMalloc(&dpts, sizeof(long long) * n_points));
+    std::unique_ptr<long long, decltype(&cudaFree)> g1(dpts, &cudaFree);
+    AGB_CK(cudaMalloc(&dout, sizeof(int) * 3 * (size_t)n));
+    std::unique_ptr<int, decltype(&cudaFree)> g2(dout, &cudaFree);
+    AGB_CK(cudaMemcpyAsync(dpts, points, sizeof(long long) * n_points, cudaMemcpyHostToDevice, s));
+    FarArgs a = far_args(pl);
+    a.edge_counters = nullptr;
+    AGB_CK(launch_far_bins_debug(a, dpts, n_points, dout, dout + n, dout + 2 * n, s));
+    AGB_CK(cudaMemcpyAsync(bin_used, dout, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    AGB_CK(cudaMemcpyAsync(bin_fp32, dout + n, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    AGB_CK(cudaMemcpyAsync(flags, dout + 2 * n, sizeof(int) * (size_t)n, cudaMemcpyDeviceToHost, s));
+    AGB_CK(cudaStreamSynchronize(s));
+    return AG_OK;
+}
+
+int ag_diag_far_bins(ag_context *ctx, const ag_problem *problem, int32_t n_points, const int64_t *points,
+                     int32_t *bin_used, int32_t *bin_fp32, int32_t *flags)
+{
+    return (int)far_bins_diag(ctx, problem, n_points, points, bin_used, bin_fp32, flags);
+}
+
 ag_status ag_plan_run(ag_plan *plan, void *stream)
 {
     if (!plan) return invalid("null plan");
     cudaStream_t s = stream ? (cudaStream_t)stream : plan->ctx->stream;
     return run_plan(plan, s);
+}
+
+ag_status ag_plan_run_zslab(ag_plan *plan, int32_t z0, int32_t z1, void *stream)
+{
+    if (!plan) return invalid("null plan");
+    const DevProblem &d = plan->dp;
+    if (z0 < 0 || z1 > d.n1z || z0 >= z1) return invalid("z-slab outside the grid or empty");
+    if (z0 % FRAME_Z != 0 || (z1 != d.n1z && z1 % FRAME_Z != 0))
+        return invalid("z-slab bounds must be multiples of 8 planes (or the last plane)");
+    DeviceGuard dg(plan->ctx->device);
+    AGB_CK(dg.err);
+    return run_plan_zrange(plan, stream ? (cudaStream_t)stream : plan->ctx->stream, z0, z1);
 }
 
 const float *ag_plan_device_maps(const ag_plan *plan) { return plan ? plan->maps32 : nullptr; }
@@ -1487,8 +1706,9 @@ static ag_status batch_create(ag_context *ctx, const ag_problem *const *problems
     b->d_near = (NearInst *)v;
     AGB_CK(b->bufs.ensure("near_begin", sizeof(long long) * b->near_begin.size(), &v));
     b->d_near_begin = (long long *)v;
-    AGB_CK(b->bufs.ensure("counters", 4 * sizeof(unsigned long long), &v));
+    AGB_CK(b->bufs.ensure("counters", kCounters * sizeof(unsigned long long), &v));
     b->d_counters = (unsigned long long *)v;
+    for (FarArgs &a : b->far) a.edge_counters = b->d_counters + 4;
     AGB_CK(b->bufs.ensure("reduce", sizeof(ReduceInst) * std::max<size_t>(1, b->red.size()), &v));
     b->d_red = (ReduceInst *)v;
     AGB_CK(b->bufs.ensure("reduce_begin", sizeof(long long) * b->red_begin.size(), &v));

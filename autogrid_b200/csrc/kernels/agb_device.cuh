@@ -8,6 +8,7 @@
 // from exactly the same FP32 operations on exactly the same FP32 inputs, so
 // every (point, atom) pair is counted by exactly one of them.
 #pragma once
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -20,6 +21,11 @@ constexpr int FAR_BIN0 = AG_NEINT;          // bins below this belong to the nea
 constexpr float FAR_T0 = (float)AG_NEINT;   // t = A_DIV * r threshold, same meaning
 constexpr float TINY_T2 = 1.0e-20f;         // keeps rsqrt finite for coincident points
 constexpr float FAR_MAX_T = (float)(AG_NDIEL - 1);
+// The guarded far kernel clamps t half a bin past the last table bin, so that
+// both guard bins of a clamped pair are the last bin (the reference clamps
+// the bin, min(lookup(r), NDIEL-1), main.cpp:2956).
+constexpr float FAR_CLAMP_T = (float)(AG_NDIEL - 1) + 0.5f;
+constexpr uint32_t MAGIC_BITS = 0x4B000000u;  // bits of 2^23: bits(2^23 + k) = MAGIC_BITS + k, 0 <= k < 2^23
 
 // Frame origin in bins: ((o - ne) * spacing) * A_DIV, formed like the
 // reference forms a grid coordinate (main.cpp:2859); the scaling by A_DIV = 2^7
@@ -82,8 +88,43 @@ struct FarArgs {
     //   FAR_TAB_CONST  far_tab is one constant (constant dielectric): no gather.
     int tab_mode;
     float tab_const;
+    // Bin-edge guard (FAR_TAB_TABLE): the kernel takes the bins of t*edge_lo
+    // and t*edge_hi, edge_lo/hi = 1 -/+ d with d above the relative error of
+    // the FP32 distance t; pairs whose two bins differ get their bin in FP64
+    // (far_exact_bin).  tab_full [NDIEL]: the table without the zeros below
+    // FAR_BIN0, for pairs whose exact bin is there.
+    float edge_lo, edge_hi;
+    const float *tab_full;
+    // [0] guarded pairs resolved in FP64, [1] of those, pairs whose plain FP32
+    // bin floor(t) was not the exact bin, [2] pairs decided by the reference's
+    // own expression because their FP64 squared distance lies within 1e-12 of
+    // the edge.  May be null (not counted).
+    unsigned long long *edge_counters;
 };
 enum { FAR_TAB_TABLE = 0, FAR_TAB_CONST = 2 };
+
+// Guard multipliers for a grid: the relative error bound of the canonical
+// FP32 distance t of a far pair (t >= FAR_T0 bins), rounded up so that 1 - d
+// and 1 + d are floats.  With D the exact frame-relative distance (bins), A
+// the atom's and P the point's frame-relative coordinates (|A| <= |D| + |P|):
+//   coordinates rounded to FP32 and dx = A - P rounded:
+//       |error vector| <= 2^-24 (|A| + |D| + |P| [P inexact]) <= 2^-24 (2|D| + (1 + [P inexact])|P|)
+//   t2 = dx^2 + (dy^2 + dz^2) by two FMAs: relative 3 * 2^-24, 1.5 * 2^-24 on t
+//   rsqrt.approx: relative rho;  t = t2 * rs rounded: 2^-24
+// so |t/D - 1| <= 2^-24 (4.5 + (1 + [P inexact]) |P|max / FAR_T0) + rho.
+// rho_ulps is rho in units of 2^-24; p_max the largest |P| of a frame point;
+// p_exact whether every frame point coordinate is an exact float.
+__host__ inline void far_edge_multipliers(double p_max, bool p_exact, double rho_ulps, float *lo, float *hi)
+{
+    const double u = 1.0 / 16777216.0;  // 2^-24
+    const double d = u * (4.5 + rho_ulps + (p_exact ? 1.0 : 2.0) * p_max / (double)FAR_T0) * 1.0625;
+    const double kl = std::ceil(d / u), kh = std::ceil(d / (2 * u));
+    *lo = (float)(1.0 - kl * u);        // floats below 1 are spaced 2^-24
+    *hi = (float)(1.0 + kh * 2 * u);    // floats above 1 are spaced 2^-23
+}
+
+// Streaming multiprocessors of the current device (launch sizing).
+int current_device_sms();
 
 // Device image of one problem instance.
 struct DevProblem {

@@ -1,5 +1,6 @@
 // Microbenchmarks for the roofline denominators: MUFU rsqrt rate and FP32 FMA rate.
 #include <algorithm>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "agb_device.cuh"
@@ -38,7 +39,41 @@ __global__ void __launch_bounds__(256) k_peak_ffma(float *out, int iters)
     if (s == 12345.f) out[threadIdx.x] = s;
 }
 
+// Relative error of rsqrt.approx.f32 at every float of [2^lo_exp, 2^hi_exp):
+// the largest |rsqrt(x)*sqrt(x) - 1| (FP64) as order-preserving bits of a
+// non-negative double.
+__global__ void __launch_bounds__(256) k_rsqrt_error(uint32_t bits0, uint32_t n, unsigned long long *max_bits)
+{
+    double worst = 0.0;
+    for (uint32_t i = blockIdx.x * 256u + threadIdx.x; i < n; i += gridDim.x * 256u) {
+        const float x = __uint_as_float(bits0 + i);
+        const double e = fabs((double)rsqrt_approx(x) * sqrt((double)x) - 1.0);
+        worst = fmax(worst, e);
+    }
+    for (int o = 16; o; o >>= 1) worst = fmax(worst, __shfl_xor_sync(0xffffffffu, worst, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(max_bits, (unsigned long long)__double_as_longlong(worst));
+}
+
 }  // namespace agb
+
+extern "C" int ag_diag_rsqrt_error(int32_t device, int32_t lo_exp, int32_t hi_exp, double *max_rel_ulps)
+{
+    if (!max_rel_ulps || lo_exp < -126 || hi_exp > 127 || lo_exp >= hi_exp) return 1;
+    if (cudaSetDevice(device) != cudaSuccess) return 1;
+    unsigned long long *d = nullptr;
+    if (cudaMalloc(&d, sizeof *d) != cudaSuccess) return 1;
+    cudaMemset(d, 0, sizeof *d);
+    const uint32_t b0 = (uint32_t)(lo_exp + 127) << 23, b1 = (uint32_t)(hi_exp + 127) << 23;
+    agb::k_rsqrt_error<<<4096, 256>>>(b0, b1 - b0, d);
+    unsigned long long h = 0;
+    const cudaError_t e = cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess || cudaGetLastError() != cudaSuccess) return 1;
+    double v;
+    std::memcpy(&v, &h, sizeof v);
+    *max_rel_ulps = v * 16777216.0;
+    return 0;
+}
 
 extern "C" int ag_diag_peak_rates(int32_t device, double *rsqrt_per_s, double *fp32_flops_per_s,
                                   double *sm_clock_mhz)

@@ -185,7 +185,7 @@ cudaError_t launch_emap_lin_adj(bool fp64, const DiffArgs &a, const void *eps, c
     if (a.n_atoms == 0 || a.P == 0) return cudaSuccess;
     // about four blocks per SM over (atom blocks x point ranges)
     const int atom_blocks = (a.n_atoms + EL_THREADS - 1) / EL_THREADS;
-    long long ranges = (148LL * 4 + atom_blocks - 1) / atom_blocks;
+    long long ranges = (4LL * current_device_sms() + atom_blocks - 1) / atom_blocks;
     long long ppb = (a.P + ranges - 1) / ranges;
     ppb = ((ppb + EL_TILE - 1) / EL_TILE) * EL_TILE;
     if (ppb < EL_TILE) ppb = EL_TILE;

@@ -34,9 +34,44 @@ __device__ __forceinline__ float lds_f32(uint32_t addr)
     return v;
 }
 
+constexpr int FAR_TIE_FLAG = 1 << 30;
+
 __device__ __forceinline__ void load_far_table(float4 *s_tab4, const float *far_tab)
 {
     for (int i = threadIdx.x; i < AG_NDIEL / 4; i += EF_THREADS) s_tab4[i] = __ldg(((const float4 *)far_tab) + i);
+}
+
+// Exact LOOP 1 bin of a far pair whose guard bins differ (kb and kb + 1):
+// the reference's bin (int)(r*A_DIV) with r = hypot(dx, hypot(dy, dz))
+// (main.cpp:97, :2951-2956).  The FP64 differences are the reference's
+// coordinate differences scaled by A_DIV = 2^7 (exact: x*A_DIV, and the grid
+// coordinate ((i - ne)*spacing)*A_DIV = (i - ne)*(spacing*A_DIV); ix, iy, iz
+// are i - ne); the squared distance decides against the edge (kb + 1)^2
+// unless it lies within 1e-12 of it, where the reference's own expression
+// decides and the result carries FAR_TIE_FLAG.  Scalars only: a struct
+// argument of a non-inlined function would be copied to local memory.
+__device__ __noinline__ int far_exact_bin(const double *ax128, const double *ay128, const double *az128, int at,
+                                         double spacing_adiv, int ix, int iy, int iz, int kb)
+{
+    const double dx = __dsub_rn(__ldg(ax128 + at), __dmul_rn((double)ix, spacing_adiv));
+    const double dy = __dsub_rn(__ldg(ay128 + at), __dmul_rn((double)iy, spacing_adiv));
+    const double dz = __dsub_rn(__ldg(az128 + at), __dmul_rn((double)iz, spacing_adiv));
+    const double t2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    const double e = (double)(kb + 1), e2 = __dmul_rn(e, e);  // exact: kb < 2^23
+    if (fabs(__dsub_rn(t2, e2)) > 1.0e-12 * e2) return t2 >= e2 ? kb + 1 : kb;
+    const double inv = 1.0 / AG_A_DIV;  // exact
+    const double r = hypot(__dmul_rn(dx, inv), hypot(__dmul_rn(dy, inv), __dmul_rn(dz, inv)));
+    return (int)__dmul_rn(r, (double)AG_A_DIV) | FAR_TIE_FLAG;
+}
+
+// The guard bins of a packed pair of distances: bit patterns MAGIC_BITS +
+// floor(t*edge_lo) and MAGIC_BITS + floor(t*edge_hi) (one FMA each, rounded
+// toward zero onto 2^23).
+__device__ __forceinline__ void far_guard_bins(float2 t, float2 lom, float2 him, float2 &lo, float2 &hi)
+{
+    const float2 magic = make_float2(8388608.f, 8388608.f);
+    lo = __ffma2_rz(t, lom, magic);
+    hi = __ffma2_rz(t, him, magic);
 }
 
 // One work unit: frame `f` of one instance against atom chunk `chunk`.
@@ -45,8 +80,65 @@ __device__ __forceinline__ void load_far_table(float4 *s_tab4, const float *far_
 // The first NJ pairs of each thread hold the frame's x columns inside the box
 // (the rest is padding and is skipped), and a warp whose 4 rows or 2 planes
 // all lie past the box skips the pairs.
+//
+// Table bins (FAR_TAB_TABLE).  Each pair's table value is T[floor(t*edge_lo)];
+// a pair whose second guard bin floor(t*edge_hi) differs lies within the FP32
+// error bound of a bin edge.  Each thread records, per block of 32 atoms, a
+// bit per atom with such a pair among its own (s_hist); after the tile it
+// re-evaluates the pairs of those atoms with the same FP32 operations, takes
+// the exact bin of each flagged pair it owns (t >= FAR_T0) from far_exact_bin
+// and adds w/r * (T[exact] - T[used]) to its own point.  The bins of every far
+// pair are therefore the reference's, and the result stays deterministic.
+template <int MODE, int NJ>
+__device__ __forceinline__ void far_fix_atom(const FarArgs &a, const float4 A, int at, const float2 *npx, float2 npyz,
+                                             float2 lom, float2 him, uint32_t tab_base, int ox, int iy, int iz, int tx,
+                                             float2 *tot, unsigned *s_cnt)
+{
+    const float2 dyz = __fadd2_rn(make_float2(A.y, A.z), npyz);
+    const float s = __fmaf_rn(dyz.x, dyz.x, __fmaf_rn(dyz.y, dyz.y, TINY_T2));
+    const float2 s2 = make_float2(s, s);
+    const float2 ax2 = make_float2(A.x, A.x);
+    const float2 q2 = make_float2(A.w, A.w);
+    const float2 tmax = make_float2(FAR_CLAMP_T, FAR_CLAMP_T);
+#pragma unroll
+    for (int j = 0; j < NJ; j++) {
+        const float2 dx = __fadd2_rn(ax2, npx[j]);
+        const float2 t2 = __ffma2_rn(dx, dx, s2);
+        const float2 rs = make_float2(rsqrt_approx(t2.x), rsqrt_approx(t2.y));
+        float2 t = __fmul2_rn(t2, rs);
+        t = make_float2(fminf(t.x, tmax.x), fminf(t.y, tmax.y));
+        float2 lo, hi;
+        far_guard_bins(t, lom, him, lo, hi);
+        const float2 wv = __fmul2_rn(q2, rs);
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            const float tc = c ? t.y : t.x;
+            const uint32_t bl = __float_as_uint(c ? lo.y : lo.x), bh = __float_as_uint(c ? hi.y : hi.x);
+            const int ix = ox + tx + 8 * j + 4 * c;
+            if (bl == bh || !(tc >= FAR_T0) || ix >= a.n1x) continue;  // unflagged, near-field, or past the box
+            const int kb = (int)(bl - MAGIC_BITS);
+            const int kr = far_exact_bin(a.ax128, a.ay128, a.az128, at, a.spacing_adiv, ix - a.nex, iy - a.ney,
+                                         iz - a.nez, kb);
+            const int kx = kr & ~FAR_TIE_FLAG;
+            const int kf = (int)(__float_as_uint(__fadd_rz(tc, 8388608.f)) - MAGIC_BITS);  // plain FP32 floor(t)
+            atomicAdd(s_cnt, 1u);
+            if (kf != kx) atomicAdd(s_cnt + 1, 1u);
+            if (kr & FAR_TIE_FLAG) atomicAdd(s_cnt + 2, 1u);
+            if (kx != kb) {
+                const float used = lds_f32(tab_base + (bl << 2));
+                const float dT = __fsub_rn(__ldg(a.tab_full + min(kx, AG_NDIEL - 1)), used);
+                if (c) tot[j].y = __fmaf_rn(wv.y, dT, tot[j].y);
+                else tot[j].x = __fmaf_rn(wv.x, dT, tot[j].x);
+            }
+        }
+    }
+}
+
+// s_cnt: three shared counters of the CTA (far_fix_atom), zero on entry;
+// the unit adds them to a.edge_counters and leaves them zero.
 template <int TILE, int MODE, int NJ>
-__device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
+__device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom,
+                                           uint32_t *s_hist, unsigned *s_cnt)
 {
     const int tid = threadIdx.x;
     const int fx = f % a.nfx, fy = (f / a.nfx) % a.nfy, fz = f / (a.nfx * a.nfy);
@@ -77,9 +169,8 @@ __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, c
     // 32-bit shared address of the table, pre-biased so that the bit pattern of
     // (t + 2^23) rounded toward zero indexes it directly:
     // bits(t + 2^23) = 0x4B000000 + floor(t) for 0 <= t < 2^23.
-    const uint32_t tab_base = (uint32_t)__cvta_generic_to_shared(s_tab4) - (0x4B000000u << 2);
-    const float2 magic = make_float2(8388608.f, 8388608.f);
-    const float2 tmax = make_float2(FAR_MAX_T, FAR_MAX_T);
+    const uint32_t tab_base = (uint32_t)__cvta_generic_to_shared(s_tab4) - (MAGIC_BITS << 2);
+    const float2 lom = make_float2(a.edge_lo, a.edge_lo), him = make_float2(a.edge_hi, a.edge_hi);
 
     const int a_begin = chunk * a.chunk_atoms;
     const int a_end = min(a.n_atoms, a_begin + a.chunk_atoms);
@@ -104,36 +195,79 @@ __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, c
         float2 acc[NJ];
 #pragma unroll
         for (int j = 0; j < NJ; j++) acc[j] = make_float2(0.f, 0.f);
+        if (MODE == FAR_TAB_CONST) {
+            const float2 fT0 = make_float2(FAR_T0, FAR_T0);
 #pragma unroll 2
-        for (int i = 0; i < na; i++) {
-            const float4 A = s_atom[i];
-            const float2 dyz = __fadd2_rn(make_float2(A.y, A.z), npyz);
-            const float s = __fmaf_rn(dyz.x, dyz.x, __fmaf_rn(dyz.y, dyz.y, TINY_T2));
-            const float2 s2 = make_float2(s, s);
-            const float2 ax2 = make_float2(A.x, A.x);
-            const float2 q2 = make_float2(A.w, A.w);
+            for (int i = 0; i < na; i++) {
+                const float4 A = s_atom[i];
+                const float2 dyz = __fadd2_rn(make_float2(A.y, A.z), npyz);
+                const float s = __fmaf_rn(dyz.x, dyz.x, __fmaf_rn(dyz.y, dyz.y, TINY_T2));
+                const float2 s2 = make_float2(s, s);
+                const float2 ax2 = make_float2(A.x, A.x);
+                const float2 q2 = make_float2(A.w, A.w);
 #pragma unroll
-            for (int j = 0; j < NJ; j++) {
-                const float2 dx = __fadd2_rn(ax2, npx[j]);
-                const float2 t2 = __ffma2_rn(dx, dx, s2);
-                const float2 rs = make_float2(rsqrt_approx(t2.x), rsqrt_approx(t2.y));
-                float2 t = __fmul2_rn(t2, rs);
-                t = make_float2(fminf(t.x, tmax.x), fminf(t.y, tmax.y));
-                const float2 mg = __fadd2_rz(t, magic);
-                float T0, T1;
-                if (MODE == FAR_TAB_CONST) {
-                    T0 = t.x < (float)AG_NEINT ? 0.f : a.tab_const;
-                    T1 = t.y < (float)AG_NEINT ? 0.f : a.tab_const;
-                } else {
-                    T0 = lds_f32(tab_base + (__float_as_uint(mg.x) << 2));
-                    T1 = lds_f32(tab_base + (__float_as_uint(mg.y) << 2));
+                for (int j = 0; j < NJ; j++) {
+                    const float2 dx = __fadd2_rn(ax2, npx[j]);
+                    const float2 t2 = __ffma2_rn(dx, dx, s2);
+                    const float2 rs = make_float2(rsqrt_approx(t2.x), rsqrt_approx(t2.y));
+                    const float2 t = __fmul2_rn(t2, rs);
+                    const float T0 = t.x < fT0.x ? 0.f : a.tab_const;
+                    const float T1 = t.y < fT0.y ? 0.f : a.tab_const;
+                    const float2 wv = __fmul2_rn(q2, rs);
+                    acc[j] = __ffma2_rn(wv, make_float2(T0, T1), acc[j]);
                 }
-                const float2 wv = __fmul2_rn(q2, rs);
-                acc[j] = __ffma2_rn(wv, make_float2(T0, T1), acc[j]);
+            }
+        } else {
+            const float2 tmax = make_float2(FAR_CLAMP_T, FAR_CLAMP_T);
+            for (int ib = 0; ib < na; ib += 32) {
+                const int nb = min(32, na - ib);
+                uint32_t hist = 0;
+#pragma unroll 2
+                for (int ii = 0; ii < nb; ii++) {
+                    const float4 A = s_atom[ib + ii];
+                    const float2 dyz = __fadd2_rn(make_float2(A.y, A.z), npyz);
+                    const float s = __fmaf_rn(dyz.x, dyz.x, __fmaf_rn(dyz.y, dyz.y, TINY_T2));
+                    const float2 s2 = make_float2(s, s);
+                    const float2 ax2 = make_float2(A.x, A.x);
+                    const float2 q2 = make_float2(A.w, A.w);
+                    bool edge = false;
+#pragma unroll
+                    for (int j = 0; j < NJ; j++) {
+                        const float2 dx = __fadd2_rn(ax2, npx[j]);
+                        const float2 t2 = __ffma2_rn(dx, dx, s2);
+                        const float2 rs = make_float2(rsqrt_approx(t2.x), rsqrt_approx(t2.y));
+                        float2 t = __fmul2_rn(t2, rs);
+                        t = make_float2(fminf(t.x, tmax.x), fminf(t.y, tmax.y));
+                        float2 lo, hi;
+                        far_guard_bins(t, lom, him, lo, hi);
+                        edge |= (__float_as_uint(lo.x) != __float_as_uint(hi.x)) |
+                                (__float_as_uint(lo.y) != __float_as_uint(hi.y));
+                        const float T0 = lds_f32(tab_base + (__float_as_uint(lo.x) << 2));
+                        const float T1 = lds_f32(tab_base + (__float_as_uint(lo.y) << 2));
+                        const float2 wv = __fmul2_rn(q2, rs);
+                        acc[j] = __ffma2_rn(wv, make_float2(T0, T1), acc[j]);
+                    }
+                    hist = (hist << 1) | (edge ? 1u : 0u);
+                }
+                s_hist[(ib >> 5) * EF_THREADS + tid] = hist << (32 - nb);  // atom ib + k at bit 31 - k
             }
         }
 #pragma unroll
         for (int j = 0; j < NJ; j++) tot[j] = __fadd2_rn(tot[j], acc[j]);
+        if (MODE != FAR_TAB_CONST && oy + ty < a.n1y && oz + tz < a.n1z) {
+            // the flagged atoms of this tile, in atom order (s_hist and s_atom
+            // are this tile's); points past the box are not written, not fixed
+            const int iy = oy + ty, iz = oz + tz;
+            for (int ib = 0; ib < na; ib += 32) {
+                uint32_t h = s_hist[(ib >> 5) * EF_THREADS + tid];
+                while (h) {
+                    const int k = __clz(h);
+                    h &= ~(0x80000000u >> k);
+                    far_fix_atom<MODE, NJ>(a, s_atom[ib + k], a0 + ib + k, npx, npyz, lom, him, tab_base, ox, iy, iz,
+                                           tx, tot, s_cnt);
+                }
+            }
+        }
     }
 
     const int iy = oy + ty, iz = oz + tz;
@@ -146,27 +280,45 @@ __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, c
             if (ix1 < a.n1x) out[ix1] = tot[j].y;
         }
     }
+    if (MODE != FAR_TAB_CONST) {
+        __syncthreads();
+        if (tid < 3) {
+            const unsigned v = s_cnt[tid];
+            if (v && a.edge_counters) atomicAdd(a.edge_counters + tid, (unsigned long long)v);
+            s_cnt[tid] = 0u;
+        }
+    }
 }
 
 // The unit with as many x pairs as the frame has columns inside the box
 // (CTA-uniform: only a box's last x frame can be partial).
 template <int TILE, int MODE>
-__device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
+__device__ __forceinline__ void far_unit(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom,
+                                         uint32_t *s_hist, unsigned *s_cnt)
 {
     static_assert(EF_PAIRS == 4, "x-pair dispatch below");
     const int nj = (a.n1x - (f % a.nfx) * FRAME_X + 7) / 8;
-    if (nj >= 4) far_unit_n<TILE, MODE, 4>(a, f, chunk, s_tab4, s_atom);
-    else if (nj == 3) far_unit_n<TILE, MODE, 3>(a, f, chunk, s_tab4, s_atom);
-    else if (nj == 2) far_unit_n<TILE, MODE, 2>(a, f, chunk, s_tab4, s_atom);
-    else far_unit_n<TILE, MODE, 1>(a, f, chunk, s_tab4, s_atom);
+    if (nj >= 4) far_unit_n<TILE, MODE, 4>(a, f, chunk, s_tab4, s_atom, s_hist, s_cnt);
+    else if (nj == 3) far_unit_n<TILE, MODE, 3>(a, f, chunk, s_tab4, s_atom, s_hist, s_cnt);
+    else if (nj == 2) far_unit_n<TILE, MODE, 2>(a, f, chunk, s_tab4, s_atom, s_hist, s_cnt);
+    else far_unit_n<TILE, MODE, 1>(a, f, chunk, s_tab4, s_atom, s_hist, s_cnt);
 }
 
 // The unit for the instance's table mode (batch kernel).
 template <int TILE>
-__device__ __forceinline__ void far_dispatch(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom)
+__device__ __forceinline__ void far_dispatch(const FarArgs &a, int f, int chunk, const float4 *s_tab4, float4 *s_atom,
+                                             uint32_t *s_hist, unsigned *s_cnt)
 {
-    if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST>(a, f, chunk, s_tab4, s_atom);
-    else far_unit<TILE, FAR_TAB_TABLE>(a, f, chunk, s_tab4, s_atom);
+    if (a.tab_mode == FAR_TAB_CONST) far_unit<TILE, FAR_TAB_CONST>(a, f, chunk, s_tab4, s_atom, s_hist, s_cnt);
+    else far_unit<TILE, FAR_TAB_TABLE>(a, f, chunk, s_tab4, s_atom, s_hist, s_cnt);
+}
+
+// Dynamic shared memory of the far kernels: the table (AG_NDIEL floats), the
+// atom tile (TILE float4) and the per-thread edge bits (TILE/32 words per thread).
+template <int TILE>
+__device__ __forceinline__ uint32_t *far_hist_smem(float4 *smem)
+{
+    return (uint32_t *)(smem + AG_NDIEL / 4 + TILE);
 }
 
 // Single instance: one CTA per (frame, chunk) = (blockIdx.x, blockIdx.y).  The
@@ -178,16 +330,19 @@ __global__ void __launch_bounds__(EF_THREADS, 3) k_emap_far(FarArgs a)
     extern __shared__ float4 ef_smem[];
     float4 *s_tab4 = ef_smem;                 // AG_NDIEL floats
     float4 *s_atom = ef_smem + AG_NDIEL / 4;  // TILE entries
+    uint32_t *s_hist = far_hist_smem<TILE>(ef_smem);
+    __shared__ unsigned s_cnt[3];
+    if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0u;
     if (a.tab_mode != FAR_TAB_CONST) load_far_table(s_tab4, a.far_tab);
     __syncthreads();
     const int f = a.frame0 + blockIdx.x;
     const bool last = NJ_LAST < EF_PAIRS && f % a.nfx == a.nfx - 1;
     if (a.tab_mode == FAR_TAB_CONST) {
-        if (last) far_unit_n<TILE, FAR_TAB_CONST, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
-        else far_unit_n<TILE, FAR_TAB_CONST, EF_PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
+        if (last) far_unit_n<TILE, FAR_TAB_CONST, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom, s_hist, s_cnt);
+        else far_unit_n<TILE, FAR_TAB_CONST, EF_PAIRS>(a, f, blockIdx.y, s_tab4, s_atom, s_hist, s_cnt);
     } else {
-        if (last) far_unit_n<TILE, FAR_TAB_TABLE, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom);
-        else far_unit_n<TILE, FAR_TAB_TABLE, EF_PAIRS>(a, f, blockIdx.y, s_tab4, s_atom);
+        if (last) far_unit_n<TILE, FAR_TAB_TABLE, NJ_LAST>(a, f, blockIdx.y, s_tab4, s_atom, s_hist, s_cnt);
+        else far_unit_n<TILE, FAR_TAB_TABLE, EF_PAIRS>(a, f, blockIdx.y, s_tab4, s_atom, s_hist, s_cnt);
     }
 }
 
@@ -202,6 +357,9 @@ k_emap_far_batch(const FarArgs *__restrict__ insts, const long long *__restrict_
     extern __shared__ float4 ef_smem[];
     float4 *s_tab4 = ef_smem;
     float4 *s_atom = ef_smem + AG_NDIEL / 4;
+    uint32_t *s_hist = far_hist_smem<TILE>(ef_smem);
+    __shared__ unsigned s_cnt[3];
+    if (threadIdx.x < 3) s_cnt[threadIdx.x] = 0u;
     __shared__ long long s_unit;
     __shared__ FarArgs s_a;
     int cur = -1;
@@ -227,8 +385,57 @@ k_emap_far_batch(const FarArgs *__restrict__ insts, const long long *__restrict_
         const long long lu = u - unit_begin[lo];
         const int frames = s_a.nfx * s_a.nfy * s_a.nfz;
         const int fr = (int)(lu % frames), ch = (int)(lu / frames);
-        far_dispatch<TILE>(s_a, fr, ch, s_tab4, s_atom);
+        far_dispatch<TILE>(s_a, fr, ch, s_tab4, s_atom, s_hist, s_cnt);
     }
+}
+
+// Bins of the far field for every (listed point, atom) pair, with the far
+// kernel's own arithmetic (frame-relative FP32 coordinates of the point's
+// frame, guard bins, far_exact_bin): used[k] = the bin the far kernel's
+// result carries for the pair (-1 for a near-field pair, t < FAR_T0),
+// fp32[k] = floor(t) of the FP32 distance, flags[k] = 1 when the guard bins
+// differ (resolved in FP64), | 2 when that resolution was a tie.  k = point
+// slot * n_atoms + atom.  A diagnostic for tests on small problems.
+__global__ void __launch_bounds__(256) k_far_bins_debug(FarArgs a, const long long *__restrict__ pts, int n_pts,
+                                                        int *__restrict__ used, int *__restrict__ fp32,
+                                                        int *__restrict__ flags)
+{
+    const long long k = (long long)blockIdx.x * 256 + threadIdx.x;
+    if (k >= (long long)n_pts * a.n_atoms) return;
+    const int at = (int)(k % a.n_atoms);
+    const long long lin = pts[k / a.n_atoms];
+    const int ix = (int)(lin % a.n1x), iy = (int)((lin / a.n1x) % a.n1y), iz = (int)(lin / ((long long)a.n1x * a.n1y));
+    const int ox = ix / FRAME_X * FRAME_X, oy = iy / FRAME_Y * FRAME_Y, oz = iz / FRAME_Z * FRAME_Z;
+    const float ax = frame_atom_coord(a.ax128[at], frame_origin_bins(ox, a.nex, a.spacing_adiv));
+    const float ay = frame_atom_coord(a.ay128[at], frame_origin_bins(oy, a.ney, a.spacing_adiv));
+    const float az = frame_atom_coord(a.az128[at], frame_origin_bins(oz, a.nez, a.spacing_adiv));
+    const float s = far_pair_s(ay, az, frame_point_coord(iy - oy, a.spacing_adiv),
+                               frame_point_coord(iz - oz, a.spacing_adiv));
+    const float t = fminf(far_pair_t(ax, frame_point_coord(ix - ox, a.spacing_adiv), s), FAR_CLAMP_T);
+    const int kl = (int)(__float_as_uint(__fmaf_rz(t, a.edge_lo, 8388608.f)) - MAGIC_BITS);
+    const int kh = (int)(__float_as_uint(__fmaf_rz(t, a.edge_hi, 8388608.f)) - MAGIC_BITS);
+    fp32[k] = (int)(__float_as_uint(__fadd_rz(t, 8388608.f)) - MAGIC_BITS);
+    int u = kl, fl = 0;
+    if (kl != kh) {
+        fl = 1;
+        if (t >= FAR_T0) {
+            const int kr = far_exact_bin(a.ax128, a.ay128, a.az128, at, a.spacing_adiv, ix - a.nex, iy - a.ney,
+                                         iz - a.nez, kl);
+            u = kr & ~FAR_TIE_FLAG;
+            if (kr & FAR_TIE_FLAG) fl |= 2;
+        }
+    }
+    used[k] = t >= FAR_T0 ? min(u, AG_NDIEL - 1) : -1;
+    flags[k] = fl;
+}
+
+cudaError_t launch_far_bins_debug(const FarArgs &a, const long long *pts, int n_pts, int *used, int *fp32, int *flags,
+                                  cudaStream_t s)
+{
+    const long long n = (long long)n_pts * a.n_atoms;
+    if (n <= 0) return cudaSuccess;
+    k_far_bins_debug<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a, pts, n_pts, used, fp32, flags);
+    return cudaGetLastError();
 }
 
 // FP64 twin of LOOP 1: one thread per point, all atoms in file order.
@@ -274,7 +481,10 @@ int frames_x(int n1x) { return (n1x + FRAME_X - 1) / FRAME_X; }
 int frames_y(int n1y) { return (n1y + FRAME_Y - 1) / FRAME_Y; }
 int frames_z(int n1z) { return (n1z + FRAME_Z - 1) / FRAME_Z; }
 
-size_t far_smem_bytes(int tile) { return AG_NDIEL * sizeof(float) + (size_t)tile * sizeof(float4); }
+size_t far_smem_bytes(int tile)
+{
+    return AG_NDIEL * sizeof(float) + (size_t)tile * sizeof(float4) + (size_t)(tile / 32) * EF_THREADS * sizeof(uint32_t);
+}
 
 // Frame z-rows [fz0, fz1) of one instance (fz1 < 0: through the last).
 cudaError_t launch_emap_far(const FarArgs &args, int n_chunks, int tile, cudaStream_t s, int fz0, int fz1)
@@ -294,25 +504,47 @@ cudaError_t launch_emap_far(const FarArgs &args, int n_chunks, int tile, cudaStr
     return cudaGetLastError();
 }
 
+int current_device_sms()
+{
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        sms <= 0)
+        return 148;
+    return sms;
+}
+
+cudaError_t prepare_far_kernels()
+{
+    const int s512 = (int)far_smem_bytes(512);
+    const void *single[] = {(const void *)k_emap_far<512, 1>, (const void *)k_emap_far<512, 2>,
+                            (const void *)k_emap_far<512, 3>, (const void *)k_emap_far<512, 4>};
+    for (const void *fn : single) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, s512);
+        if (e != cudaSuccess) return e;
+    }
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute((const void *)k_emap_far_batch<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)far_smem_bytes(256))) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute((const void *)k_emap_far_batch<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  s512)) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute((const void *)k_emap_far_batch<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)far_smem_bytes(1024));
+}
+
+// The persistent batch kernel: as many CTAs as fit (at most ctas_per_sm) on
+// every SM.  Its shared-memory limit is set by prepare_far_kernels().
 template <int TILE>
 static cudaError_t far_batch_t(const FarArgs *insts, const long long *unit_begin, int n_inst,
                                unsigned long long *counter, int ctas_per_sm, cudaStream_t s)
 {
     const size_t smem = far_smem_bytes(TILE);
-    static bool attr_set = false;  // set once, outside any stream capture (the first call is the autotuner's)
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(k_emap_far_batch<TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)smem);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
-    int dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_emap_far_batch<TILE>, EF_THREADS, smem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_emap_far_batch<TILE>, EF_THREADS, smem);
+    if (e != cudaSuccess) return e;
     const int per_sm = std::max(1, std::min(ctas_per_sm, occ));
-    k_emap_far_batch<TILE><<<sms * per_sm, EF_THREADS, smem, s>>>(insts, unit_begin, n_inst, counter);
+    k_emap_far_batch<TILE><<<current_device_sms() * per_sm, EF_THREADS, smem, s>>>(insts, unit_begin, n_inst, counter);
     return cudaGetLastError();
 }
 
@@ -360,7 +592,7 @@ __global__ void __launch_bounds__(256) k_emap_reduce_range(ReduceInst r, long lo
 cudaError_t launch_emap_reduce_range(const ReduceInst &r, long long lin0, long long lin1, cudaStream_t s)
 {
     if (lin1 <= lin0) return cudaSuccess;
-    const unsigned nb = (unsigned)std::min<long long>((lin1 - lin0 + 255) / 256, 148LL * 16);
+    const unsigned nb = (unsigned)std::min<long long>((lin1 - lin0 + 255) / 256, 16LL * current_device_sms());
     k_emap_reduce_range<<<nb, 256, 0, s>>>(r, lin0, lin1);
     return cudaGetLastError();
 }
@@ -370,7 +602,7 @@ cudaError_t launch_emap_reduce(const ReduceInst *insts, const long long *begin, 
 {
     if (n <= 0 || total <= 0) return cudaSuccess;
     const long long want = (total + 255) / 256;
-    const unsigned nb = (unsigned)std::min<long long>(want, 148LL * 16);
+    const unsigned nb = (unsigned)std::min<long long>(want, 16LL * current_device_sms());
     k_emap_reduce<<<nb, 256, 0, s>>>(insts, begin, n);
     return cudaGetLastError();
 }

@@ -40,6 +40,10 @@ struct NearInst {
 
 
 size_t far_smem_bytes(int tile);
+// Dynamic shared-memory limits of the far kernels on the current device.
+cudaError_t prepare_far_kernels();
+cudaError_t launch_far_bins_debug(const FarArgs &a, const long long *pts, int n_pts, int *used, int *fp32, int *flags,
+                                  cudaStream_t s);
 cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s, int fz0 = 0, int fz1 = -1);
 cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_begin, int n_inst,
                                   unsigned long long *counter, int tile, int ctas_per_sm, cudaStream_t s);

@@ -11,11 +11,15 @@
 // partial sums) in one file-scope __device__ array of fixed size.
 //
 // It is a variant of k_emap_far (emap.cu): the same frame decomposition,
-// canonical FP32 distances and shared-memory table gather, but it also covers
-// the pairs nearer than 8 A itself -- those are evaluated in FP64 with the
-// reference's LOOP 1 expression -- so it needs no near-field kernel, cell list
-// or closest-hydrogen buffer.
+// canonical FP32 distances, bin guard and shared-memory table gather, but it
+// also covers the pairs nearer than 8 A itself -- those, and the far pairs
+// the bin guard flags, are evaluated in FP64 with the reference's LOOP 1
+// expression -- so it needs no near-field kernel, cell list or
+// closest-hydrogen buffer.  Table bins are the reference's (pairs within
+// 1e-12 of an edge in FP64 aside, where CUDA's hypot decides); this entry
+// point reports no statistics.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -72,7 +76,8 @@ __device__ __forceinline__ double loop1_term(const double *coord, const double *
 __global__ void __launch_bounds__(NA_THREADS)
 k_emap_noalloc(const double *__restrict__ coord, const double *__restrict__ charge, int n_atoms, int dddiel,
                const double *__restrict__ reps, double invdielcal, double coeff_estat, double spacing,
-               int n1x, int n1y, int n1z, int nex, int ney, int nez, int nfx, int nfy, long long P, NoallocLayout L)
+               int n1x, int n1y, int n1z, int nex, int ney, int nez, int nfx, int nfy, long long P, NoallocLayout L,
+               float edge_lo, float edge_hi)
 {
     extern __shared__ float4 na_smem[];
     float *s_tab = (float *)na_smem;
@@ -126,12 +131,15 @@ k_emap_noalloc(const double *__restrict__ coord, const double *__restrict__ char
                 const float dx = __fsub_rn(A.x, px[k]);
                 const float t2 = __fmaf_rn(dx, dx, s);
                 const float rs = rsqrt_approx(t2);
-                const float t = __fmul_rn(t2, rs);
-                if (t < NA_NEAR_T) {
+                const float t = fminf(__fmul_rn(t2, rs), FAR_CLAMP_T);
+                // the far kernel's bin guard: a pair within the FP32 error bound
+                // of a bin edge takes the FP64 term, with the reference's bin
+                const uint32_t lo = __float_as_uint(__fmaf_rz(t, edge_lo, 8388608.f));
+                const uint32_t hi = __float_as_uint(__fmaf_rz(t, edge_hi, 8388608.f));
+                if (t < NA_NEAR_T || lo != hi) {
                     acc[k] += (float)loop1_term(coord, charge, a, cxp[k], cy, cz, dddiel, reps, invdielcal, coeff_estat);
                 } else {
-                    const int bin = min((int)t, AG_NDIEL - 1);
-                    acc[k] = __fmaf_rn(qa * rs, s_tab[bin], acc[k]);
+                    acc[k] = __fmaf_rn(qa * rs, s_tab[lo - MAGIC_BITS], acc[k]);
                 }
             }
         }
@@ -161,6 +169,31 @@ __global__ void k_noalloc_reduce(NoallocLayout L, long long P, float *__restrict
 namespace {
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[64] = {};  // device address of g_noalloc_scratch, per device ordinal
+
+// Guard multipliers of the far kernel's bin guard for this spacing (bins):
+// the largest frame point coordinate and whether the frame point
+// coordinates are exact floats (see far_edge_multipliers).
+void noalloc_guard(double spacing_adiv, float *lo, float *hi)
+{
+    bool exact = true;
+    for (int il = 0; il < FRAME_X; il++) {
+        const double v = (double)il * spacing_adiv;
+        exact &= std::fma((double)il, spacing_adiv, -v) == 0.0 && (double)(float)v == v;
+    }
+    const double px = (FRAME_X - 1) * spacing_adiv, pyz = (FRAME_Y - 1) * spacing_adiv;
+    far_edge_multipliers(std::sqrt(px * px + 2 * pyz * pyz), exact, 2.5, lo, hi);
+}
+
+// The caller's current device, given back when the entry point returns.
+struct RestoreDevice {
+    int prev = -1;
+    RestoreDevice() { cudaGetDevice(&prev); }
+    ~RestoreDevice()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 }
 
 }  // namespace agb
@@ -210,10 +243,19 @@ extern "C" ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, co
         set_last_error("ag_emap_compute_noalloc: the buffers must be device memory of the given GPU");
         return AG_ERR_INVALID;
     }
+    RestoreDevice restore;
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {
         set_last_error(std::string("cudaSetDevice: ") + cudaGetErrorString(e));
         return AG_ERR_CUDA;
+    }
+    if (stream) {
+        int sdev = -1;
+        e = cudaStreamGetDevice((cudaStream_t)stream, &sdev);
+        if (e != cudaSuccess || sdev != device) {
+            set_last_error("ag_emap_compute_noalloc: the stream does not belong to the given device");
+            return AG_ERR_INVALID;
+        }
     }
     void *base = nullptr;
     {
@@ -243,7 +285,7 @@ extern "C" ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, co
     const int nfx = (n1[0] + FRAME_X - 1) / FRAME_X, nfy = (n1[1] + FRAME_Y - 1) / FRAME_Y, nfz = (n1[2] + FRAME_Z - 1) / FRAME_Z;
     const long long frames = (long long)nfx * nfy * nfz;
     const size_t max_chunks = (NOALLOC_SCRATCH_BYTES - fixed) / up(sizeof(float) * (size_t)P);
-    int chunks = (int)std::max(1LL, (148LL * 8 * 3 + frames - 1) / frames);
+    int chunks = (int)std::max(1LL, ((long long)current_device_sms() * 8 * 3 + frames - 1) / frames);
     chunks = (int)std::min<long long>(chunks, (long long)max_chunks);
     chunks = std::min(chunks, std::max(1, (n_atoms + NA_TILE - 1) / NA_TILE));
     L.chunk_atoms = ((std::max(n_atoms, 1) + chunks - 1) / chunks + NA_TILE - 1) / NA_TILE * NA_TILE;
@@ -255,10 +297,12 @@ extern "C" ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, co
     if (n_atoms > 0) {
         const size_t smem = AG_NDIEL * sizeof(float) + NA_TILE * sizeof(float4);
         e = cudaFuncSetAttribute(k_emap_noalloc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        float edge_lo = 1.f, edge_hi = 1.f;
+        noalloc_guard(spacing * AG_A_DIV, &edge_lo, &edge_hi);
         if (e == cudaSuccess) {
             k_emap_noalloc<<<dim3((unsigned)frames, (unsigned)L.chunks), NA_THREADS, smem, s>>>(
                 d_coord, d_charge, n_atoms, dddiel, d_r_epsilon_fn, invdielcal, coeff_estat, spacing, n1[0], n1[1],
-                n1[2], (n1[0] - 1) / 2, (n1[1] - 1) / 2, (n1[2] - 1) / 2, nfx, nfy, P, L);
+                n1[2], (n1[0] - 1) / 2, (n1[1] - 1) / 2, (n1[2] - 1) / 2, nfx, nfy, P, L, edge_lo, edge_hi);
         }
     } else {
         L.chunks = 0;  // no atoms: the map is zero

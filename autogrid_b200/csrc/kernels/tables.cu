@@ -119,7 +119,8 @@ __global__ void __launch_bounds__(kThreads) k_sol_eps(TableArgs a, double *sol_f
 }
 
 // Plan tables from device-resident problem tables: vdwT [type][bin][mpad]
-// (column c holds map colmap[c], or zeros), far_tab / etab / solf (FP32) and
+// (column c holds map colmap[c], or zeros), far_tab [2][NDIEL] (zero below
+// FAR_BIN0, then the whole table) / etab / solf (FP32) and
 // reps (FP64, distance-dependent dielectric only).
 __global__ void __launch_bounds__(kThreads) k_pack_vdw(const float *e_vdw_hb, int n_rec_types, int n_atom_maps,
                                                        const int *colmap, int mpad, float *vdwT)
@@ -143,6 +144,7 @@ __global__ void __launch_bounds__(kThreads) k_pack_lines(const double *sol_fn, c
     const double f = dddiel ? r_eps[k] : invdielcal;
     if (reps) reps[k] = dddiel ? r_eps[k] : 0.0;
     far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
+    far_tab[AG_NDIEL + k] = (float)f;  // the whole table, for the far kernel's bin guard
     etab[k] = (float)__dmul_rn(f, coeff_estat);
     solf[k] = (float)sol_fn[k];
 }

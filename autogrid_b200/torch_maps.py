@@ -16,6 +16,12 @@ adjoint kernels and the bond-vector chain rule on the device
 (ag_diff_backward_device).  The closest DS/D1 atom of each grid point is
 searched at the first forward and kept afterwards (keep_closest_h=False
 searches it at every forward).
+
+Sharded over GPUs (one process per GPU): GridMaps(job, device, zslab=(z0, z1))
+computes grid planes [z0, z1) only (autogrid_b200.shard.zslab_ranges gives each
+rank its slab); the loss over those planes gives each rank a partial gradient
+over all atoms, and autogrid_b200.shard.allreduce_gradients([coords.grad,
+charges.grad]) sums them with one all-reduce.
 """
 from __future__ import annotations
 
@@ -27,9 +33,13 @@ from .api import Context, Diff, Job
 class GridMaps:
     """Callable (coords [N,3], charges [N]) -> maps, differentiable in both."""
 
-    def __init__(self, job: Job, device: int = 0, precision: str = "fp32", keep_closest_h: bool = True):
+    def __init__(self, job: Job, device: int = 0, precision: str = "fp32", keep_closest_h: bool = True,
+                 zslab: tuple | None = None):
         self.job = job
         self.problem = job.problem()
+        if zslab is not None:
+            from .shard import zslab_problem
+            self.problem = zslab_problem(self.problem, int(zslab[0]), int(zslab[1]))
         self.device = torch.device("cuda", device)
         self.ctx = Context(device)
         self.diff = Diff(self.ctx, self.problem, precision)

@@ -18,8 +18,11 @@ spacing 0.375 A, distance-dependent dielectric.  One step = one full map set.
            compiled from the reference sources) on a bounded sample of the same
            workload: same receptor and 16 maps, fewer z-planes.
 
-Multi-GPU (torchrun): one independent map set per rank (weak scaling, no
-collective on the data path); time = max over ranks.
+Multi-GPU (torchrun, one process per GPU): the one map set is split by
+z-slab (autogrid_b200.shard.zslab_ranges; ag_plan_run_zslab for `value`,
+ag_maps_compute_zslab for `e2e`), strong scaling: total work fixed, time =
+max over ranks, no collective on the data path (the timing reduction is the
+only one).  The batched ensemble splits by instance (shard.partition_instances).
 """
 from __future__ import annotations
 
@@ -179,10 +182,19 @@ def main():
     from autogrid_b200._abi import ag_stats  # noqa: F401
 
     work = Path(tempfile.mkdtemp(prefix=f"agb_bench_r{rank}_"))
-    rec, spec, job, prob = make_problem(args.workload, seed=rank, workdir=work)
+    rec, spec, job, prob = make_problem(args.workload, seed=0, workdir=work)  # one map set, split over ranks
     P, M = prob.points, prob.n_maps
+    from autogrid_b200.shard import zslab_ranges
+    z0, z1 = zslab_ranges(prob.n1[2], world)[rank]
+    slab_planes = z1 - z0
     ctx = Context(local)
     plan = ctx.plan(prob)
+
+    def run_step():
+        if world == 1:
+            plan.run(sptr)
+        elif slab_planes > 0:
+            plan.run_zslab(z0, z1, sptr)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     # a dedicated stream: the library launches on it, and the events below are recorded on it
     stream = torch.cuda.Stream()
@@ -191,7 +203,7 @@ def main():
     assert sptr, "need a non-default CUDA stream"
 
     for _ in range(args.warmup):
-        plan.run(sptr)
+        run_step()
     torch.cuda.synchronize()
 
     # ---------------- device-resident timed region ----------------
@@ -205,7 +217,7 @@ def main():
     for k in range(args.steps):
         flush.zero_()
         starts[k].record(stream)
-        plan.run(sptr)
+        run_step()
         ends[k].record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -226,22 +238,33 @@ def main():
     plan_serial.close()
 
     # ---------------- end to end through the C ABI ----------------
-    out = torch.empty(prob.map_shape, dtype=torch.float32, pin_memory=True).numpy()
-    ctx.compute(prob, "fp32", out=out)  # warm the context's buffers
+    out_shape = prob.map_shape if world == 1 else (prob.n_out, slab_planes, prob.n1[1], prob.n1[0])
+    out = torch.empty(out_shape, dtype=torch.float32, pin_memory=True).numpy()
+
+    def e2e_step():
+        if world == 1:
+            ctx.compute(prob, "fp32", out=out)
+        elif slab_planes > 0:
+            ctx.compute_zslab(prob, z0, z1, out=out)
+
+    e2e_step()  # warm the context's buffers
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
     e2e_t = []
     for k in range(args.steps):
         t0 = time.perf_counter()
-        ctx.compute(prob, "fp32", out=out)
+        e2e_step()
         e2e_t.append(time.perf_counter() - t0)
     e2e_s = float(np.mean(e2e_t))
 
     ms, e2e_s = max_over_ranks([ms, e2e_s], world, "cuda")
+    batch_sh = None
+    if world > 1 and not args.no_batch:
+        batch_sh = batched_sharded(ctx, args.batch_instances, work, stream, rank, world)
 
     if rank == 0:
-        evals = P * M * world
+        evals = P * M  # the whole map set, whatever the number of ranks
         rate_r, rate_f, clk_nominal = peak_rates(lib, local)
         pairs = prob.points * prob.n_atoms  # far-field pair terms (near pairs excluded are < 1%)
         achieved = pairs / (ker_ms * 1e-3) if ker_ms else None
@@ -257,18 +280,27 @@ def main():
         line = {
             "metric": METRIC, "value": evals / (ms * 1e-3), "unit": "evals/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (FP64 fallback near table-bin edges)",
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32 (FP64 fallback near table-bin edges)",
             "data": "synthetic (seeded receptor, shapes of the plain large map set)",
             "config": {"workload": args.workload, "atoms": prob.n_atoms, "points": P, "maps": M,
-                       "npts": list(spec.npts), "spacing": spec.spacing, "parallelism": f"replica x{world}",
+                       "npts": list(spec.npts), "spacing": spec.spacing,
+                       "parallelism": "single GPU" if world == 1 else f"z-slab x{world}",
                        "l2": "flushed (256 MiB write) before every timed step"},
             "e2e": {"value": evals / e2e_s, "unit": "evals/s", "ms_per_step": e2e_s * 1e3,
-                    "h2d_bytes_per_step": prob.bytes_h2d(), "d2h_bytes_per_step": P * M * 4},
+                    "h2d_bytes_per_step": prob.bytes_h2d() * world, "d2h_bytes_per_step": P * M * 4},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": roof,
             "clocks": clk,
-            "diagnostics": {"near_pairs_per_step": st.near_pairs, "fp64_fallbacks_per_step": st.fp64_fallbacks},
+            "diagnostics": {"near_pairs_per_step": st.near_pairs, "fp64_fallbacks_per_step": st.fp64_fallbacks,
+                            "far_pairs_per_step": st.far_pairs,
+                            # far-field bin guard: pairs resolved in FP64, of which the plain FP32
+                            # bin was wrong, and FP64 ties decided by the reference expression
+                            "far_edge_pairs_per_step": st.far_edge_pairs,
+                            "far_fp32_bin_errors_per_step": st.far_fp32_bin_errors,
+                            "far_fp64_ties_per_step": st.far_fp64_ties},
         }
+        if batch_sh is not None:
+            line["batched_sharded"] = batch_sh
         if not args.no_text and world == 1:
             line["map_text"] = map_text(ctx, plan, prob, rec, spec, work, args.steps)
         if not args.no_batch and world == 1:
@@ -431,6 +463,45 @@ def batched_ensemble(ctx, n, work: Path, stream):
             "create_s": create_s, "tuning": tune}
 
 
+def batched_sharded(ctx, n, work: Path, stream, rank: int, world: int):
+    """The batched ensemble split by instance over the ranks
+    (shard.partition_instances, greedy by points x atoms): each rank runs its
+    share as one batch; the ensemble's time is the slowest rank's (L2 flushed,
+    CUDA events, mean of 5)."""
+    import torch
+    from autogrid_b200 import Batch, Job, synth
+    from autogrid_b200.shard import instance_cost, partition_instances
+    d = work / "ensemble"
+    gpfs = synth.write_ensemble(d, n, seed=2024)
+    cwd = os.getcwd()
+    os.chdir(d)
+    try:
+        probs = [Job(os.path.basename(g), None).problem() for g in gpfs]
+    finally:
+        os.chdir(cwd)
+    share = partition_instances([instance_cost(p) for p in probs], world)[rank]
+    mine = [probs[i] for i in share]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    b = Batch(ctx, mine) if mine else None
+    vals = []
+    if b is not None:
+        b.run(stream.cuda_stream)
+        torch.cuda.synchronize()
+        for _ in range(5):
+            flush.zero_()
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            b.run(stream.cuda_stream)
+            e_.record(stream)
+            torch.cuda.synchronize()
+            vals.append(s_.elapsed_time(e_))
+        b.close()
+    ms = max_over_ranks([float(np.mean(vals)) if vals else 0.0], world, "cuda")[0]
+    evals = sum(p.points * p.n_maps for p in probs)
+    return {"instances": n, "split": f"by instance over {world} ranks (greedy, points x atoms)",
+            "ms_per_ensemble": ms, "evals_per_s": evals / (ms * 1e-3) if ms else None}
+
+
 def differentiable_maps(ctx, work: Path, stream, reps: int = 10):
     """The differentiable form: 4,000-atom receptor (same generator), npts
     60^3, 8 maps, linear-table mode.  Forward and adjoint device times of the
@@ -489,7 +560,7 @@ def differentiable_maps(ctx, work: Path, stream, reps: int = 10):
             e2e.append(time.perf_counter() - t0)
     atoms = rng.choice(prob.n_atoms, 64, replace=False)
     hs = (1e-3, 1e-5)
-    chk = gradcheck.check(job, prob, ctx, atoms, w, h_coord=hs)
+    chk = gradcheck.check(job, prob, ctx, atoms, w, h_coord=hs, kink_free=True)
     return {
         "workload": "diff_4000_61cube_8maps", "atoms": prob.n_atoms, "points": P, "maps": M,
         "tables": "linear interpolation between bins (AG_TABLE_LINEAR)", "dtype": "f32 (FP64 twin as error oracle)",
@@ -506,6 +577,13 @@ def differentiable_maps(ctx, work: Path, stream, reps: int = 10):
             "fp32_adjoint_vs_fd_charge": chk["fp32_vs_fd_charge"],
             "fp64_adjoint_vs_fd_coord": {str(h): chk["fp64_vs_fd_coord"][h] for h in hs},
             "fp32_adjoint_vs_fd_coord": {str(h): chk["fp32_vs_fd_coord"][h] for h in hs},
+            # the loss restricted, per component, to the grid points at which it has no slope
+            # kink along the stencil (autogrid_b200.gradcheck.kink_mask): adjoint vs central
+            # differences of that loss
+            "fd_kink_free_error": {str(h): chk["fd_kink_free_coord"][h] for h in hs},
+            "fd_kinked_components": {str(h): chk["fd_kinked_components"][h] for h in hs},
+            "fd_components": chk["fd_components"],
+            "fd_masked_point_fraction": {str(h): chk["fd_masked_point_fraction"][h] for h in hs},
             "error_norm": "||a - b||_2 / ||b||_2 over the checked components",
             "seconds": chk["fd_seconds"],
         },

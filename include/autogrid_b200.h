@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-#define AG_ABI_VERSION 1
+#define AG_ABI_VERSION 2   /* 2: ag_stats gained the far-field bin counters */
 
 /* Table geometry of the reference build (-DUSE_8A_NBCUTOFF):
  * NEINT = NBC*A_DIV = 8*128 (constants.h:149-160), NDIEL = 64*128
@@ -155,6 +155,18 @@ typedef struct ag_stats {
                                   kernels (measure, scan and write passes)      */
     int64_t text_bytes;        /* bytes of map text that call produced          */
     double  table_ms;          /* device time of the last ag_tables_build        */
+    /* Far-field table bins (e map, pairs beyond 8 A, distance-dependent
+     * dielectric).  Every far pair's bin equals the reference's
+     * (int)(r*A_DIV) of main.cpp:2951-2956: a pair whose FP32 distance lies
+     * within its error bound of a bin edge is resolved in FP64. */
+    int64_t far_edge_pairs;    /* far pairs resolved in FP64                     */
+    int64_t far_fp32_bin_errors; /* of those, pairs whose plain FP32 bin
+                                  floor(A_DIV*r) differed from the exact bin    */
+    int64_t far_fp64_ties;     /* of those, pairs whose FP64 squared distance
+                                  lay within 1e-12 of the edge; their bin is
+                                  the reference expression's (nested hypot) in
+                                  CUDA's libm, which may differ from the host
+                                  libm's by one ulp of r                        */
 } ag_stats;
 
 typedef struct ag_context ag_context;
@@ -185,6 +197,20 @@ ag_status ag_maps_compute_f64(ag_context *ctx, const ag_problem *problem,
                               const ag_opts *opts, double *maps);
 
 /*
+ * One z-slab of the map set: grid planes [z0, z1) of every map (FP32), the
+ * shard a device computes when a map set is split across GPUs.  The
+ * reference parallelises its grid loop over the same axis (one OpenMP task
+ * per z-plane, main.cpp:2805); a slab's points need every atom but nothing of
+ * the other planes, so shards need no exchange.  z0 must be a multiple of 8
+ * and z1 a multiple of 8 or n1[2] (AG_ERR_INVALID otherwise).  maps:
+ * [n_out][z1-z0][n1[1]][n1[0]] (n_out as for ag_maps_compute), host or device
+ * memory.  The planes equal those of ag_maps_compute bit for bit.  The
+ * context's device is made current for the call and the caller's restored.
+ */
+ag_status ag_maps_compute_zslab(ag_context *ctx, const ag_problem *problem,
+                                const ag_opts *opts, int32_t z0, int32_t z1, float *maps);
+
+/*
  * Device-resident plan: the problem is validated and uploaded once, device
  * scratch (cell list, sorted atom tiles, padded tables) is allocated once,
  * and ag_plan_run() only launches kernels on `stream` (a cudaStream_t, or
@@ -194,6 +220,9 @@ typedef struct ag_plan ag_plan;
 ag_status    ag_plan_create(ag_context *ctx, const ag_problem *problem,
                             const ag_opts *opts, ag_plan **out);
 ag_status    ag_plan_run(ag_plan *plan, void *stream);
+/* ag_plan_run for grid planes [z0, z1) only (bounds as ag_maps_compute_zslab);
+ * the planes land at their places in the plan's device maps. */
+ag_status    ag_plan_run_zslab(ag_plan *plan, int32_t z0, int32_t z1, void *stream);
 const float *ag_plan_device_maps(const ag_plan *plan);   /* device pointer  */
 size_t       ag_plan_points(const ag_plan *plan);        /* n1x*n1y*n1z     */
 ag_status    ag_plan_download(ag_plan *plan, float *host_maps);
@@ -268,10 +297,14 @@ ag_status ag_maps_compute_text(ag_context *ctx, const ag_problem *problem, const
  * every GPU which loads this entry point's module keeps until process exit;
  * grids that do not fit (about 7.5 million points at 10,000 atoms) are
  * rejected with AG_ERR_TOO_LARGE.  The first call on a device resolves the
- * array's device address (cudaGetSymbolAddress), so make that first call
- * before any stream capture.  All calls share the array: calls that overlap on
- * the GPU (other streams, other host threads) race.  Every scratch word read
- * is written earlier in the same call, so nothing needs clearing.
+ * array's device address (cudaGetSymbolAddress) and keeps it for the process,
+ * so make that first call before any stream capture, and do not use this entry
+ * point on a device after a cudaDeviceReset of it.  All calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads) race.
+ * Every scratch word read is written earlier in the same call, so nothing
+ * needs clearing.  `stream` must belong to `device` (AG_ERR_INVALID
+ * otherwise); the caller's current device is restored on return.  Table bins
+ * follow the far-field bin guard of ag_maps_compute (no statistics).
  */
 #define AG_NOALLOC_SCRATCH_BYTES (32u << 20)
 ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, const double *d_coord,

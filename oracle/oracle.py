@@ -15,6 +15,10 @@ HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "_build" / "liboracle_ag4.so"
 REF_BIN = HERE / "_ref" / "autogrid4"
 REF_FULLPREC_BIN = HERE / "_ref" / "autogrid4_fullprec"
+# The reference source tree: AG_REFERENCE_SRC, or where this build's image
+# mounts it.  Only the oracle build and the tests that read the reference's
+# own test inputs use it; when it is absent those tests skip and the prebuilt
+# oracle/_ref binaries (if any) are used as they are.
 REFERENCE_SRC = Path(os.environ.get("AG_REFERENCE_SRC", "/root/reference"))
 
 EDGE_BIN, EDGE_CUTOFF, EDGE_ANGLE, EDGE_CLOSEH = 1, 2, 4, 8

@@ -9,7 +9,8 @@ ROOT = Path(__file__).resolve().parents[1]
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 
-REFERENCE = Path(os.environ.get("AG_REFERENCE_SRC", "/root/reference"))
+# the reference sources (tests that read them skip when they are absent)
+from oracle.oracle import REFERENCE_SRC as REFERENCE  # noqa: E402
 
 
 def pytest_configure(config):

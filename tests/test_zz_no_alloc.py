@@ -12,7 +12,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from conftest import tolerance_ok
+from conftest import make_case, tolerance_ok
 from test_oracle_pinning import GOLDEN, load_golden
 
 pytestmark = pytest.mark.gpu
@@ -26,13 +26,21 @@ def _bind(lib):
     return fn
 
 
-@pytest.mark.parametrize("case", ["basic_400", "types14_600", "constdiel_nbp"])
+def _problem(case, tmp_path):
+    if case == "synthetic_10000":
+        # 10,000 atoms on 41^3 points: many 512-atom chunks of the scratch's
+        # partial sums, and a dense interior for the FP64 near-pair branch
+        return make_case(tmp_path, "big", 10000, (40, 40, 40), seed=5)[1]
+    path = [p for p in GOLDEN if p.stem == case][0]
+    return load_golden(path, tmp_path)[2]
+
+
+@pytest.mark.parametrize("case", ["basic_400", "types14_600", "constdiel_nbp", "synthetic_10000"])
 def test_noalloc_emap_matches_regular_entry_point(case, tmp_path, built):
     import torch
     from autogrid_b200 import Context, load_library
     from autogrid_b200._abi import check
-    path = [p for p in GOLDEN if p.stem == case][0]
-    z, job, prob = load_golden(path, tmp_path)
+    prob = _problem(case, tmp_path)
     ctx = Context(0)
     regular = ctx.compute(prob, "fp32").reshape(prob.n_maps, -1)[prob.scalars["elec_map"]]
     ctx.close()
@@ -52,6 +60,7 @@ def test_noalloc_emap_matches_regular_entry_point(case, tmp_path, built):
         check(fn(0, prob.n_atoms, coord.data_ptr(), charge.data_ptr(), n1, sc["spacing"], sc["dddiel"],
                  reps.data_ptr(), sc["invdielcal"], sc["coeff_estat"], out.data_ptr(), None))
         torch.cuda.synchronize()
+        assert torch.cuda.current_device() == 0  # the caller's current device is left as it was
         if call == 1:  # the first call on a device resolves the static array's address
             assert torch.cuda.mem_get_info(0)[0] == free_before, "the no-alloc entry point changed free memory"
         got = out.cpu().numpy().astype(np.float64)
