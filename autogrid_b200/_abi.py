@@ -54,7 +54,7 @@ class ag_problem(C.Structure):
         ("separate_desolvation_maps", C.c_int32),
         ("cov_pos", C.c_double * 3), ("cov_half_width", C.c_double), ("cov_barrier", C.c_double),
         ("floating_grid", C.c_int32), ("constriction_grid", C.c_int32),
-        ("constriction_cutoff", C.c_double),
+        ("constriction_cutoff", C.c_double), ("report_collisions", C.c_int32),
     ]
 
 

@@ -42,7 +42,7 @@ class Problem:
     SCALARS = ("n_rec_types", "n_atom_maps", "n_maps", "elec_map", "dsolv_map", "spacing", "dddiel",
                "invdielcal", "coeff_estat", "solpar_q", "disorder_h", "hydrogen_type",
                "separate_desolvation_maps", "cov_half_width", "cov_barrier", "floating_grid",
-               "constriction_grid", "constriction_cutoff")
+               "constriction_grid", "constriction_cutoff", "report_collisions")
 
     def __init__(self, **kw):
         self.arrays = {}

@@ -235,12 +235,14 @@ struct ag_plan {
     bool any_cov = false;
     int floating = 0, constriction = 0;  // distance maps after the n_maps energy maps
     int far_mode = FAR_TAB_TABLE;        // how k_emap_far obtains far table values (FarArgs::tab_mode)
+    int tab_len = AG_NDIEL, far_clamp = 1;  // shared-memory far table (FarArgs::tab_len, clamp)
     float far_const = 0.f;
     double constriction_cutoff = 7.5;
     float *maps32 = nullptr;
     double *maps64 = nullptr;
     double *cov = nullptr;
     float *far_partial = nullptr;
+    uint32_t *edge_bits = nullptr;     // far-field bin guard: per (thread, atom) edge bits (FarArgs::edge_bits)
     ReduceInst *d_reduce = nullptr;    // e-map reduction of this plan (one instance)
     long long *d_reduce_begin = nullptr;
     double *x128 = nullptr, *y128 = nullptr, *z128 = nullptr;
@@ -254,8 +256,11 @@ struct ag_plan {
 
 namespace {
 
-// Validate an ag_problem against the limits of the reference build.
-ag_status validate(const ag_problem *p)
+// Validate an ag_problem against the limits of the reference build.  The
+// reference's grids are symmetric: n1 odd and ne = (n1-1)/2 (check_size.cpp:
+// 79-83, main.cpp:1083-1097).  symmetric = false accepts any box (n1 >= 1,
+// any offset ne), such as a z-slab of a grid (the differentiable mode's shards).
+ag_status validate(const ag_problem *p, bool symmetric = true)
 {
     if (!p) return invalid("null problem");
     if (p->n_atoms < 0 || p->n_atoms > AG_MAX_ATOMS) {
@@ -263,6 +268,11 @@ ag_status validate(const ag_problem *p)
         return AG_ERR_TOO_LARGE;
     }
     for (int i = 0; i < 3; i++) {
+        if (!symmetric) {
+            if (p->n1[i] < 1 || p->n1[i] > AG_MAX_GRID_PTS + 1 || p->ne[i] < -(1 << 20) || p->ne[i] > (1 << 20))
+                return invalid("n1 must be within [1, MAX_GRID_PTS+1] and |ne| <= 2^20");
+            continue;
+        }
         if (p->n1[i] < 1 || p->n1[i] > AG_MAX_GRID_PTS + 1 || (p->n1[i] % 2) != 1)
             return invalid("n1 must be odd and within [1, MAX_GRID_PTS+1]");
         if (p->ne[i] != (p->n1[i] - 1) / 2) return invalid("ne must equal (n1-1)/2");
@@ -309,6 +319,7 @@ ag_status validate(const ag_problem *p)
 // Internal accessors for the other host modules of the library.
 namespace agb {
 ag_status validate_problem(const ag_problem *p) { return validate(p); }
+ag_status validate_problem_box(const ag_problem *p) { return validate(p, false); }
 cudaStream_t context_stream(const ag_context *c) { return c->stream; }
 int context_device(const ag_context *c) { return c->device; }
 // True when kernels on `device` may dereference ptr: device memory of that
@@ -379,6 +390,7 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
     d.invdielcal = p->invdielcal; d.coeff_estat = p->coeff_estat; d.solpar_q = p->solpar_q;
     for (int i = 0; i < 3; i++) d.cov_pos[i] = p->cov_pos[i];
     d.cov_half_width = p->cov_half_width; d.cov_barrier = p->cov_barrier;
+    d.report_collisions = p->report_collisions ? 1 : 0;
     pl->h2d_bytes = 0;
     size_t *acc = &pl->h2d_bytes;
 
@@ -397,17 +409,45 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
         x128[a] = x[a] * AG_A_DIV; y128[a] = y[a] * AG_A_DIV; z128[a] = z[a] * AG_A_DIV;
         qw[a] = (float)(p->charge[a] * p->coeff_estat * AG_A_DIV);
     }
+    // The far kernel's table length: past the largest distance (bins) from an
+    // atom to any point the kernel evaluates -- the box padded to whole
+    // frames, whose points past the box are computed and not stored -- so
+    // that no pair's bin needs a clamp; the bins from NDIEL-1 on repeat its
+    // value (the reference clamps the bin, main.cpp:2956).  Beyond FAR_TAB_MAX
+    // the kernel clamps t instead.
+    {
+        const int padded[3] = {frames_x(p->n1[0]) * FRAME_X, frames_y(p->n1[1]) * FRAME_Y, frames_z(p->n1[2]) * FRAME_Z};
+        double dmax2 = 0.0;
+        for (int a = 0; a < N; a++) {
+            double d2 = 0.0;
+            for (int i = 0; i < 3; i++) {
+                const double c = i == 0 ? x[a] : (i == 1 ? y[a] : z[a]);
+                const double lo_c = (double)(-p->ne[i]) * p->spacing;
+                const double hi_c = (double)(padded[i] - 1 - p->ne[i]) * p->spacing;
+                const double dd = std::max(std::fabs(c - lo_c), std::fabs(c - hi_c));
+                d2 += dd * dd;
+            }
+            dmax2 = std::max(dmax2, d2);
+        }
+        const double tmax = std::sqrt(dmax2) * AG_A_DIV * (1.0 + 1.0e-5) + 8.0;
+        if (tmax < (double)FAR_TAB_MAX - 4.0) {
+            pl->far_clamp = 0;
+            pl->tab_len = ((int)std::ceil(tmax) + 4) / 4 * 4;
+        } else {
+            pl->far_clamp = 1;
+            pl->tab_len = AG_NDIEL;
+        }
+    }
+    const int TL = pl->tab_len;
     std::vector<float> far_tab;
     if (!dev_tables) {
-        // [0, NDIEL): the far kernel's table, zero below FAR_BIN0 (those pairs
-        // are the near kernel's); [NDIEL, 2 NDIEL): the whole table, for far
-        // pairs whose exact bin the bin guard finds below FAR_BIN0
-        far_tab.assign(2 * AG_NDIEL, 0.f);
-        for (int k = 0; k < AG_NDIEL; k++) {
-            const float f = (float)(p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal);
-            far_tab[AG_NDIEL + k] = f;
-            if (k >= AG_NEINT) far_tab[k] = f;
-        }
+        // [0, tab_len): the far kernel's table, zero below FAR_BIN0 (those
+        // pairs are the near kernel's), bin NDIEL-1 repeated past it;
+        // [tab_len, tab_len + NDIEL): the whole table, for far pairs whose
+        // exact bin the bin guard finds below FAR_BIN0
+        far_tab.assign((size_t)TL + AG_NDIEL, 0.f);
+        for (int k = 0; k < AG_NDIEL; k++) far_tab[TL + k] = (float)(p->dddiel ? p->r_epsilon_fn[k] : p->invdielcal);
+        for (int k = AG_NEINT; k < TL; k++) far_tab[k] = far_tab[TL + std::min(k, AG_NDIEL - 1)];
         // a constant dielectric needs no far-field table gather
         if (!p->dddiel) {
             pl->far_mode = FAR_TAB_CONST;
@@ -437,6 +477,12 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
         pl->far_partial = (float *)v;
     } else {
         pl->far_partial = nullptr;
+    }
+    pl->edge_bits = nullptr;
+    if (pl->far_partial && pl->far_mode != FAR_TAB_CONST) {
+        const int nframes = frames_x(d.n1x) * frames_y(d.n1y) * frames_z(d.n1z);
+        AGB_CK(B->ensure("edge_bits", far_edge_bits_bytes(pl->n_chunks, pl->chunk_atoms, nframes), &v));
+        pl->edge_bits = (uint32_t *)v;
     }
     AGB_CK(upload(B, "x128", x128.data(), N, &pl->x128, s, acc));
     AGB_CK(upload(B, "y128", y128.data(), N, &pl->y128, s, acc));
@@ -650,7 +696,7 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
         void *vv;
         AGB_CK(upload(B, "colmap", colmap.data(), colmap.size(), &dcol, s, acc));
         AGB_CK(B->ensure("vdwT", (size_t)nT * AG_NEINT * pl->mpad * sizeof(float), &vv)); pl->vdwT = (float *)vv;
-        AGB_CK(B->ensure("far_tab", 2 * AG_NDIEL * sizeof(float), &vv)); pl->far_tab = (float *)vv;
+        AGB_CK(B->ensure("far_tab", ((size_t)pl->tab_len + AG_NDIEL) * sizeof(float), &vv)); pl->far_tab = (float *)vv;
         AGB_CK(B->ensure("etab", AG_NDIEL * sizeof(float), &vv)); pl->etab = (float *)vv;
         AGB_CK(B->ensure("solf", AG_NDIEL * sizeof(float), &vv)); pl->solf = (float *)vv;
         AGB_CK(B->ensure("sol_fn", AG_NDIEL * sizeof(double), &vv)); dsolfn = (double *)vv;
@@ -659,7 +705,7 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
         AGB_CK(cudaMemsetAsync(pl->vdwT, 0, (size_t)nT * AG_NEINT * pl->mpad * sizeof(float), s));
         AGB_CK(launch_pack_tables(p->e_vdw_hb, p->n_rec_types, nAM, dcol, pl->mpad, pl->vdwT, p->sol_fn,
                                   p->dddiel ? p->r_epsilon_fn : nullptr, p->dddiel, p->invdielcal, p->coeff_estat,
-                                  pl->far_tab, pl->etab, pl->solf, dreps, s));
+                                  pl->far_tab, pl->tab_len, pl->etab, pl->solf, dreps, s));
     }
 
     d.x = dx; d.y = dy; d.z = dz; d.q = dq; d.vol = dvol; d.solpar = dsol; d.rv = drv; d.rv2 = drv2;
@@ -735,8 +781,12 @@ FarArgs far_args(const ag_plan *pl)
     a.nfx = frames_x(d.n1x); a.nfy = frames_y(d.n1y); a.nfz = frames_z(d.n1z);
     a.tab_mode = pl->far_mode;
     a.tab_const = pl->far_const;
-    a.tab_full = pl->far_tab ? pl->far_tab + AG_NDIEL : nullptr;
+    a.tab_full = pl->far_tab ? pl->far_tab + pl->tab_len : nullptr;
+    a.tab_len = pl->far_mode == FAR_TAB_CONST ? 0 : pl->tab_len;
+    a.clamp = pl->far_clamp;
     far_guard(a.spacing_adiv, &a.edge_lo, &a.edge_hi);
+    a.edge_bits = pl->edge_bits;
+    a.edge_words = far_edge_words(pl->chunk_atoms);
     a.edge_counters = pl->ctx ? pl->ctx->d_counters + 2 : nullptr;
     return a;
 }
@@ -763,7 +813,9 @@ ag_status launch_far_slab(ag_plan *pl, cudaStream_t s, int k, int nslab)
     int z0, z1;
     slab_range(pl->dp, k, &z0, &z1);
     const int fz0 = z0 / FRAME_Z, fz1 = (k == nslab - 1) ? -1 : z1 / FRAME_Z;
-    AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, fz0, fz1));
+    const FarArgs fa = far_args(pl);
+    AGB_CK(launch_emap_far(fa, pl->n_chunks, 512, c->side, fz0, fz1));
+    AGB_CK(launch_far_fixup(fa, pl->n_chunks, c->side, fz0, fz1));
     AGB_CK(cudaEventRecord(c->far_done[k], c->side));
     if (k == nslab - 1) AGB_CK(cudaEventRecord(c->evf1, c->side));
     return AG_OK;
@@ -811,6 +863,25 @@ ag_status enqueue_slabs(ag_plan *pl, cudaStream_t s, int nslab, int &launches)
 }
 
 
+// 'map_receptor_interior off': the collision rule over points [lin0, lin1),
+// after the e map and the distance maps are complete.
+ag_status launch_plan_collisions(ag_plan *pl, cudaStream_t s, long long lin0, long long lin1)
+{
+    const DevProblem &d = pl->dp;
+    const size_t P = (size_t)d.P, f = (size_t)d.n_maps * P, cc = f + (size_t)pl->floating * P;
+    if (pl->maps64)
+        AGB_CK(launch_collisions(d, lin0, lin1, pl->constriction_cutoff, nullptr, nullptr, nullptr,
+                                 d.elec_map >= 0 ? pl->maps64 + (size_t)d.elec_map * P : nullptr,
+                                 pl->floating ? pl->maps64 + f : nullptr, pl->constriction ? pl->maps64 + cc : nullptr,
+                                 s));
+    else
+        AGB_CK(launch_collisions(d, lin0, lin1, pl->constriction_cutoff,
+                                 d.elec_map >= 0 ? pl->maps32 + (size_t)d.elec_map * P : nullptr,
+                                 pl->floating ? pl->maps32 + f : nullptr, pl->constriction ? pl->maps32 + cc : nullptr,
+                                 nullptr, nullptr, nullptr, s));
+    return AG_OK;
+}
+
 // A z-slab [z0, z1) of the grid is a shard of the map set: its points need
 // every atom but no other plane.  z0 is a multiple of FRAME_Z (whole far-field
 // frame rows, which hold whole near-field brick rows) and z1 one too or n1z.
@@ -841,7 +912,9 @@ ag_status run_plan_zrange(ag_plan *pl, cudaStream_t s, int z0, int z1)
         AGB_CK(cudaEventRecord(c->fork, s));
         AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
         AGB_CK(cudaEventRecord(c->evf0, c->side));
-        AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, c->side, z0 / FRAME_Z, last ? -1 : z1 / FRAME_Z));
+        const FarArgs fa = far_args(pl);
+        AGB_CK(launch_emap_far(fa, pl->n_chunks, 512, c->side, z0 / FRAME_Z, last ? -1 : z1 / FRAME_Z));
+        AGB_CK(launch_far_fixup(fa, pl->n_chunks, c->side, z0 / FRAME_Z, last ? -1 : z1 / FRAME_Z));
         AGB_CK(cudaEventRecord(c->evf1, c->side));
         AGB_CK(cudaEventRecord(c->join, c->side));
         launches++;
@@ -867,6 +940,12 @@ ag_status run_plan_zrange(ag_plan *pl, cudaStream_t s, int z0, int z1)
         const ReduceInst r{d.P, pl->n_chunks, pl->far_partial, pl->maps32 + (size_t)d.elec_map * d.P};
         AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
         AGB_CK(launch_emap_reduce_range(r, (long long)z0 * plane, (long long)z1 * plane, s));
+        launches++;
+    }
+    if (d.report_collisions) {
+        const long long plane = (long long)d.n1x * d.n1y;
+        ag_status st = launch_plan_collisions(pl, s, (long long)z0 * plane, (long long)z1 * plane);
+        if (st != AG_OK) return st;
         launches++;
     }
     AGB_CK(cudaEventRecord(c->ev1, s));
@@ -901,7 +980,9 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
             AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
         }
         AGB_CK(cudaEventRecord(c->evf0, fs));
-        AGB_CK(launch_emap_far(far_args(pl), pl->n_chunks, 512, fs));
+        const FarArgs fa = far_args(pl);
+        AGB_CK(launch_emap_far(fa, pl->n_chunks, 512, fs));
+        AGB_CK(launch_far_fixup(fa, pl->n_chunks, fs));
         AGB_CK(cudaEventRecord(c->evf1, fs));
         if (!serial) AGB_CK(cudaEventRecord(c->join, fs));
         launches++;
@@ -931,6 +1012,11 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
     if (far) {
         if (!serial) AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
         AGB_CK(launch_emap_reduce(pl->d_reduce, pl->d_reduce_begin, 1, d.P, s));
+        launches++;
+    }
+    if (d.report_collisions) {
+        ag_status st = launch_plan_collisions(pl, s, 0, d.P);
+        if (st != AG_OK) return st;
         launches++;
     }
     AGB_CK(cudaEventRecord(c->ev1, s));
@@ -1012,6 +1098,7 @@ ag_status batch_upload_far(ag_batch *b, bool chunked)
     for (size_t i = 0; i < b->far.size(); i++) {
         FarArgs &a = b->far[i];
         a.chunk_atoms = chunked ? std::min(2048, std::max(a.n_atoms, 1)) : std::max(a.n_atoms, 1);
+        a.edge_words = far_edge_words(a.chunk_atoms);
         b->far_begin.push_back(b->far_begin.back() + (a.n_atoms > 0 ? far_units(a) : 0));
     }
     // e-map reduction: each instance's partial chunks, for this chunking
@@ -1049,9 +1136,13 @@ ag_status batch_launch(ag_batch *b, cudaStream_t s, int tile, int shape, cudaEve
         AGB_CK(cudaStreamWaitEvent(c->side, c->fork, 0));
         fs = c->side;
     }
-    if (far)
+    if (far) {
+        int max_tab = 0;
+        for (const FarArgs &fa : b->far) max_tab = std::max(max_tab, fa.tab_len);
         AGB_CK(launch_emap_far_batch(b->d_far, b->d_far_begin, (int)b->far.size(), b->d_counters, tile,
-                                     b->far_ctas_per_sm, fs));
+                                     b->far_ctas_per_sm, max_tab, fs));
+        AGB_CK(launch_far_fixup_batch(b->d_far, b->d_far_begin, (int)b->far.size(), b->far_begin.back(), fs));
+    }
     if (far && concurrent) AGB_CK(cudaEventRecord(c->join, fs));
     if (e1) AGB_CK(cudaEventRecord(e1, s));
     if (b->near_begin.back() > 0)
@@ -1300,7 +1391,9 @@ static ag_status compute_common(ag_context *ctx, const ag_problem *problem, cons
 {
     if (!maps) return invalid("null maps");
     ag_plan *pl = nullptr;
-    const bool pipelined = elem == 4 && problem && problem->n1[2] > kSlabZ && !(opts && opts->serial);
+    // the collision rule rewrites finished planes: one-shot calls with it do not pipeline copies
+    const bool pipelined = elem == 4 && problem && problem->n1[2] > kSlabZ && !(opts && opts->serial) &&
+                           !problem->report_collisions;
     ag_status st = make_plan(ctx, problem, opts, false, &pl, nullptr, pipelined);
     if (st != AG_OK) return st;
     std::unique_ptr<ag_plan> guard(pl);
@@ -1343,7 +1436,8 @@ ag_status ag_maps_compute_zslab(ag_context *ctx, const ag_problem *problem, cons
     AGB_CK(dg.err);
     ag_plan *pl = nullptr;
     // the one-shot call's far-field chunking (bit-identical planes), no early launch
-    st = make_plan(ctx, problem, opts, false, &pl, nullptr, problem->n1[2] > kSlabZ, nullptr, false);
+    st = make_plan(ctx, problem, opts, false, &pl, nullptr, problem->n1[2] > kSlabZ && !problem->report_collisions,
+                   nullptr, false);
     if (st != AG_OK) return st;
     std::unique_ptr<ag_plan> guard(pl);
     st = run_plan_zrange(pl, ctx->stream, z0, z1);
@@ -1626,16 +1720,17 @@ static ag_status batch_create(ag_context *ctx, const ag_problem *const *problems
     ag_opts o{};
     if (opts) o = *opts;
     if (o.precision != AG_PREC_FP32) return invalid("batches run the FP32 path");
+    for (int i = 0; i < n; i++)
+        if (problems[i] && problems[i]->report_collisions) {
+            set_last_error("instance " + std::to_string(i) + ": batches do not report collisions "
+                           "(map_receptor_interior off); use ag_maps_compute");
+            return AG_ERR_UNSUPPORTED;
+        }
     AGB_CK(cudaSetDevice(ctx->device));
     std::unique_ptr<ag_batch> b(new ag_batch());
     b->ctx = ctx;
     b->stream = us;
     b->arena.reset(new Arena(&ctx->blocks));
-    for (int i = 0; i < n; i++)
-        if (problems[i] && (problems[i]->floating_grid || problems[i]->constriction_grid)) {
-            set_last_error("ag_batch_create: batches compute the energy maps only (no fmap/cmap)");
-            return AG_ERR_UNSUPPORTED;
-        }
     // Instance plans (validation, cell lists, packed atoms, tables, uploads)
     // are built by a pool of host threads; device buffers come from the arena.
     b->plans.resize(n);
@@ -1678,6 +1773,15 @@ static ag_status batch_create(ag_context *ctx, const ag_problem *const *problems
             void *v = nullptr;
             AGB_CK(pl->bufs->ensure("far_partial", (size_t)max_chunks * (size_t)pl->dp.P * sizeof(float), &v));
             pl->far_partial = (float *)v;
+            if (pl->far_mode != FAR_TAB_CONST) {
+                // edge bits for either chunking of batch_upload_far (2048-atom chunks or all atoms)
+                const int nframes = frames_x(pl->dp.n1x) * frames_y(pl->dp.n1y) * frames_z(pl->dp.n1z);
+                const int na = std::max(pl->dp.n_atoms, 1);
+                const size_t eb = std::max(far_edge_bits_bytes(max_chunks, std::min(2048, na), nframes),
+                                           far_edge_bits_bytes(1, na, nframes));
+                AGB_CK(pl->bufs->ensure("edge_bits", eb, &v));
+                pl->edge_bits = (uint32_t *)v;
+            }
             b->far.push_back(far_args(pl));
             b->red.push_back(ReduceInst{pl->dp.P, 0, pl->far_partial, pl->maps32 + (size_t)pl->dp.elec_map * pl->dp.P});
             b->red_begin.push_back(b->red_begin.back() + pl->dp.P);
@@ -1695,6 +1799,13 @@ static ag_status batch_create(ag_context *ctx, const ag_problem *const *problems
             }
         if (pl->any_cov) {
             AGB_CK(launch_covalent(pl->dp, pl->cov, us));  // geometry only: computed once
+        }
+        if (pl->floating || pl->constriction) {
+            // the floating and constriction grids depend on the geometry only:
+            // computed once, after the instance's energy maps (main.cpp:2958-2966)
+            const size_t P = (size_t)pl->dp.P, f = (size_t)pl->dp.n_maps * P, c = f + (size_t)pl->floating * P;
+            AGB_CK(launch_distance_maps(pl->dp, pl->constriction_cutoff, pl->floating ? pl->maps32 + f : nullptr,
+                                        pl->constriction ? pl->maps32 + c : nullptr, nullptr, nullptr, us));
         }
     }
     void *v = nullptr;
@@ -1771,8 +1882,9 @@ ag_status ag_batch_download(ag_batch *b, int32_t i, float *host_maps)
 {
     if (!b || !host_maps || i < 0 || i >= (int32_t)b->plans.size()) return invalid("ag_batch_download: bad argument");
     const ag_plan *pl = b->plans[i].get();
-    AGB_CK(cudaMemcpyAsync(host_maps, pl->maps32, (size_t)pl->dp.n_maps * (size_t)pl->dp.P * sizeof(float),
-                           cudaMemcpyDefault, b->ctx->stream));
+    const size_t n_out = (size_t)pl->dp.n_maps + pl->floating + pl->constriction;
+    AGB_CK(cudaMemcpyAsync(host_maps, pl->maps32, n_out * (size_t)pl->dp.P * sizeof(float), cudaMemcpyDefault,
+                           b->ctx->stream));
     AGB_CK(cudaStreamSynchronize(b->ctx->stream));
     return AG_OK;
 }
@@ -1822,10 +1934,6 @@ ag_status ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *proble
             set_last_error("instance " + std::to_string(i) + ": " + ag_last_error());
             return vs;
         }
-        if (problems[i]->floating_grid || problems[i]->constriction_grid) {
-            set_last_error("ag_batch_create: batches compute the energy maps only (no fmap/cmap)");
-            return AG_ERR_UNSUPPORTED;
-        }
     }
     std::vector<int> order(n);
     for (int i = 0; i < n; i++) order[i] = i;
@@ -1860,7 +1968,8 @@ ag_status ag_maps_compute_batch(ag_context *ctx, const ag_problem *const *proble
         if ((ce = cudaStreamWaitEvent(ctx->copy, done[g], 0)) != cudaSuccess) break;
         for (size_t k = 0; k < groups[g].size() && ce == cudaSuccess; k++) {
             const ag_plan *pl = batches[g]->plans[k].get();
-            ce = cudaMemcpyAsync(maps[groups[g][k]], pl->maps32, (size_t)pl->dp.n_maps * (size_t)pl->dp.P * sizeof(float),
+            ce = cudaMemcpyAsync(maps[groups[g][k]], pl->maps32,
+                                 ((size_t)pl->dp.n_maps + pl->floating + pl->constriction) * (size_t)pl->dp.P * sizeof(float),
                                  cudaMemcpyDefault, ctx->copy);
         }
     }

@@ -11,10 +11,12 @@
 
 #include "autogrid_b200.h"
 #include "kernels/diff.h"
+#include "kernels/kernels.h"
 
 namespace agb {
 void set_last_error(const std::string &m);
 ag_status validate_problem(const ag_problem *p);
+ag_status validate_problem_box(const ag_problem *p);
 cudaStream_t context_stream(const ag_context *c);
 int context_device(const ag_context *c);
 bool device_accessible(const void *ptr, int device);
@@ -64,6 +66,9 @@ struct ag_diff {
     bool fp64 = false;
     size_t esz = 4;
     int N = 0, n_conf = 1, n_maps = 0, n_atom_maps = 0, elec = -1;
+    // distance maps after the energy maps (main.cpp:2958-2966): n_out maps per conformer
+    int floating = 0, constriction = 0, n_out = 0;
+    double cmap_cutoff = 7.5;
     bool need_h = false;
     long long P = 0;
     size_t ncells = 0;
@@ -101,7 +106,8 @@ struct ag_diff {
         }
         return e;
     }
-    size_t map_bytes() const { return esz * (size_t)P * n_maps * n_conf; }
+    size_t map_bytes() const { return esz * (size_t)P * n_out * n_conf; }
+    DevProblem conformer_geometry(int k) const;
     ag_status upload_conformer(int k);
     ag_status refresh_host();
 };
@@ -150,6 +156,20 @@ bool act_uses_angles(uint8_t a) { return a != DA_PLAIN && a != DA_NONE; }
 bool act_uses_ramp(uint8_t a) { return a == DA_SUMA || a == DA_SUMA_DIS || a == DA_SUMD_DIS; }
 
 }  // namespace
+
+// The distance-map kernels' view of conformer k: its atoms and the grid.
+DevProblem ag_diff::conformer_geometry(int k) const
+{
+    DevProblem g;
+    std::memset(&g, 0, sizeof g);
+    g.n_atoms = N;
+    g.n1x = args.n1x; g.n1y = args.n1y; g.n1z = args.n1z;
+    g.nex = args.nex; g.ney = args.ney; g.nez = args.nez;
+    g.P = P;
+    g.spacing = args.spacing;
+    g.x = d_x + (size_t)N * k; g.y = d_y + (size_t)N * k; g.z = d_z + (size_t)N * k;
+    return g;
+}
 
 // Coordinates, charges, bond vectors and cell list of conformer k.
 ag_status ag_diff::upload_conformer(int k)
@@ -234,14 +254,14 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
         set_last_error("ag_diff_create: unknown precision");
         return AG_ERR_INVALID;
     }
-    if (p->floating_grid || p->constriction_grid) {
-        set_last_error("ag_diff_create: the differentiable mode computes the energy maps only (no fmap/cmap)");
+    if (p->report_collisions) {
+        set_last_error("ag_diff_create: the differentiable mode does not report collisions (map_receptor_interior off)");
         return AG_ERR_UNSUPPORTED;
     }
     // the closest-hydrogen requirement is checked below, only if a map uses Hramp
     ag_problem pv = *p;
     const int nAM = p->n_atom_maps;
-    ag_status st = validate_problem(&pv);
+    ag_status st = validate_problem_box(&pv);  // any box: a z-slab of a grid is a shard
     if (st != AG_OK && st != AG_ERR_NO_CLOSEST_H) return st;
     // tables in device memory (ag_tables_build): read them here once; the
     // interpolation pairs are formed on the host at creation
@@ -330,6 +350,10 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
     d->N = p->n_atoms;
     d->n_conf = n_conformers;
     d->n_maps = p->n_maps;
+    d->floating = p->floating_grid ? 1 : 0;
+    d->constriction = p->constriction_grid ? 1 : 0;
+    d->cmap_cutoff = p->constriction_cutoff;
+    d->n_out = d->n_maps + d->floating + d->constriction;
     d->n_atom_maps = nAM;
     d->elec = p->elec_map;
     d->need_h = need_h;
@@ -373,7 +397,7 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
     A.elec_map = p->elec_map;
     A.n_slots = (int)slots.size();
     A.n_mm = n_mm;
-    A.n_maps_out = p->n_maps;
+    A.n_maps_out = d->n_out;  // per-conformer stride of the maps (energy maps, then fmap/cmap)
     A.tab_stride = std::max(4, (A.n_slots + 3) / 4 * 4);
     for (int s = 0; s < A.n_slots; s++) {
         const Slot &sl = slots[s];
@@ -391,7 +415,7 @@ ag_status ag_diff_create_batch(ag_context *ctx, const ag_problem *p, const ag_op
     const double span = (DF_BRICK_X - 1) * p->spacing + 2 * DF_RADIUS;
     A.cell_size = std::max(4.0, span / 5.0);
     for (int i = 0; i < 3; i++) {
-        const double lo = -p->ne[i] * p->spacing - DF_RADIUS, hi = p->ne[i] * p->spacing + DF_RADIUS;
+        const double lo = -p->ne[i] * p->spacing - DF_RADIUS, hi = (p->n1[i] - 1 - p->ne[i]) * p->spacing + DF_RADIUS;
         A.cell0[i] = lo;
         const int n = (int)std::ceil((hi - lo) / A.cell_size) + 1;
         if (i == 0) A.ncx = n; else if (i == 1) A.ncy = n; else A.ncz = n;
@@ -497,6 +521,19 @@ ag_status ag_diff_forward(ag_diff *d, int32_t keep_closest_h, void *device_out)
     DF_CK(cudaEventRecord(d->ev[0], s));
     if (d->elec >= 0) DF_CK(launch_emap_lin(d->fp64, A, d->d_eps, out + d->esz * d->P * d->elec, s));
     DF_CK(launch_near_lin(d->fp64, A, d->d_vdw, d->d_sol, out, d->d_ch, d->d_mmarg, s));
+    if (d->floating || d->constriction)
+        for (int k = 0; k < d->n_conf; k++) {
+            // floating and constriction grids of conformer k (FP64, the reference's distances)
+            unsigned char *base = out + d->esz * (size_t)d->P * ((size_t)k * d->n_out + d->n_maps);
+            unsigned char *fm = d->floating ? base : nullptr;
+            unsigned char *cm = d->constriction ? base + d->esz * (size_t)d->P * d->floating : nullptr;
+            if (d->fp64)
+                DF_CK(launch_distance_maps(d->conformer_geometry(k), d->cmap_cutoff, nullptr, nullptr, (double *)fm,
+                                           (double *)cm, s));
+            else
+                DF_CK(launch_distance_maps(d->conformer_geometry(k), d->cmap_cutoff, (float *)fm, (float *)cm, nullptr,
+                                           nullptr, s));
+        }
     DF_CK(cudaEventRecord(d->ev[1], s));
     DF_CK(cudaStreamSynchronize(s));
     DF_CK(cudaEventElapsedTime(&d->fwd_ms, d->ev[0], d->ev[1]));
@@ -560,6 +597,11 @@ ag_status ag_diff_backward(ag_diff *d, const void *grad_maps, int32_t grad_on_de
     DF_CK(cudaEventRecord(d->ev[2], s));
     if (d->elec >= 0) DF_CK(launch_emap_lin_adj(d->fp64, d->args, d->d_eps, gm + d->esz * d->P * d->elec, g, s));
     DF_CK(launch_near_lin_adj(d->fp64, d->args, d->d_vdw, d->d_sol, gm, d->d_ch, d->d_mmarg, g, s));
+    if (d->floating)  // the constriction grid is piecewise constant: no gradient
+        for (size_t k = 0; k < K; k++)
+            DF_CK(launch_fmap_adjoint(d->conformer_geometry((int)k),
+                                      gm + d->esz * (size_t)d->P * (k * d->n_out + d->n_maps), d->fp64,
+                                      d->d_grad + 10 * N * k, s));
     DF_CK(cudaEventRecord(d->ev[3], s));
     for (size_t k = 0; k < K; k++) {
         const double *base = d->d_grad + 10 * N * k;

@@ -216,7 +216,11 @@ struct Job {
     std::string floating_filename, constriction_filename;
     std::FILE *floating_fp = nullptr, *constriction_fp = nullptr;
     double constriction_cutoff = 7.5;
-    bool map_receptor_interior = false;
+    // The reference's default build never tests collisions (main.cpp:2893-2927
+    // is compiled out); its USE_BHTREE build tests them unless the GPF says
+    // "map_receptor_interior on" (main.cpp:580).  This front end keeps the
+    // default build's behaviour unless the GPF says "off".
+    bool map_receptor_interior = true;
 
     // physics switches
     double covpos[3] = {0, 0, 0}, covhalfwidth = 1.0, covbarrier = 1000.0;
@@ -679,8 +683,16 @@ void Job::load(const std::string &gpf)
             case K_MAP_RECEPTOR_INTERIOR: {  // main.cpp:1642-1659
                 char tok[64] = "true";
                 std::sscanf(line, "%*s %63s", tok);
-                if (strcasecmp(tok, "true") == 0 || strcasecmp(tok, "on") == 0) map_receptor_interior = true;
-                else fatal("'map_receptor_interior off'  is supported only with USE_BHTREE.", AG_ERR_UNSUPPORTED);
+                // the reference's USE_BHTREE build accepts "off" (collisions
+                // reported); its default build stops with a fatal error there.
+                // This front end takes the USE_BHTREE behaviour.
+                if (strcasecmp(tok, "true") == 0 || strcasecmp(tok, "on") == 0) {
+                    map_receptor_interior = true;
+                    log("Mapping receptor interior instead of reporting collision if nearer than 1.50 to any atom.");
+                } else {
+                    map_receptor_interior = false;
+                    log("Reporting collision if nearer than 1.50 to any atom.");
+                }
             } break;
             case K_FMAP: case K_CMAP: {  // main.cpp:1663-1695
                 const bool fm = (kw == K_FMAP);
@@ -1254,6 +1266,7 @@ void Job::make_problem()
     p.floating_grid = floating_grid ? 1 : 0;
     p.constriction_grid = constriction_grid ? 1 : 0;
     p.constriction_cutoff = constriction_cutoff;
+    p.report_collisions = map_receptor_interior ? 0 : 1;
 }
 
 // ------------------------------------------------------------- map writer --

@@ -90,11 +90,20 @@ struct FarArgs {
     float tab_const;
     // Bin-edge guard (FAR_TAB_TABLE): the kernel takes the bins of t*edge_lo
     // and t*edge_hi, edge_lo/hi = 1 -/+ d with d above the relative error of
-    // the FP32 distance t; pairs whose two bins differ get their bin in FP64
+    // the FP32 distance t, and sets a bit per (thread, atom) with a pair whose
+    // two bins differ in edge_bits (edge_words 32-bit words per thread and
+    // unit); the fix-up kernel gives those pairs their bin in FP64
     // (far_exact_bin).  tab_full [NDIEL]: the table without the zeros below
     // FAR_BIN0, for pairs whose exact bin is there.
     float edge_lo, edge_hi;
     const float *tab_full;
+    uint32_t *edge_bits;
+    int edge_words;
+    // The shared-memory table: tab_len floats of far_tab (a multiple of 4).
+    // clamp = 1: tab_len = NDIEL and t is clamped at FAR_CLAMP_T; clamp = 0:
+    // the table repeats bin NDIEL-1 up to a length that covers every distance
+    // of the instance (far_table_len), and t is used unclamped.
+    int tab_len, clamp;
     // [0] guarded pairs resolved in FP64, [1] of those, pairs whose plain FP32
     // bin floor(t) was not the exact bin, [2] pairs decided by the reference's
     // own expression because their FP64 squared distance lies within 1e-12 of
@@ -102,6 +111,8 @@ struct FarArgs {
     unsigned long long *edge_counters;
 };
 enum { FAR_TAB_TABLE = 0, FAR_TAB_CONST = 2 };
+// Longest extended far table (bins): 128 A.  Instances with longer distances clamp.
+constexpr int FAR_TAB_MAX = 16384;
 
 // Guard multipliers for a grid: the relative error bound of the canonical
 // FP32 distance t of a far pair (t >= FAR_T0 bins), rounded up so that 1 - d
@@ -137,6 +148,7 @@ struct DevProblem {
     double invdielcal, coeff_estat, solpar_q;
     double cov_pos[3], cov_half_width, cov_barrier;
     int any_covalent;
+    int report_collisions;             // 'map_receptor_interior off' (ag_problem)
 
     // atoms in file order (FP64, centred)
     const double *x, *y, *z, *q, *vol, *solpar;

@@ -39,14 +39,22 @@ struct NearInst {
 };
 
 
-size_t far_smem_bytes(int tile);
+size_t far_smem_bytes(int tile, int tab_len);
 // Dynamic shared-memory limits of the far kernels on the current device.
 cudaError_t prepare_far_kernels();
 cudaError_t launch_far_bins_debug(const FarArgs &a, const long long *pts, int n_pts, int *used, int *fp32, int *flags,
                                   cudaStream_t s);
 cudaError_t launch_emap_far(const FarArgs &a, int n_chunks, int tile, cudaStream_t s, int fz0 = 0, int fz1 = -1);
 cudaError_t launch_emap_far_batch(const FarArgs *insts, const long long *unit_begin, int n_inst,
-                                  unsigned long long *counter, int tile, int ctas_per_sm, cudaStream_t s);
+                                  unsigned long long *counter, int tile, int ctas_per_sm, int max_tab_len,
+                                  cudaStream_t s);
+// The far-field bin fix-up after launch_emap_far (same frames) / the batch kernel.
+cudaError_t launch_far_fixup(const FarArgs &a, int n_chunks, cudaStream_t s, int fz0 = 0, int fz1 = -1);
+cudaError_t launch_far_fixup_batch(const FarArgs *insts, const long long *unit_begin, int n_inst, long long n_units,
+                                   cudaStream_t s);
+// Bytes of the edge-bit words of one instance: chunks x frames x words x threads.
+size_t far_edge_bits_bytes(int n_chunks, int chunk_atoms, int nframes);
+int far_edge_words(int chunk_atoms);
 // One instance of the e-map reduction: out[lin] = sum_c partial[c][lin] + out[lin].
 struct ReduceInst {
     long long P;
@@ -61,6 +69,15 @@ cudaError_t launch_emap_exact(const DevProblem &p, double *emap, cudaStream_t s)
 cudaError_t launch_covalent(const DevProblem &p, double *cov, cudaStream_t s);
 cudaError_t launch_distance_maps(const DevProblem &p, double cutoff, float *fmap32, float *cmap32, double *fmap64,
                                  double *cmap64, cudaStream_t s);
+// 'map_receptor_interior off': collision points of [lin0, lin1) get e = 0 and
+// fmap = 1.5, the constriction grid the BH tree's single-precision count
+// (any map pointer may be null).
+cudaError_t launch_collisions(const DevProblem &p, long long lin0, long long lin1, double cc_cut, float *emap32,
+                              float *fmap32, float *cmap32, double *emap64, double *fmap64, double *cmap64,
+                              cudaStream_t s);
+// Adjoint of the floating grid (dL/d(coord) of the nearest atom of each point),
+// added into g_xyz [3N] (FP64); g_fmap [P] in FP32 or FP64.
+cudaError_t launch_fmap_adjoint(const DevProblem &p, const void *g_fmap, bool fp64, double *g_xyz, cudaStream_t s);
 int near_bricks(const DevProblem &p, int shape);
 cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int shape,
                         cudaStream_t s, int bz0 = 0, int bz1 = -1);

@@ -119,8 +119,9 @@ __global__ void __launch_bounds__(kThreads) k_sol_eps(TableArgs a, double *sol_f
 }
 
 // Plan tables from device-resident problem tables: vdwT [type][bin][mpad]
-// (column c holds map colmap[c], or zeros), far_tab [2][NDIEL] (zero below
-// FAR_BIN0, then the whole table) / etab / solf (FP32) and
+// (column c holds map colmap[c], or zeros), far_tab [tab_len + NDIEL] (the
+// far kernel's table: zero below FAR_BIN0, bin NDIEL-1 repeated up to
+// tab_len; then the whole table) / etab / solf (FP32) and
 // reps (FP64, distance-dependent dielectric only).
 __global__ void __launch_bounds__(kThreads) k_pack_vdw(const float *e_vdw_hb, int n_rec_types, int n_atom_maps,
                                                        const int *colmap, int mpad, float *vdwT)
@@ -137,14 +138,18 @@ __global__ void __launch_bounds__(kThreads) k_pack_vdw(const float *e_vdw_hb, in
 
 __global__ void __launch_bounds__(kThreads) k_pack_lines(const double *sol_fn, const double *r_eps, int dddiel,
                                                          double invdielcal, double coeff_estat, float *far_tab,
-                                                         float *etab, float *solf, double *reps)
+                                                         int tab_len, float *etab, float *solf, double *reps)
 {
     const int k = blockIdx.x * kThreads + threadIdx.x;
+    if (k >= AG_NDIEL && k < tab_len) {  // the far table's extension repeats its last bin
+        far_tab[k] = (float)(dddiel ? r_eps[AG_NDIEL - 1] : invdielcal);
+        return;
+    }
     if (k >= AG_NDIEL) return;
     const double f = dddiel ? r_eps[k] : invdielcal;
     if (reps) reps[k] = dddiel ? r_eps[k] : 0.0;
-    far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
-    far_tab[AG_NDIEL + k] = (float)f;  // the whole table, for the far kernel's bin guard
+    if (k < tab_len) far_tab[k] = k < AG_NEINT ? 0.f : (float)f;
+    far_tab[tab_len + k] = (float)f;  // the whole table, for the far kernel's bin guard
     etab[k] = (float)__dmul_rn(f, coeff_estat);
     solf[k] = (float)sol_fn[k];
 }
@@ -167,13 +172,14 @@ cudaError_t launch_tables_build(const TableArgs &a, float *raw, float *e_vdw_hb,
 
 cudaError_t launch_pack_tables(const float *e_vdw_hb, int n_rec_types, int n_atom_maps, const int *colmap, int mpad,
                                float *vdwT, const double *sol_fn, const double *r_eps, int dddiel, double invdielcal,
-                               double coeff_estat, float *far_tab, float *etab, float *solf, double *reps,
-                               cudaStream_t s)
+                               double coeff_estat, float *far_tab, int tab_len, float *etab, float *solf,
+                               double *reps, cudaStream_t s)
 {
     const long long n = (long long)n_rec_types * AG_NEINT * mpad;
     if (n > 0) k_pack_vdw<<<blocks_for(n), kThreads, 0, s>>>(e_vdw_hb, n_rec_types, n_atom_maps, colmap, mpad, vdwT);
-    k_pack_lines<<<blocks_for(AG_NDIEL), kThreads, 0, s>>>(sol_fn, r_eps, dddiel, invdielcal, coeff_estat, far_tab,
-                                                            etab, solf, reps);
+    k_pack_lines<<<blocks_for(std::max(AG_NDIEL, tab_len)), kThreads, 0, s>>>(sol_fn, r_eps, dddiel, invdielcal,
+                                                                               coeff_estat, far_tab, tab_len, etab,
+                                                                               solf, reps);
     return cudaGetLastError();
 }
 

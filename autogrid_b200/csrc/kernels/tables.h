@@ -22,7 +22,7 @@ cudaError_t launch_tables_build(const TableArgs &a, float *raw, float *e_vdw_hb,
 // vdW column, -1 for none).
 cudaError_t launch_pack_tables(const float *e_vdw_hb, int n_rec_types, int n_atom_maps, const int *colmap, int mpad,
                                float *vdwT, const double *sol_fn, const double *r_eps, int dddiel, double invdielcal,
-                               double coeff_estat, float *far_tab, float *etab, float *solf, double *reps,
-                               cudaStream_t s);
+                               double coeff_estat, float *far_tab, int tab_len, float *etab, float *solf,
+                               double *reps, cudaStream_t s);
 
 }  // namespace agb

@@ -309,6 +309,8 @@ def main():
             line["differentiable"] = differentiable_maps(ctx, work, stream)
         if not args.no_vina and world == 1:
             line["vina_conformers"] = vina_conformers(ctx, work, stream)
+        if world == 1:
+            line["cli_e2e"] = cli_e2e(work, P * M)
         if not args.no_cpu_baseline and world == 1:
             threads = min(32, os.cpu_count() or 1)
             res = reference_sample(rec, spec, work, threads)
@@ -461,6 +463,28 @@ def batched_ensemble(ctx, n, work: Path, stream):
             "plain_per_box_ms": plain_ms, "plain_per_box_evals_per_s": evals / (plain_ms * 1e-3),
             "speedup_vs_plain_per_box": plain_ms / batch_ms, "max_diff_over_tolerance": worst,
             "create_s": create_s, "tuning": tune}
+
+
+def cli_e2e(work: Path, evals: int):
+    """The drop-in executable end to end on the same map set: `autogrid4_b200
+    -p bench.gpf -l cli.glg` as a user runs it (process start, CUDA context,
+    GPF and PDBQT parsing, tables, bond vectors, maps, map text formatted on
+    the GPU, .map/.fld/.xyz files written).  Whole-process wall time, best of 2
+    (the first run also pages the image in)."""
+    cli = ROOT / "autogrid_b200" / "_build" / "autogrid4_b200"
+    if not cli.exists():
+        return None
+    walls = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        r = subprocess.run([str(cli), "-p", "bench.gpf", "-l", "cli.glg"], cwd=work, capture_output=True, text=True)
+        walls.append(time.perf_counter() - t0)
+        if r.returncode != 0:
+            return {"error": r.stderr[-300:]}
+    ok = "Successful Completion" in (work / "cli.glg").read_text()
+    return {"command": "autogrid4_b200 -p bench.gpf -l cli.glg", "seconds": min(walls), "ok": ok,
+            "evals_per_s": evals / min(walls),
+            "note": "whole process, files written; compare the reference's whole-process wall in cpu_baseline"}
 
 
 def batched_sharded(ctx, n, work: Path, stream, rank: int, world: int):

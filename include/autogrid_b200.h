@@ -120,6 +120,17 @@ typedef struct ag_problem {
     int32_t floating_grid;       /* fmap: distance to the nearest atom            */
     int32_t constriction_grid;   /* cmap: atoms within constriction_cutoff        */
     double  constriction_cutoff;
+    /* 'map_receptor_interior off' (main.cpp:1642-1656), which the reference
+     * supports in its USE_BHTREE build: a grid point with a receptor atom within
+     * 1.5 A (BH_collision_dist, main.cpp:346) is a collision -- LOOP 1 is
+     * skipped there, so its e-map value is 0 and its floating-grid value 1.5
+     * (main.cpp:2907-2940) -- and the constriction grid counts the atoms within
+     * the cutoff with the BH tree's single-precision test (bhtree.cpp:338-366,
+     * main.cpp:2894-2899).  The test: float differences of the float grid point
+     * and float atom coordinates, each within the cutoff, and their float
+     * squared sum not above the float squared cutoff.  0 (default): the receptor
+     * interior is mapped.  Drop-in path only (ag_maps_compute*, plans). */
+    int32_t report_collisions;
 } ag_problem;
 
 enum { AG_PREC_FP32 = 0,   /* production path                                  */
@@ -321,6 +332,9 @@ ag_status ag_emap_compute_noalloc(int32_t device, int32_t n_atoms, const double 
  * size and chunking and the near-field brick shape on this batch and keeps
  * the fastest.  No counterpart
  * in the reference, which computes one box per process.  FP32 path only.
+ * Instances that ask for the floating or constriction grid get them after
+ * their energy maps, as ag_maps_compute lays them out; they depend on the
+ * geometry only and are computed once, at creation.
  */
 typedef struct ag_batch ag_batch;
 typedef struct ag_tuning {
@@ -342,7 +356,8 @@ ag_status    ag_batch_tuning(const ag_batch *batch, ag_tuning *out);
  * ag_context_destroy. */
 ag_status    ag_batch_destroy(ag_batch *batch);
 /* One-shot: create, run, download every instance's maps (maps[i] host or
- * device, [n_maps_i][P_i] each), destroy.  From 8 instances on (without
+ * device, [n_out_i][P_i] each: the energy maps, then fmap/cmap when asked
+ * for), destroy.  From 8 instances on (without
  * autotuning) the instances run as 8 groups, each its own batch: a group's
  * plans are built on the host while the previous group computes, and each
  * group's maps are copied back while later groups compute.  Results are those

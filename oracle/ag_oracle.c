@@ -56,6 +56,36 @@ int32_t ag_oracle_abi_version(void) { return AG_ABI_VERSION; }
  *   flags:    [n_pts] or NULL  (EDGE_* bits, see header)
  * Returns 0, AG_ERR_NO_CLOSEST_H (main.cpp:3011-3014) or AG_ERR_INVALID.
  */
+/*
+ * 'map_receptor_interior off' (the reference's USE_BHTREE build,
+ * main.cpp:2893-2927): the BH tree's single-precision close-atom test
+ * (bhtree.cpp:338-366) -- float differences of the float grid point and the
+ * float atom coordinates, each within the cutoff, and their float squared sum
+ * not above the float squared cutoff.  Built with -ffp-contract=off.
+ */
+static int bh_close(const float x[3], const double *coord, float cut)
+{
+    const float a0 = (float)coord[0], a1 = (float)coord[1], a2 = (float)coord[2];
+    float d0 = x[0] - a0;
+    if (d0 > cut || d0 < -cut) return 0;
+    float d1 = x[1] - a1;
+    if (d1 > cut || d1 < -cut) return 0;
+    float d2 = x[2] - a2;
+    if (d2 > cut || d2 < -cut) return 0;
+    float D = d0 * d0 + d1 * d1 + d2 * d2;
+    float C = cut * cut;
+    return !(D > C);
+}
+
+/* A grid point with an atom within BH_collision_dist = 1.5 A (main.cpp:346). */
+static int bh_collision(const ag_problem *p, const double c[3])
+{
+    const float x[3] = {(float)c[0], (float)c[1], (float)c[2]};  /* fcc, main.cpp:2860 */
+    for (int ia = 0; ia < p->n_atoms; ia++)
+        if (bh_close(x, p->coord + 3 * ia, 1.5f)) return 1;
+    return 0;
+}
+
 int32_t ag_oracle_points(const ag_problem *p, int64_t n_pts, const int64_t *pt_index,
                          double *out, uint8_t *flags)
 {
@@ -101,8 +131,11 @@ int32_t ag_oracle_points(const ag_problem *p, int64_t n_pts, const int64_t *pt_i
         /* main.cpp:2882-2886 */
         for (int m = 0; m < nAM; m++) { hbmin[m] = 999999.; hbmax[m] = -999999.; hbflag[m] = 0; }
 
-        /* LOOP 1: electrostatics over all atoms, main.cpp:2940-2982 */
-        if (p->elec_map >= 0) {
+        /* LOOP 1: electrostatics over all atoms, main.cpp:2940-2982; skipped at
+         * a collision point with map_receptor_interior off (main.cpp:2907-2926) */
+        if (p->elec_map >= 0 && p->report_collisions && bh_collision(p, c)) {
+            E[p->elec_map] = 0.0;
+        } else if (p->elec_map >= 0) {
             double e = 0;
             for (int ia = 0; ia < nA; ia++) {
                 const double *a = p->coord + 3 * ia;
@@ -519,6 +552,15 @@ int32_t ag_oracle_distance_maps(const ag_problem *p, int64_t n_pts, const int64_
             if (r < O_APPROX_ZERO) r = O_APPROX_ZERO;
             r_min = dmin(r, r_min);
             if (r <= p->constriction_cutoff) count++;
+        }
+        if (p->report_collisions) {
+            /* the USE_BHTREE build: the BH tree's count (main.cpp:2894-2899) and,
+             * at a collision point, r_min = BH_collision_dist (main.cpp:2925) */
+            const float x[3] = {(float)c[0], (float)c[1], (float)c[2]};
+            count = 0;
+            for (int ia = 0; ia < p->n_atoms; ia++)
+                if (bh_close(x, p->coord + 3 * ia, (float)p->constriction_cutoff)) count++;
+            if (bh_collision(p, c)) r_min = 1.5;
         }
         int k = 0;
         if (p->floating_grid) out[(size_t)(k++) * n_pts + ip] = r_min;

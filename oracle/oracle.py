@@ -15,6 +15,8 @@ HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "_build" / "liboracle_ag4.so"
 REF_BIN = HERE / "_ref" / "autogrid4"
 REF_FULLPREC_BIN = HERE / "_ref" / "autogrid4_fullprec"
+# the same with the reference's USE_BHTREE switch (accepts 'map_receptor_interior off')
+REF_BHTREE_BIN = HERE / "_ref" / "autogrid4_bhtree_fullprec"
 # The reference source tree: AG_REFERENCE_SRC, or where this build's image
 # mounts it.  Only the oracle build and the tests that read the reference's
 # own test inputs use it; when it is absent those tests skip and the prebuilt

@@ -8,6 +8,14 @@ oracle/_ref/autogrid4 (unmodified, %.3f output).  Stored per case: the GPF and
 PDBQT text, the map names, the full-precision maps (float64 of the printed
 float values), the %.3f maps, and the .fld text.
 
+The collision fixtures (tests/golden/collision/*.npz) come from
+oracle/_ref/autogrid4_bhtree_fullprec, the same sources built with the
+reference's USE_BHTREE switch: the only build in which
+'map_receptor_interior off' (collision points) exists.  Its LOOP 2 uses the
+BH tree's single-precision distances, so only its e map, floating grid and
+constriction grid are pinned exactly; the other maps are stored for the
+parity bar.
+
 Run here, where the reference sources exist:
     python tests/golden/make_golden.py [case ...]
 """
@@ -53,6 +61,19 @@ CASES = {
     "distance_maps": dict(n=300, seed=17, radius=10.0, dist=["f", "c"], spec=dict(
         npts=(10, 8, 12), ligand_types=["C", "OA"],
         extra_lines=["fmap g.f.map", "constriction_distance_cutoff 5.5", "cmap g.c.map"])),
+}
+
+
+COLLISION_CASES = {
+    # map_receptor_interior off: e = 0 and fmap = 1.5 within 1.5 A of an atom,
+    # the BH tree's constriction count (main.cpp:2893-2927)
+    "bhtree_collision": dict(n=300, seed=18, radius=9.0, spec=dict(
+        npts=(10, 12, 8), ligand_types=["A", "C", "HD", "OA"],
+        extra_lines=["map_receptor_interior off", "fmap g.f.map", "constriction_distance_cutoff 5.5",
+                     "cmap g.c.map"])),
+    # the same without distance maps, constant dielectric, a denser receptor
+    "bhtree_collision_constdiel": dict(n=500, seed=19, radius=9.0, spec=dict(
+        npts=(8, 8, 10), dielectric=10.0, ligand_types=["C", "NA"], extra_lines=["map_receptor_interior off"])),
 }
 
 
@@ -102,6 +123,25 @@ def make(name: str, case: dict) -> Path:
     return out
 
 
+def make_collision(name: str, case: dict) -> Path:
+    rec = synth.make_receptor(case["n"], seed=case["seed"], radius=case["radius"], center=(2.125, -1.5, 0.75))
+    spec = synth.GridSpec(**case["spec"])
+    names = map_names(spec)
+    dist = [n for n, line in (("f", "fmap"), ("c", "cmap")) if any(x.startswith(line) for x in spec.extra_lines)]
+    with tempfile.TemporaryDirectory() as td:
+        d = Path(td)
+        gpf = synth.write_case(d, "g", rec, spec)
+        run_reference(orc.REF_BHTREE_BIN, d, "g")
+        full = [orc.read_map(d / f"g.{n}.map") for n in names]
+        dist_full = [orc.read_map(d / f"g.{n}.map") for n in dist]
+        (OUT / "collision").mkdir(exist_ok=True)
+        out = OUT / "collision" / f"{name}.npz"
+        np.savez_compressed(out, gpf=gpf.read_text(), pdbqt=(d / "g.pdbqt").read_text(), names=np.array(names),
+                            maps_full=np.array(full), dist_names=np.array(dist),
+                            dist_full=np.array(dist_full) if dist else np.zeros((0, 0)), npts=np.array(spec.npts))
+    return out
+
+
 def main():
     orc.build(ref=True)
     only = sys.argv[1:]
@@ -110,6 +150,11 @@ def main():
             continue
         p = make(name, case)
         print(f"{p.name}: {p.stat().st_size} bytes")
+    for name, case in COLLISION_CASES.items():
+        if only and name not in only:
+            continue
+        p = make_collision(name, case)
+        print(f"collision/{p.name}: {p.stat().st_size} bytes")
 
 
 if __name__ == "__main__":

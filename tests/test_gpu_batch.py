@@ -84,3 +84,29 @@ def test_batch_one_shot_pipelined(tmp_path, gpu_ctx):
     with pytest.raises(AutoGridError) as e:
         compute_batch(gpu_ctx, probs[:6] + [bad] + probs[7:])
     assert e.value.status == 1 and "instance 6" in e.value.message
+
+
+def test_batch_with_distance_maps(tmp_path, gpu_ctx):
+    """Instances asking for the floating and constriction grids get them after
+    their energy maps, in the batch and in the one-shot batch call, equal to
+    the single-instance path's (same FP64 kernel, computed once)."""
+    from autogrid_b200 import Batch, synth
+    from autogrid_b200.api import compute_batch
+    from conftest import make_case
+    probs = []
+    for k, (n, npts) in enumerate([(300, (10, 12, 8)), (700, (16, 10, 14)), (500, (8, 8, 20))]):
+        extra = ["fmap d%d.f.map" % k, "constriction_distance_cutoff 5.5", "cmap d%d.c.map" % k] if k != 1 else []
+        probs.append(make_case(tmp_path, f"d{k}", n, npts, seed=40 + k, extra_lines=extra)[1])
+    assert probs[0].n_out == probs[0].n_maps + 2 and probs[1].n_out == probs[1].n_maps
+    singles = [gpu_ctx.compute(p) for p in probs]
+    b = Batch(gpu_ctx, probs, autotune=False)
+    b.run()
+    for i, p in enumerate(probs):
+        got = b.download(i)
+        assert tolerance_ok(got[:p.n_maps], singles[i][:p.n_maps]).all()
+        assert np.array_equal(got[p.n_maps:], singles[i][p.n_maps:])
+    b.close()
+    outs = compute_batch(gpu_ctx, probs * 3)  # 9 instances: the grouped one-shot path
+    for i, o in enumerate(outs):
+        p = probs[i % 3]
+        assert np.array_equal(o[p.n_maps:], singles[i % 3][p.n_maps:])

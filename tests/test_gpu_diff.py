@@ -134,3 +134,37 @@ def test_torch_binding_matches_c_abi(tmp_path, gpu_ctx):
     np.testing.assert_allclose(coords.grad.numpy(), gc, rtol=1e-9, atol=1e-9)
     np.testing.assert_allclose(charges.grad.numpy(), gq, rtol=1e-9, atol=1e-9)
     d.close()
+
+
+def test_distance_maps_in_differentiable_mode(tmp_path, gpu_ctx):
+    """fmap/cmap after the energy maps: equal to the drop-in path's (same FP64
+    kernel); the floating grid's gradient (nearest atom's unit vector) matches
+    central differences, the constriction grid contributes none."""
+    from autogrid_b200 import Diff
+    job, prob = make_case(tmp_path, "dm", 300, (10, 12, 8), seed=31, radius=9.0,
+                          extra_lines=["fmap dm.f.map", "constriction_distance_cutoff 5.5", "cmap dm.c.map"])
+    nm = prob.n_maps
+    assert prob.n_out == nm + 2
+    drop = gpu_ctx.compute(prob, "fp64").reshape(prob.n_out, -1)
+    d = Diff(gpu_ctx, prob, "fp64")
+    d.forward()
+    got = d.maps().reshape(prob.n_out, -1)
+    assert np.array_equal(got[nm:], drop[nm:])
+    # gradient of L = sum w * fmap (energy and constriction weights zero)
+    rng = np.random.default_rng(2)
+    w = np.zeros(prob.map_shape)
+    w[nm] = rng.normal(size=prob.map_shape[1:])
+    gc = d.backward(w)["coord"]
+    c0 = prob.arrays["coord"].reshape(-1, 3).copy()
+    near = np.flatnonzero(np.abs(gc).sum(1) > 0)
+    assert near.size > 0
+    h = 1e-6
+    for a in rng.choice(near, min(6, near.size), replace=False):
+        for i in range(3):
+            cp = c0.copy(); cp[a, i] += h
+            cm = c0.copy(); cm[a, i] -= h
+            d.set_atoms(cp); d.forward(keep_closest_h=True); lp = float(np.sum(w * d.maps()))
+            d.set_atoms(cm); d.forward(keep_closest_h=True); lm = float(np.sum(w * d.maps()))
+            fd = (lp - lm) / (2 * h)
+            assert abs(fd - gc[a, i]) <= 1e-5 * max(1.0, abs(gc[a, i])), (a, i, fd, gc[a, i])
+    d.close()

@@ -121,3 +121,35 @@ def test_only_e_and_d_maps(tmp_path, gpu_ctx):
     got = gpu_ctx.compute(p2).reshape(2, -1)
     ref, flags = oracle_points(p2)
     assert (tolerance_ok(got, ref) | (flags[None, :] != 0)).all()
+
+
+COLLISION = sorted((ROOT / "tests" / "golden" / "collision").glob("*.npz"))
+
+
+@pytest.mark.parametrize("path", COLLISION, ids=[p.stem for p in COLLISION])
+def test_collision_mode_matches_bhtree_reference(path, tmp_path, gpu_ctx):
+    """'map_receptor_interior off' on the GPU against the reference's USE_BHTREE
+    build: e map (zero at the collision points), floating and constriction
+    grids as the oracle pins them; every map within the parity bar; the FP64
+    twin's e map to the printed float precision.  Batches and the
+    differentiable mode refuse the mode."""
+    from autogrid_b200 import AutoGridError, Batch, Diff
+    z, job, prob = load_golden(path, tmp_path)
+    names = [str(n) for n in z["names"]]
+    for prec in ("fp32", "fp64"):
+        out = gpu_ctx.compute(prob, prec).reshape(prob.n_out, -1)
+        for k, n in enumerate(names):
+            assert tolerance_ok(out[k].astype(np.float64), z["maps_full"][k]).all(), (prec, n)
+        if "e" in names:
+            e = names.index("e")
+            assert np.array_equal(out[e] == 0, z["maps_full"][e] == 0), prec
+            if prec == "fp64":
+                assert full_precision_ok(out[e][None], z["maps_full"][e][None]).all()
+        if z["dist_full"].size:
+            nm = prob.n_maps
+            assert np.all(np.abs(out[nm] - z["dist_full"][0]) <= 1e-6 * np.abs(z["dist_full"][0]) + 1e-6), prec
+            assert np.array_equal(out[nm + 1], z["dist_full"][1]), prec
+    for make in (lambda: Batch(gpu_ctx, [prob], autotune=False), lambda: Diff(gpu_ctx, prob, "fp32")):
+        with pytest.raises(AutoGridError) as err:
+            make()
+        assert err.value.status == 4

@@ -179,3 +179,67 @@ def test_oracle_vs_live_reference_random(seed, tmp_path, built):
         ref = read_map(ref_dir / f)
         ok = full_precision_ok(got[i], ref)
         assert ok.all(), f"seed {seed} {f}: {int((~ok).sum())} values off, max |d| {np.abs(got[i] - ref).max()}"
+
+
+COLLISION = sorted((ROOT / "tests" / "golden" / "collision").glob("*.npz"))
+
+
+def _collision_check(prob, z):
+    """The oracle against the USE_BHTREE reference: e map, floating and
+    constriction grids exactly (the printed float precision), the LOOP 2 maps
+    within the parity bar (that build's LOOP 2 takes the BH tree's
+    single-precision distances)."""
+    from conftest import tolerance_ok
+    from oracle.oracle import oracle_distance_maps, oracle_points
+    o, _ = oracle_points(prob)
+    ref = z["maps_full"]
+    names = [str(n) for n in z["names"]]
+    for k, n in enumerate(names):
+        if n == "e":
+            assert full_precision_ok(o[k][None], ref[k][None]).all()
+        else:
+            assert tolerance_ok(o[k], ref[k]).all(), n
+    e = names.index("e") if "e" in names else None
+    if e is not None:
+        assert (o[e] == 0.0).sum() == (ref[e] == 0.0).sum() > 0  # the collision points
+    if z["dist_full"].size:
+        dm = oracle_distance_maps(prob)
+        assert np.all(np.abs(dm[0] - z["dist_full"][0]) <= 1.5e-7 * np.abs(z["dist_full"][0]))
+        assert np.array_equal(dm[1], z["dist_full"][1])
+
+
+@pytest.mark.parametrize("path", COLLISION, ids=[p.stem for p in COLLISION])
+def test_oracle_collision_mode_matches_bhtree_reference(path, tmp_path, built):
+    assert len(COLLISION) == 2
+    z, job, prob = load_golden(path, tmp_path)
+    assert prob.scalars["report_collisions"] == 1
+    _collision_check(prob, z)
+
+
+@needs_reference
+@pytest.mark.parametrize("seed", [0, 1])
+def test_oracle_collision_mode_vs_live_bhtree(seed, tmp_path, built):
+    """Random receptors with 'map_receptor_interior off' through the reference's
+    USE_BHTREE build, live."""
+    import subprocess
+    from autogrid_b200 import Job, synth
+    from oracle.oracle import REF_BHTREE_BIN, read_map
+    rng = np.random.default_rng(700 + seed)
+    rec = synth.make_receptor(int(rng.integers(150, 500)), seed=seed + 90, radius=float(rng.uniform(6.0, 10.0)))
+    spec = synth.GridSpec(npts=tuple(int(v) for v in rng.integers(4, 14, 3)), spacing=float(rng.choice([0.3, 0.375, 0.5])),
+                          ligand_types=["C", "OA", "HD"],
+                          extra_lines=["map_receptor_interior off", "fmap g.f.map",
+                                       f"constriction_distance_cutoff {rng.uniform(3.0, 7.9):.2f}", "cmap g.c.map"])
+    synth.write_case(tmp_path, "g", rec, spec)
+    r = subprocess.run([str(REF_BHTREE_BIN), "-p", "g.gpf", "-l", "g.glg"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    names = ["C", "OA", "HD", "e", "d"]
+    z = {"names": np.array(names), "maps_full": np.array([read_map(tmp_path / f"g.{n}.map") for n in names]),
+         "dist_full": np.array([read_map(tmp_path / "g.f.map"), read_map(tmp_path / "g.c.map")])}
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        prob = Job("g.gpf", "mine.glg").problem()
+    finally:
+        os.chdir(cwd)
+    _collision_check(prob, z)
