@@ -68,7 +68,7 @@ class ag_stats(C.Structure):
                 ("gpu_launches", C.c_int32), ("reserved", C.c_int32), ("kernel_ms", C.c_double),
                 ("far_ms", C.c_double), ("text_ms", C.c_double), ("text_bytes", C.c_int64),
                 ("table_ms", C.c_double), ("far_edge_pairs", C.c_int64), ("far_fp32_bin_errors", C.c_int64),
-                ("far_fp64_ties", C.c_int64)]
+                ("far_fp64_ties", C.c_int64), ("fixup_ms", C.c_double), ("near_ms", C.c_double)]
 
 
 class ag_table_params(C.Structure):

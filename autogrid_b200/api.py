@@ -280,6 +280,8 @@ class Stats:
     far_edge_pairs: int = 0
     far_fp32_bin_errors: int = 0
     far_fp64_ties: int = 0
+    fixup_ms: float = 0.0
+    near_ms: float = 0.0
 
 
 class Context:
@@ -343,7 +345,8 @@ class Context:
         st = ag_stats()
         check(self._lib.ag_context_stats(self._h, C.byref(st)))
         return Stats(st.near_pairs, st.fp64_fallbacks, st.far_pairs, st.gpu_launches, st.kernel_ms, st.far_ms,
-                     st.text_ms, st.text_bytes, st.far_edge_pairs, st.far_fp32_bin_errors, st.far_fp64_ties)
+                     st.text_ms, st.text_bytes, st.far_edge_pairs, st.far_fp32_bin_errors, st.far_fp64_ties,
+                     st.fixup_ms, st.near_ms)
 
     def far_bins(self, problem: Problem, points) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         """Far-field table bins of the given grid points (linear indices, X

@@ -207,6 +207,10 @@ struct ag_context {
     std::vector<cudaEvent_t> far_done, red_done;
     cudaEvent_t copy_done = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf0 = nullptr, evf1 = nullptr;
+    // evfx: between the far-field kernel and its fix-up; evn0/evn1: around
+    // the near-field launches (run_plan only)
+    cudaEvent_t evfx = nullptr, evn0 = nullptr, evn1 = nullptr;
+    bool had_near = false, had_fixup_event = false;
     ag_stats stats{};
     BufferSet pool;
     unsigned long long *d_counters = nullptr;
@@ -791,6 +795,10 @@ FarArgs far_args(const ag_plan *pl)
     return a;
 }
 
+// Kernels launched for the far field of one run: the far-field kernel, and
+// the fix-up unless the table is constant (no guard bins then).
+int far_launches(const FarArgs &fa) { return (fa.tab_mode != FAR_TAB_CONST && fa.edge_bits) ? 2 : 1; }
+
 NearPtrs near_ptrs(const ag_plan *pl, unsigned long long *counters)
 {
     NearPtrs q;
@@ -840,7 +848,7 @@ ag_status enqueue_slabs(ag_plan *pl, cudaStream_t s, int nslab, int &launches)
                 ag_status st = launch_far_slab(pl, s, k, nslab);
                 if (st != AG_OK) return st;
             }
-            launches++;
+            launches += far_launches(far_args(pl));
         }
         int sz0, sz1;
         slab_range(d, k, &sz0, &sz1);
@@ -914,10 +922,11 @@ ag_status run_plan_zrange(ag_plan *pl, cudaStream_t s, int z0, int z1)
         AGB_CK(cudaEventRecord(c->evf0, c->side));
         const FarArgs fa = far_args(pl);
         AGB_CK(launch_emap_far(fa, pl->n_chunks, 512, c->side, z0 / FRAME_Z, last ? -1 : z1 / FRAME_Z));
+        AGB_CK(cudaEventRecord(c->evfx, c->side));
         AGB_CK(launch_far_fixup(fa, pl->n_chunks, c->side, z0 / FRAME_Z, last ? -1 : z1 / FRAME_Z));
         AGB_CK(cudaEventRecord(c->evf1, c->side));
         AGB_CK(cudaEventRecord(c->join, c->side));
-        launches++;
+        launches += far_launches(fa);
     }
     if (pl->any_cov) {
         AGB_CK(launch_covalent(d, pl->cov, s));
@@ -952,6 +961,8 @@ ag_status run_plan_zrange(ag_plan *pl, cudaStream_t s, int z0, int z1)
     pl->last_launches = launches;
     c->pending = true;
     c->had_far = far;
+    c->had_fixup_event = far;
+    c->had_near = false;
     c->last_launches = launches;
     c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)(z1 - z0) * d.n1x * d.n1y * d.n_atoms : 0;
     return AG_OK;
@@ -982,10 +993,11 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
         AGB_CK(cudaEventRecord(c->evf0, fs));
         const FarArgs fa = far_args(pl);
         AGB_CK(launch_emap_far(fa, pl->n_chunks, 512, fs));
+        AGB_CK(cudaEventRecord(c->evfx, fs));
         AGB_CK(launch_far_fixup(fa, pl->n_chunks, fs));
         AGB_CK(cudaEventRecord(c->evf1, fs));
         if (!serial) AGB_CK(cudaEventRecord(c->join, fs));
-        launches++;
+        launches += far_launches(fa);
     }
     if (pl->any_cov) {
         AGB_CK(launch_covalent(d, pl->cov, s));
@@ -1003,12 +1015,14 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
         launches++;
     }
     const bool need_near = d.n_atom_maps > 0 || d.dsolv_map >= 0 || (!exact && d.elec_map >= 0);
+    AGB_CK(cudaEventRecord(c->evn0, s));
     if (need_near) {
         for (const NearGroup &g : pl->groups) {
             AGB_CK(launch_near(exact, d, g, near_ptrs(pl, c->d_counters), 0, s));
             launches++;
         }
     }
+    AGB_CK(cudaEventRecord(c->evn1, s));
     if (far) {
         if (!serial) AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
         AGB_CK(launch_emap_reduce(pl->d_reduce, pl->d_reduce_begin, 1, d.P, s));
@@ -1023,6 +1037,8 @@ ag_status run_plan(ag_plan *pl, cudaStream_t s)
     pl->last_launches = launches;
     c->pending = true;
     c->had_far = !exact && d.elec_map >= 0 && pl->n_chunks > 0;
+    c->had_near = true;
+    c->had_fixup_event = c->had_far;
     c->last_launches = launches;
     c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
     return AG_OK;
@@ -1032,9 +1048,11 @@ ag_status settle_stats(ag_context *c)
 {
     if (!c->pending) return AG_OK;
     AGB_CK(cudaEventSynchronize(c->ev1));
-    float ms = 0.f, fms = 0.f;
+    float ms = 0.f, fms = 0.f, xms = 0.f, nms = 0.f;
     AGB_CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     if (c->had_far) AGB_CK(cudaEventElapsedTime(&fms, c->evf0, c->evf1));
+    if (c->had_far && c->had_fixup_event) AGB_CK(cudaEventElapsedTime(&xms, c->evfx, c->evf1));
+    if (c->had_near) AGB_CK(cudaEventElapsedTime(&nms, c->evn0, c->evn1));
     unsigned long long h[kCounters] = {};
     AGB_CK(cudaMemcpy(h, c->d_counters, sizeof h, cudaMemcpyDeviceToHost));
     c->stats.near_pairs = (int64_t)h[0];
@@ -1046,6 +1064,8 @@ ag_status settle_stats(ag_context *c)
     c->stats.gpu_launches = c->last_launches;
     c->stats.kernel_ms = ms;
     c->stats.far_ms = fms;
+    c->stats.fixup_ms = xms;
+    c->stats.near_ms = nms;
     c->pending = false;
     return AG_OK;
 }
@@ -1291,6 +1311,9 @@ ag_status ag_context_create(int32_t device, ag_context **out)
     AGB_CK(cudaEventCreate(&c->ev1));
     AGB_CK(cudaEventCreate(&c->evf0));
     AGB_CK(cudaEventCreate(&c->evf1));
+    AGB_CK(cudaEventCreate(&c->evfx));
+    AGB_CK(cudaEventCreate(&c->evn0));
+    AGB_CK(cudaEventCreate(&c->evn1));
     AGB_CK(cudaMalloc(&c->d_counters, kCounters * sizeof(unsigned long long)));
     AGB_CK(cudaMemset(c->d_counters, 0, kCounters * sizeof(unsigned long long)));
     for (cudaEvent_t &e : c->tev) AGB_CK(cudaEventCreate(&e));
@@ -1321,6 +1344,9 @@ ag_status ag_context_destroy(ag_context *ctx)
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->evf0) cudaEventDestroy(ctx->evf0);
     if (ctx->evf1) cudaEventDestroy(ctx->evf1);
+    if (ctx->evfx) cudaEventDestroy(ctx->evfx);
+    if (ctx->evn0) cudaEventDestroy(ctx->evn0);
+    if (ctx->evn1) cudaEventDestroy(ctx->evn1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     if (ctx->h_text) cudaFreeHost(ctx->h_text);
     for (cudaEvent_t e : ctx->tev)
@@ -1371,6 +1397,8 @@ static ag_status run_plan_pipelined(ag_plan *pl, void *out, size_t n_out)
     pl->last_launches = launches;
     c->pending = true;
     c->had_far = far;
+    c->had_fixup_event = false;
+    c->had_near = false;
     c->last_launches = launches;
     c->last_far_pairs = (d.elec_map >= 0) ? (int64_t)d.P * d.n_atoms : 0;
     for (int k = 0; k < nslab; k++) {

@@ -327,13 +327,18 @@ __device__ __forceinline__ int far_exact_bin_d(double ax128, double ay128, doubl
     return (int)__dmul_rn(r, (double)AG_A_DIV) | FAR_TIE_FLAG;
 }
 
+// Per-lane tallies of the resolved pairs (summed once per unit).
+struct FixCount {
+    unsigned pairs, fp32_errors, ties;
+};
+
 // One (owner thread, atom) item: the owner's pairs with the atom re-evaluated
 // by the far kernel's own FP32 operations (packed, as there), then each
 // flagged pair the owner keeps (t >= FAR_T0, point inside the box, bin below
 // the last) resolved in FP64 and its correction added.
 template <int NJ, bool CLAMP>
 __device__ __forceinline__ void far_fix_item(const FarArgs &a, FixSmem &S, uint32_t item, int a_begin, int ox, int oy,
-                                             int oz, double X0, double Y0, double Z0)
+                                             int oz, double X0, double Y0, double Z0, FixCount &n)
 {
     const int owner = (int)(item & 255u), at = a_begin + (int)(item >> 8);
     const int lane = owner & 31, w = owner >> 5;
@@ -382,9 +387,9 @@ __device__ __forceinline__ void far_fix_item(const FarArgs &a, FixSmem &S, uint3
                                        kb);
         const int kx = kr & ~FAR_TIE_FLAG;
         const int kf = (int)(__float_as_uint(__fadd_rz(t, 8388608.f)) - MAGIC_BITS);  // plain FP32 floor(t)
-        atomicAdd(&S.cnt[0], 1u);
-        if (min(kf, AG_NDIEL - 1) != kx) atomicAdd(&S.cnt[1], 1u);
-        if (kr & FAR_TIE_FLAG) atomicAdd(&S.cnt[2], 1u);
+        n.pairs++;
+        n.fp32_errors += min(kf, AG_NDIEL - 1) != kx ? 1u : 0u;
+        n.ties += (kr & FAR_TIE_FLAG) ? 1u : 0u;
         // the far kernel added T_far[kb]; T_far is zero below FAR_BIN0, so an
         // owned pair whose exact bin is 1023 needs T[1023] even when kx == kb
         const float used = __ldg(a.far_tab + kb);
@@ -423,6 +428,7 @@ __device__ __forceinline__ void far_fix_unit(const FarArgs &a, int f, int chunk,
     const int nwords = (a_end - a_begin + 31) >> 5;
     const uint32_t *bits = a.edge_bits + far_bits_base(a, f, chunk) + tid;
     uint32_t *list = S.items[w];
+    FixCount cnt = {0u, 0u, 0u};
     if (L.warp_in) {  // the far kernel wrote no words for the other warps
         int nlist = 0;  // warp-uniform: pending items in list[0, nlist)
         const unsigned below = (1u << lane) - 1u;
@@ -442,7 +448,7 @@ __device__ __forceinline__ void far_fix_unit(const FarArgs &a, int f, int chunk,
                 nlist += __popc(have);
                 __syncwarp();
                 if (nlist >= 32) {
-                    far_fix_item<NJ, CLAMP>(a, S, list[lane], a_begin, ox, oy, oz, X0, Y0, Z0);
+                    far_fix_item<NJ, CLAMP>(a, S, list[lane], a_begin, ox, oy, oz, X0, Y0, Z0, cnt);
                     nlist -= 32;
                     const uint32_t rest = lane < nlist ? list[32 + lane] : 0u;
                     __syncwarp();
@@ -451,7 +457,7 @@ __device__ __forceinline__ void far_fix_unit(const FarArgs &a, int f, int chunk,
                 }
             }
         }
-        if (lane < nlist) far_fix_item<NJ, CLAMP>(a, S, list[lane], a_begin, ox, oy, oz, X0, Y0, Z0);
+        if (lane < nlist) far_fix_item<NJ, CLAMP>(a, S, list[lane], a_begin, ox, oy, oz, X0, Y0, Z0, cnt);
     }
     __syncwarp();
     // each thread adds its own points' corrections to the unit's partial sums
@@ -466,6 +472,14 @@ __device__ __forceinline__ void far_fix_unit(const FarArgs &a, int f, int chunk,
                 const int ix = ox + L.tx + 8 * j + 4 * c;
                 if (v != 0 && ix < a.n1x) out[ix] = __fadd_rn(out[ix], (float)((double)v / FX_SCALE));
             }
+    }
+    const unsigned c0 = __reduce_add_sync(0xffffffffu, cnt.pairs);
+    const unsigned c1 = __reduce_add_sync(0xffffffffu, cnt.fp32_errors);
+    const unsigned c2 = __reduce_add_sync(0xffffffffu, cnt.ties);
+    if (lane == 0 && (c0 | c1 | c2)) {
+        atomicAdd(&S.cnt[0], c0);
+        atomicAdd(&S.cnt[1], c1);
+        atomicAdd(&S.cnt[2], c2);
     }
     __syncthreads();
     if (tid < 3 && a.edge_counters && S.cnt[tid]) atomicAdd(a.edge_counters + tid, (unsigned long long)S.cnt[tid]);

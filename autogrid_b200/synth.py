@@ -177,6 +177,10 @@ WORKLOADS = {
     # 10,000 atoms in a 45 A sphere, npts 126^3 (127^3 points), 14 types + e + d = 16 maps
     "ad4_10000_127cube_16maps": dict(n_atoms=10000, radius=45.0,
                                      spec=GridSpec(npts=(126, 126, 126), ligand_types=list(LIGAND_TYPES_14))),
+    # the same receptor and maps on 49 of the 127 planes (a profiling case:
+    # ~0.2 GB on the device, above the L2's 126 MB, one launch per kernel)
+    "ad4_10000_127x127x49_16maps": dict(n_atoms=10000, radius=45.0,
+                                        spec=GridSpec(npts=(126, 126, 48), ligand_types=list(LIGAND_TYPES_14))),
 }
 
 

@@ -178,6 +178,12 @@ typedef struct ag_stats {
                                   the reference expression's (nested hypot) in
                                   CUDA's libm, which may differ from the host
                                   libm's by one ulp of r                        */
+    double  fixup_ms;          /* device time of the far-field fix-up kernel
+                                  (part of far_ms; plans only)                  */
+    double  near_ms;           /* device time from the first to the last
+                                  near-field launch (ag_plan_run; with
+                                  ag_opts.serial the near kernels' own time,
+                                  otherwise overlapped with the far field)      */
 } ag_stats;
 
 typedef struct ag_context ag_context;
