@@ -93,6 +93,8 @@ SIGNATURES = {
     "ag_context_create": (C.c_int, [C.c_int32, C.POINTER(C.c_void_p)]),
     "ag_context_destroy": (C.c_int, [C.c_void_p]),
     "ag_context_stats": (C.c_int, [C.c_void_p, C.POINTER(ag_stats)]),
+    "ag_context_cached_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
+    "ag_context_trim": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "ag_maps_compute": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_void_p]),
     "ag_maps_compute_f64": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.c_void_p]),
     "ag_plan_create": (C.c_int, [C.c_void_p, C.POINTER(ag_problem), C.POINTER(ag_opts), C.POINTER(C.c_void_p)]),

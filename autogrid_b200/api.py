@@ -348,6 +348,18 @@ class Context:
                      st.text_ms, st.text_bytes, st.far_edge_pairs, st.far_fp32_bin_errors, st.far_fp64_ties,
                      st.fixup_ms, st.near_ms)
 
+    def cached_bytes(self) -> int:
+        """Device memory the context keeps for later batches (ag_context_cached_bytes)."""
+        v = C.c_int64()
+        check(self._lib.ag_context_cached_bytes(self._h, C.byref(v)))
+        return int(v.value)
+
+    def trim(self) -> int:
+        """Free the context's cached batch memory; returns the bytes freed (ag_context_trim)."""
+        v = C.c_int64()
+        check(self._lib.ag_context_trim(self._h, C.byref(v)))
+        return int(v.value)
+
     def far_bins(self, problem: Problem, points) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
         """Far-field table bins of the given grid points (linear indices, X
         fastest) against every atom, with the far kernel's arithmetic

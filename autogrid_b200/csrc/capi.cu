@@ -66,6 +66,25 @@ struct BlockCache {
         std::lock_guard<std::mutex> lock(mu);
         free.emplace_back(p, bytes);
     }
+    size_t bytes()
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        size_t n = 0;
+        for (auto &b : free) n += b.second;
+        return n;
+    }
+    // Frees every cached block; returns the bytes freed.
+    size_t release()
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        size_t n = 0;
+        for (auto &b : free) {
+            cudaFree(b.first);
+            n += b.second;
+        }
+        free.clear();
+        return n;
+    }
 };
 
 // Bump allocator over a few large device blocks, released together: the
@@ -1322,6 +1341,24 @@ ag_status ag_context_create(int32_t device, ag_context **out)
     AGB_CK(prepare_far_kernels());
     AGB_CK(cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device));
     *out = c.release();
+    return AG_OK;
+}
+
+ag_status ag_context_cached_bytes(ag_context *ctx, int64_t *bytes)
+{
+    if (!ctx || !bytes) return invalid("null argument");
+    *bytes = (int64_t)ctx->blocks.bytes();
+    return AG_OK;
+}
+
+ag_status ag_context_trim(ag_context *ctx, int64_t *released)
+{
+    if (!ctx) return invalid("null context");
+    DeviceGuard dg(ctx->device);
+    // blocks in the cache belong to no live batch; work still queued on the
+    // context's streams may use blocks of live batches only
+    const size_t n = ctx->blocks.release();
+    if (released) *released = (int64_t)n;
     return AG_OK;
 }
 

@@ -27,6 +27,9 @@ struct NearSmem {
     unsigned short wl[NB_WARPS_MAX][NB_CHUNK_MAX];
     float wbox[NB_WARPS_MAX][6];  // per warp: its points' box in frame bins (lo xyz, hi xyz)
     float etab[NT_SMALL], sol[NT_SMALL];
+    // per thread: the running H-bond min/max of the MM maps (FP32 kernels;
+    // in shared memory, out of the pair loop's 80-register budget)
+    float hmin[NG_MM][NB_THREADS_MAX], hmax[NG_MM][NB_THREADS_MAX];
     int seg_start[NB_SEGS_MAX], seg_off[NB_SEGS_MAX + 1];
     int total;
     unsigned long long cnt[2];

@@ -454,11 +454,14 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     if (!EXACT && ch >= 0) rvh = make_float3(ptr.atomA[ch].x, ptr.atomA[ch].y, ptr.atomA[ch].z);
 
     // ---- B: pair terms
-    R E[NG_MAX], hmin[NG_MM], hmax[NG_MM];
+    R E[NG_MAX], hmin[NG_MM], hmax[NG_MM];  // hmin/hmax: the FP64 twin only; FP32 keeps them in S
 #pragma unroll
     for (int m = 0; m < NG_MAX; m++) E[m] = 0;
 #pragma unroll
-    for (int m = 0; m < NG_MM; m++) { hmin[m] = 999999.; hmax[m] = -999999.; }
+    for (int m = 0; m < NG_MM; m++) {
+        if (EXACT) { hmin[m] = 999999.; hmax[m] = -999999.; }
+        else { S.hmin[m][tid] = 999999.f; S.hmax[m][tid] = -999999.f; }
+    }
     uint32_t hflag = 0;
     R D1 = 0, D2 = 0, e_near = 0;
     unsigned n_near = 0, n_fb = 0;
@@ -536,7 +539,11 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                     e_pair = t < FAR_T0;  // the far-field kernel skips exactly these pairs
                     PairQ<float> qf;
                     if (!dist_fast(meta, t, rs, qf)) {
-                        dist_exact_f(p, ia, cx(), cy(), cz(), qf);
+                        // through a copy: qf itself must not have its address
+                        // taken, or it lives in local memory on the common path too
+                        PairQ<float> qx = qf;
+                        dist_exact_f(p, ia, cx(), cy(), cz(), qx);
+                        qf = qx;
                         n_fb++;
                     }
                     qf.racc = 1.f; qf.rdon = 1.f; qf.Hramp = 1.f;
@@ -608,8 +615,14 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                         } else if (m < NG_MM) {  // min/max maps are placed first by the host
                             const R f = (act == ACT_MMA) ? q.racc : q.rdon;
                             const R v = T * (f + ((R)1 - f) * rsph);
-                            hmin[m] = hmin[m] < v ? hmin[m] : v;
-                            hmax[m] = hmax[m] > v ? hmax[m] : v;
+                            if (EXACT) {
+                                hmin[m] = hmin[m] < v ? hmin[m] : v;
+                                hmax[m] = hmax[m] > v ? hmax[m] : v;
+                            } else {
+                                const float a0 = S.hmin[m][tid], a1 = S.hmax[m][tid];
+                                S.hmin[m][tid] = a0 < (float)v ? a0 : (float)v;
+                                S.hmax[m][tid] = a1 > (float)v ? a1 : (float)v;
+                            }
                             hflag |= 1u << m;
                         }
                     }
@@ -624,7 +637,10 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
         for (int m = 0; m < NG_MAX; m++) {
             if (m >= g.ng) break;
             R v = E[m];
-            if (m < NG_MM && (hflag & (1u << m))) v += hmin[m] + (hmax[m] > (R)0 ? hmax[m] : (R)0);
+            if (m < NG_MM && (hflag & (1u << m))) {
+                const R lo = EXACT ? hmin[m] : (R)S.hmin[m][tid], hi = EXACT ? hmax[m] : (R)S.hmax[m][tid];
+                v += lo + (hi > (R)0 ? hi : (R)0);
+            }
             v += (R)g.sp[m] * D1 + (R)g.vp[m] * D2;
             const size_t o = (size_t)g.out_map[m] * (size_t)p.P + (size_t)lin;
             if (g.cov[m]) {

@@ -9,6 +9,7 @@ constexpr int NG_MM = 4;                   // of which at most this many keep hb
 constexpr int NT_SMALL = 1040;             // table bins a near pair can reach (r <= 8 A + guard)
 constexpr int NB_CHUNK_MAX = 384;          // near candidates staged in shared memory at once
 constexpr int NB_WARPS_MAX = 8;            // warps of a near-kernel CTA (256 threads)
+constexpr int NB_THREADS_MAX = NB_WARPS_MAX * 32;
 constexpr int NB_SEGS_MAX = 64;            // cell-row segments laid out at once
 constexpr double AGB_NEAR_RADIUS = 8.05;   // A; > 8 A cutoff + FP32 distance error
 constexpr double AGB_CELL = 4.0;           // A; cell-list edge

@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--no-diff", action="store_true", help="skip the differentiable-mode measurement")
     ap.add_argument("--no-vina", action="store_true", help="skip the batched Vina conformer measurement")
     ap.add_argument("--no-text", action="store_true", help="skip the device map-text measurement")
+    ap.add_argument("--vina-conformers", type=int, default=32,
+                    help="conformers of the batched Vina measurement (fewer for a profiling case)")
     return ap.parse_args()
 
 
@@ -328,7 +330,7 @@ def main():
         if not args.no_diff and world == 1:
             line["differentiable"] = differentiable_maps(ctx, work, stream)
         if not args.no_vina and world == 1:
-            line["vina_conformers"] = vina_conformers(ctx, work, stream)
+            line["vina_conformers"] = vina_conformers(ctx, work, stream, K=args.vina_conformers)
         if world == 1:
             line["cli_e2e"] = cli_e2e(work, P * M)
         if not args.no_cpu_baseline and world == 1:
@@ -478,6 +480,7 @@ def batched_ensemble(ctx, n, work: Path, stream):
         compute_batch(ctx, probs, outs)
         e2e_batch.append(time.perf_counter() - t0)
     e2e_plain_s, e2e_batch_s = min(e2e_plain), min(e2e_batch)
+    cached = ctx.cached_bytes()  # device blocks the context keeps for later batch calls
     # roofline of the persistent kernels, timed alone by the autotuner: far
     # field (with its fix-up) against the measured rsqrt rate, near field as
     # algorithmic FP32 flops (as for the single map set) against the FP32 peak
@@ -500,7 +503,7 @@ def batched_ensemble(ctx, n, work: Path, stream):
             "evals_per_s": evals / (batch_ms * 1e-3), "ms_per_ensemble": batch_ms,
             "plain_per_box_ms": plain_ms, "plain_per_box_evals_per_s": evals / (plain_ms * 1e-3),
             "speedup_vs_plain_per_box": plain_ms / batch_ms, "max_diff_over_tolerance": worst,
-            "create_s": create_s, "tuning": tune}
+            "create_s": create_s, "tuning": tune, "context_cached_bytes_after": cached}
 
 
 def cli_e2e(work: Path, evals: int):

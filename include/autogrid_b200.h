@@ -194,6 +194,13 @@ int32_t     ag_abi_version(void);
 ag_status   ag_context_create(int32_t device, ag_context **out);
 ag_status   ag_context_destroy(ag_context *ctx);
 ag_status   ag_context_stats(const ag_context *ctx, ag_stats *out);
+/* Device memory the context keeps for reuse: the 256 MiB blocks of destroyed
+ * batches (ag_batch_destroy, and the groups of ag_maps_compute_batch), which
+ * later batches take again instead of allocating.  The cache holds at most
+ * what the largest batch call had in use at once; ag_context_trim frees it
+ * (released may be null) and ag_context_destroy frees it too. */
+ag_status   ag_context_cached_bytes(ag_context *ctx, int64_t *bytes);
+ag_status   ag_context_trim(ag_context *ctx, int64_t *released);
 
 /*
  * Hot path (replaces main.cpp:2805-3464).

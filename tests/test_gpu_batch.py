@@ -84,6 +84,14 @@ def test_batch_one_shot_pipelined(tmp_path, gpu_ctx):
     with pytest.raises(AutoGridError) as e:
         compute_batch(gpu_ctx, probs[:6] + [bad] + probs[7:])
     assert e.value.status == 1 and "instance 6" in e.value.message
+    # the groups' device blocks stay with the context until trimmed, and a
+    # later call after the trim allocates afresh
+    kept = gpu_ctx.cached_bytes()
+    assert kept > 0
+    assert gpu_ctx.trim() == kept and gpu_ctx.cached_bytes() == 0
+    again = compute_batch(gpu_ctx, probs)
+    for i in range(len(probs)):
+        np.testing.assert_array_equal(again[i], outs[i])
 
 
 def test_batch_with_distance_maps(tmp_path, gpu_ctx):
