@@ -32,7 +32,6 @@ struct NearSmem {
     float hmin[NG_MM][NB_THREADS_MAX], hmax[NG_MM][NB_THREADS_MAX];
     int seg_start[NB_SEGS_MAX], seg_off[NB_SEGS_MAX + 1];
     int total;
-    unsigned long long cnt[2];
 };
 
 struct NearInst {

@@ -294,7 +294,6 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     static_assert(FRAME_X % BX == 0 && FRAME_Y % BY == 0 && FRAME_Z % BZ == 0, "bricks tile far frames");
     using R = typename std::conditional<EXACT, double, float>::type;
     const int tid = threadIdx.x;
-    if (tid < 2) S.cnt[tid] = 0ull;
     for (int i = tid; i < NT_SMALL; i += NB_THREADS) {
         S.etab[i] = ptr.etab[i];
         S.sol[i] = ptr.solf[i];
@@ -659,13 +658,11 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                 ptr.out32[(size_t)p.elec_map * (size_t)p.P + (size_t)lin] = (float)e_near;
         }
     }
-    if (ptr.counters) {
-        atomicAdd(&S.cnt[0], (unsigned long long)n_near);
-        atomicAdd(&S.cnt[1], (unsigned long long)n_fb);
-        __syncthreads();
-        if (tid == 0) {
-            atomicAdd(ptr.counters + 0, S.cnt[0]);
-            atomicAdd(ptr.counters + 1, S.cnt[1]);
+    if (ptr.counters) {  // one atomic per counter and warp
+        const unsigned c0 = __reduce_add_sync(0xffffffffu, n_near), c1 = __reduce_add_sync(0xffffffffu, n_fb);
+        if ((tid & 31) == 0) {
+            if (c0) atomicAdd(ptr.counters + 0, (unsigned long long)c0);
+            if (c1) atomicAdd(ptr.counters + 1, (unsigned long long)c1);
         }
     }
 }

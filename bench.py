@@ -165,9 +165,36 @@ def reference_sample(rec, spec, workdir: Path, threads: int, nxy: int = 48):
         return None
     P = (sub.npts[0] + 1) * (sub.npts[1] + 1) * (nz + 1)
     M = len(spec.ligand_types) + 2
-    desc = (f"reference autogrid4 (OpenMP, {threads} threads) on the same receptor and {M} maps, "
-            f"npts {sub.npts[0]}x{sub.npts[1]}x{nz} ({P} points); whole-process wall time")
+    glg = glg_times((d / "ref.glg").read_text())
+    desc = (f"reference autogrid4 (OpenMP, {threads} threads, {cpu_model()}) on the same receptor and {M} maps, "
+            f"npts {sub.npts[0]}x{sub.npts[1]}x{nz} ({P} points); whole-process wall time {dt:.2f} s, "
+            f"GLG Real= total {glg['real_total_s']} s, sum of per-plane Real= {glg['plane_sum_s']} s "
+            f"({glg['planes']} planes)")
     return P * M / dt, dt, P, M, desc
+
+
+def glg_times(text: str) -> dict:
+    """The reference log's timings: the per-plane 'Real= x.xx,' lines of its
+    grid loop (timesys, main.cpp:3455) and the job's closing 'Real= [h] [m] s'
+    (timesyshms, main.cpp:3568)."""
+    planes, total = [], None
+    for m in re.finditer(r"Real=\s*((?:(\d+)h\s*)?(?:(\d+)m\s*)?([0-9.]+)(s?)),", text):
+        h, mi, sec, unit = m.group(2), m.group(3), float(m.group(4)), m.group(5)
+        if unit == "s":
+            total = (int(h or 0) * 3600 + int(mi or 0) * 60) + sec
+        else:
+            planes.append(sec)
+    return {"real_total_s": total, "plane_sum_s": round(sum(planes), 3), "planes": len(planes)}
+
+
+def cpu_model() -> str:
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "cpu model unknown"
 
 
 def main():
