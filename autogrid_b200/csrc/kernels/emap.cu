@@ -102,7 +102,10 @@ __device__ __forceinline__ size_t far_bits_base(const FarArgs &a, int f, int chu
 
 // One work unit: frame `f` of one instance against atom chunk `chunk`.
 // The caller has loaded the instance's table into s_tab4 and synchronised.
-// Atom tile entries: frame-relative X, Y, Z in bins and w = q*coeff_estat*A_DIV.
+// Atom tile entries: frame-relative (Y, Z, X) in bins and w = q*coeff_estat*A_DIV,
+// in that order so that (Y, Z) arrive in an aligned register pair, the operand
+// of the packed y/z difference: with (X, Y, Z, w) the pair needed moves, and
+// the kernel took 8.20 against 7.89 ms for 127^3 points x 10,000 atoms.
 // The first NJ pairs of each thread hold the frame's x columns inside the box
 // (the rest is padding and is skipped), and a warp whose 4 rows or 2 planes
 // all lie past the box skips the pairs.
@@ -154,9 +157,9 @@ __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, c
             float4 v;
             if (i < na) {
                 const int at = a0 + i;
-                v.x = frame_atom_coord(__ldg(a.ax128 + at), X0);
-                v.y = frame_atom_coord(__ldg(a.ay128 + at), Y0);
-                v.z = frame_atom_coord(__ldg(a.az128 + at), Z0);
+                v.z = frame_atom_coord(__ldg(a.ax128 + at), X0);
+                v.x = frame_atom_coord(__ldg(a.ay128 + at), Y0);
+                v.y = frame_atom_coord(__ldg(a.az128 + at), Z0);
                 v.w = __ldg(a.qw + at);
             } else {
                 v = make_float4(0.f, 0.f, 0.f, 0.f);  // never read: the pair loops stop at na
@@ -173,10 +176,10 @@ __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, c
 #pragma unroll 2
             for (int i = 0; i < na; i++) {
                 const float4 A = s_atom[i];
-                const float2 dyz = __fadd2_rn(make_float2(A.y, A.z), npyz);
+                const float2 dyz = __fadd2_rn(make_float2(A.x, A.y), npyz);
                 const float s = __fmaf_rn(dyz.x, dyz.x, __fmaf_rn(dyz.y, dyz.y, TINY_T2));
                 const float2 s2 = make_float2(s, s);
-                const float2 ax2 = make_float2(A.x, A.x);
+                const float2 ax2 = make_float2(A.z, A.z);
                 const float2 q2 = make_float2(A.w, A.w);
 #pragma unroll
                 for (int j = 0; j < NJ; j++) {
@@ -198,10 +201,10 @@ __device__ __forceinline__ void far_unit_n(const FarArgs &a, int f, int chunk, c
 #pragma unroll 2
                 for (int ii = 0; ii < nb; ii++) {
                     const float4 A = s_atom[ib + ii];
-                    const float2 dyz = __fadd2_rn(make_float2(A.y, A.z), npyz);
+                    const float2 dyz = __fadd2_rn(make_float2(A.x, A.y), npyz);
                     const float s = __fmaf_rn(dyz.x, dyz.x, __fmaf_rn(dyz.y, dyz.y, TINY_T2));
                     const float2 s2 = make_float2(s, s);
-                    const float2 ax2 = make_float2(A.x, A.x);
+                    const float2 ax2 = make_float2(A.z, A.z);
                     const float2 q2 = make_float2(A.w, A.w);
                     uint32_t edge = 0;
 #pragma unroll
