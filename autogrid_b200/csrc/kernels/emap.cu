@@ -355,7 +355,9 @@ __device__ __forceinline__ void far_fix_item(const FarArgs &a, FixSmem &S, uint3
     const float2 tmax = make_float2(FAR_CLAMP_T, FAR_CLAMP_T);
     const float2 lom = make_float2(a.edge_lo, a.edge_lo), him = make_float2(a.edge_hi, a.edge_hi);
     const float2 fT0 = make_float2(FAR_T0, FAR_T0);
-    // the owner's flagged pairs with this atom (slot 2j + c: x = tx + 8j + 4c)
+    // the owner's flagged pairs with this atom (slot 2j + c: x = tx + 8j + 4c):
+    // the guard bins alone; the rare flagged pairs the owner does not keep
+    // are dropped below, one at a time
     uint32_t mask = 0;
 #pragma unroll
     for (int j = 0; j < NJ; j++) {
@@ -365,13 +367,8 @@ __device__ __forceinline__ void far_fix_item(const FarArgs &a, FixSmem &S, uint3
         if (CLAMP) t = make_float2(fminf(t.x, tmax.x), fminf(t.y, tmax.y));
         float2 lo, hi;
         far_guard_bins(t, lom, him, lo, hi);
-        const int ix = ox + tx + 8 * j;
-        const bool k0 = __float_as_uint(lo.x) != __float_as_uint(hi.x) && t.x >= fT0.x && ix < a.n1x &&
-                        __float_as_uint(lo.x) < MAGIC_BITS + AG_NDIEL - 1;
-        const bool k1 = __float_as_uint(lo.y) != __float_as_uint(hi.y) && t.y >= fT0.y && ix + 4 < a.n1x &&
-                        __float_as_uint(lo.y) < MAGIC_BITS + AG_NDIEL - 1;  // at the last bin the reference clamps too
-        mask |= (k0 ? 1u : 0u) << (2 * j);
-        mask |= (k1 ? 2u : 0u) << (2 * j);
+        mask |= min(__float_as_uint(lo.x) ^ __float_as_uint(hi.x), 1u) << (2 * j);
+        mask |= min(__float_as_uint(lo.y) ^ __float_as_uint(hi.y), 1u) << (2 * j + 1);
     }
     while (mask) {
         const int sl = __ffs(mask) - 1;
@@ -386,6 +383,10 @@ __device__ __forceinline__ void far_fix_item(const FarArgs &a, FixSmem &S, uint3
         const uint32_t bl = __float_as_uint(__fmaf_rz(t, a.edge_lo, 8388608.f));
         const int kb = (int)(bl - MAGIC_BITS);
         const int ix = ox + tx + 8 * (sl >> 1) + 4 * (sl & 1);
+        // the owner keeps pairs at t >= FAR_T0 (nearer ones are the near
+        // kernel's), at points inside the box, below the last bin (there the
+        // reference clamps too)
+        if (!(t >= fT0.x) || ix >= a.n1x || kb >= AG_NDIEL - 1) continue;
         const int kr = far_exact_bin_d(ax128, ay128, az128, a.spacing_adiv, ix - a.nex, oy + ty - a.ney, oz + tz - a.nez,
                                        kb);
         const int kx = kr & ~FAR_TIE_FLAG;
