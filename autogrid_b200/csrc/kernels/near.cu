@@ -285,6 +285,48 @@ __device__ __forceinline__ double h_dist(const DevProblem &p, int a, double cx, 
 //         reference's order (strict '<' in file order == lowest index on a tie);
 //         points with no DS/D1 atom within 8 A scan all of them (rare)
 //  B      pair terms of every candidate inside 8 A (+ e-map near pairs)
+// Per-point map accumulators.  The FP32 kernels keep them as pairs, so that
+// a 16-byte table row (4 maps) adds as two packed adds; every add is the same
+// IEEE addition as a scalar one, so the sums are unchanged.  Indices are
+// compile-time constants wherever the kernels use them (unrolled loops), so
+// the accumulators stay in registers.
+template <class R>
+struct MapAcc {
+    R v[NG_MAX];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int m = 0; m < NG_MAX; m++) v[m] = (R)0;
+    }
+    __device__ __forceinline__ R get(int m) const { return v[m]; }
+    __device__ __forceinline__ void add(int m, R x) { v[m] += x; }
+    __device__ __forceinline__ void add4(int m4, float4 T)
+    {
+        v[4 * m4] += (R)T.x; v[4 * m4 + 1] += (R)T.y;
+        v[4 * m4 + 2] += (R)T.z; v[4 * m4 + 3] += (R)T.w;
+    }
+};
+template <>
+struct MapAcc<float> {
+    float2 v[NG_MAX / 2];
+    __device__ __forceinline__ void zero()
+    {
+#pragma unroll
+        for (int k = 0; k < NG_MAX / 2; k++) v[k] = make_float2(0.f, 0.f);
+    }
+    __device__ __forceinline__ float get(int m) const { return (m & 1) ? v[m >> 1].y : v[m >> 1].x; }
+    __device__ __forceinline__ void add(int m, float x)
+    {
+        if (m & 1) v[m >> 1].y += x;
+        else v[m >> 1].x += x;
+    }
+    __device__ __forceinline__ void add4(int m4, float4 T)
+    {
+        v[2 * m4] = __fadd2_rn(v[2 * m4], make_float2(T.x, T.y));
+        v[2 * m4 + 1] = __fadd2_rn(v[2 * m4 + 1], make_float2(T.z, T.w));
+    }
+};
+
 // One brick `b` of one instance (p, g).
 template <bool EXACT, int BX, int BY, int BZ>
 __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int b,
@@ -453,9 +495,9 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     if (!EXACT && ch >= 0) rvh = make_float3(ptr.atomA[ch].x, ptr.atomA[ch].y, ptr.atomA[ch].z);
 
     // ---- B: pair terms
-    R E[NG_MAX], hmin[NG_MM], hmax[NG_MM];  // hmin/hmax: the FP64 twin only; FP32 keeps them in S
-#pragma unroll
-    for (int m = 0; m < NG_MAX; m++) E[m] = 0;
+    MapAcc<R> E;
+    R hmin[NG_MM], hmax[NG_MM];  // the FP64 twin only; FP32 keeps them in S
+    E.zero();
 #pragma unroll
     for (int m = 0; m < NG_MM; m++) {
         if (EXACT) { hmin[m] = 999999.; hmax[m] = -999999.; }
@@ -582,8 +624,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                     for (int m4 = 0; m4 < NG_MAX / 4; m4++) {
                         if (4 * m4 >= g.ng) break;
                         const float4 T4 = __ldg(Trow + m4);
-                        E[4 * m4] += (R)T4.x; E[4 * m4 + 1] += (R)T4.y;
-                        E[4 * m4 + 2] += (R)T4.z; E[4 * m4 + 3] += (R)T4.w;
+                        E.add4(m4, T4);
                     }
                     continue;
                 }
@@ -602,15 +643,15 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                         const int act = (int)((aw >> (3 * m)) & 7ull);
                         if (act == ACT_SKIP) continue;
                         const R T = (R)Tv[u];
-                        if (act == ACT_PLAIN) { E[m] += T; continue; }
+                        if (act == ACT_PLAIN) { E.add(m, T); continue; }
                         R rsph = T / (R)100.;
                         rsph = rsph > (R)0 ? rsph : (R)0;
                         rsph = rsph < (R)1 ? rsph : (R)1;
                         if (act == ACT_SUMA) {
                             const R Tv2 = dis ? (R)Hv[u] : T;
-                            E[m] += Tv2 * q.Hramp * (q.racc + ((R)1 - q.racc) * rsph);
+                            E.add(m, Tv2 * q.Hramp * (q.racc + ((R)1 - q.racc) * rsph));
                         } else if (act == ACT_MMD && dis) {
-                            E[m] += (R)Hv[u] * q.Hramp * (q.rdon + ((R)1 - q.rdon) * rsph);
+                            E.add(m, (R)Hv[u] * q.Hramp * (q.rdon + ((R)1 - q.rdon) * rsph));
                         } else if (m < NG_MM) {  // min/max maps are placed first by the host
                             const R f = (act == ACT_MMA) ? q.racc : q.rdon;
                             const R v = T * (f + ((R)1 - f) * rsph);
@@ -635,7 +676,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
 #pragma unroll
         for (int m = 0; m < NG_MAX; m++) {
             if (m >= g.ng) break;
-            R v = E[m];
+            R v = E.get(m);
             if (m < NG_MM && (hflag & (1u << m))) {
                 const R lo = EXACT ? hmin[m] : (R)S.hmin[m][tid], hi = EXACT ? hmax[m] : (R)S.hmax[m][tid];
                 v += lo + (hi > (R)0 ? hi : (R)0);
