@@ -311,17 +311,20 @@ struct FixSmem {
     float2 npyz[EF_THREADS];
     unsigned long long corr[2 * EF_PAIRS][EF_THREADS];  // fixed-point corrections per point
     uint32_t items[EF_THREADS / 32][FX_LIST];  // (atom offset in the unit << 8) | owner thread
+    // the frame's point coordinates in FP64 bins, (i - ne) * spacing * A_DIV:
+    // x columns [0, FRAME_X), then y rows, then z planes
+    double pc[FRAME_X + FRAME_Y + FRAME_Z];
     unsigned cnt[3];
 };
 
-// Exact bin of one flagged pair from FP64 coordinates already loaded (the
-// atom's x*A_DIV); see far_exact_bin.
-__device__ __forceinline__ int far_exact_bin_d(double ax128, double ay128, double az128, double spacing_adiv, int ix,
-                                               int iy, int iz, int kb)
+// Exact bin of one flagged pair from FP64 coordinates already formed (the
+// atom's x*A_DIV and the point's (i - ne) * spacing * A_DIV); see far_exact_bin.
+__device__ __forceinline__ int far_exact_bin_d(double ax128, double ay128, double az128, double px, double py,
+                                               double pz, int kb)
 {
-    const double dx = __dsub_rn(ax128, __dmul_rn((double)ix, spacing_adiv));
-    const double dy = __dsub_rn(ay128, __dmul_rn((double)iy, spacing_adiv));
-    const double dz = __dsub_rn(az128, __dmul_rn((double)iz, spacing_adiv));
+    const double dx = __dsub_rn(ax128, px);
+    const double dy = __dsub_rn(ay128, py);
+    const double dz = __dsub_rn(az128, pz);
     const double t2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
     const double e = (double)(kb + 1), e2 = __dmul_rn(e, e);  // exact: kb < 2^23
     if (fabs(__dsub_rn(t2, e2)) > 1.0e-12 * e2) return t2 >= e2 ? kb + 1 : kb;
@@ -387,7 +390,7 @@ __device__ __forceinline__ void far_fix_item(const FarArgs &a, FixSmem &S, uint3
         // kernel's), at points inside the box, below the last bin (there the
         // reference clamps too)
         if (!(t >= fT0.x) || ix >= a.n1x || kb >= AG_NDIEL - 1) continue;
-        const int kr = far_exact_bin_d(ax128, ay128, az128, a.spacing_adiv, ix - a.nex, oy + ty - a.ney, oz + tz - a.nez,
+        const int kr = far_exact_bin_d(ax128, ay128, az128, S.pc[ix - ox], S.pc[FRAME_X + ty], S.pc[FRAME_X + FRAME_Y + tz],
                                        kb);
         const int kx = kr & ~FAR_TIE_FLAG;
         const int kf = (int)(__float_as_uint(__fadd_rz(t, 8388608.f)) - MAGIC_BITS);  // plain FP32 floor(t)
@@ -425,6 +428,11 @@ __device__ __forceinline__ void far_fix_unit(const FarArgs &a, int f, int chunk,
         S.corr[2 * j + 1][tid] = 0ull;
     }
     S.npyz[tid] = make_float2(-frame_point_coord(L.ty, a.spacing_adiv), -frame_point_coord(L.tz, a.spacing_adiv));
+    if (tid < FRAME_X + FRAME_Y + FRAME_Z) {
+        const int i = tid < FRAME_X ? ox + tid - a.nex
+                    : tid < FRAME_X + FRAME_Y ? oy + (tid - FRAME_X) - a.ney : oz + (tid - FRAME_X - FRAME_Y) - a.nez;
+        S.pc[tid] = __dmul_rn((double)i, a.spacing_adiv);
+    }
     if (tid < 3) S.cnt[tid] = 0u;
     __syncthreads();
     const int a_begin = chunk * a.chunk_atoms;
