@@ -109,3 +109,33 @@ def test_spacing_with_inexact_frame_coordinates(tmp_path, gpu_ctx):
     pts = np.unique(rng.integers(0, prob.points, 3000)).astype(np.int64)
     tot = check_bins(gpu_ctx, prob, pts)
     assert tot["owned"] > 0
+
+
+def test_clamped_far_table(tmp_path, gpu_ctx):
+    """A 60 A receptor with the box near its edge: atom-point distances from a
+    few A to ~135 A, beyond the longest extended far table (FAR_TAB_MAX bins,
+    128 A), so the far kernel clamps t at the last bin, as the reference's
+    min(lookup(r), NDIEL - 1) does.  Bins and the e map still match the
+    reference expression and the oracle."""
+    import os
+    from conftest import tolerance_ok
+    from autogrid_b200 import Job, synth
+    from oracle.oracle import oracle_points
+    rec = synth.make_receptor(700, seed=11, radius=60.0, center=(0.0, 0.0, 0.0))
+    spec = synth.GridSpec(npts=(10, 12, 8), center=(76.0, 5.0, -3.0))
+    gpf = synth.write_case(tmp_path, "clamp", rec, spec)
+    cwd = os.getcwd()
+    os.chdir(tmp_path)
+    try:
+        prob = Job(gpf.name, None).problem()
+    finally:
+        os.chdir(cwd)
+    coord = prob.arrays["coord"].reshape(-1, 3)  # relative to the grid centre
+    dmax = float(np.max(np.linalg.norm(coord, axis=1)))
+    assert dmax > 132.0  # the extended table would need more than FAR_TAB_MAX (16,384) bins
+    pts = np.arange(prob.points, dtype=np.int64)
+    tot = check_bins(gpu_ctx, prob, pts)
+    assert tot["owned"] > 0 and tot["flagged"] > 0
+    maps = gpu_ctx.compute(prob, "fp32").reshape(prob.n_maps, -1)
+    ref, flags = oracle_points(prob)
+    assert (tolerance_ok(maps, ref) | (flags[None, :] != 0)).all()

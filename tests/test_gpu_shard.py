@@ -84,3 +84,22 @@ def test_sharded_adjoint_gradients_sum_to_whole(tmp_path, gpu_ctx):
         sq += b
     assert np.abs(sc - gc).max() <= 1e-10 * np.abs(gc).max()
     assert np.abs(sq - gq).max() <= 1e-10 * np.abs(gq).max()
+
+
+def test_collision_mode_zslabs_equal_one_shot(tmp_path, gpu_ctx):
+    """'map_receptor_interior off' on z-slabs: the collision rule runs on each
+    slab's planes, so the slabs (energy maps, floating and constriction grids)
+    equal the one-shot call's planes bit for bit."""
+    from autogrid_b200.shard import stitch_zslabs, zslab_ranges
+    _, prob = make_case(tmp_path, "coll", 900, (14, 12, 26), seed=23, radius=11.0,
+                        ligand_types=["A", "C", "HD", "OA"],
+                        extra_lines=["map_receptor_interior off", "fmap c.f.map", "constriction_distance_cutoff 5.5",
+                                     "cmap c.c.map"])
+    assert int(prob.scalars.get("report_collisions", 0)) == 1 and prob.n_out == prob.n_maps + 2
+    whole = gpu_ctx.compute(prob, "fp32")
+    e = int(prob.scalars["elec_map"])
+    assert (whole[e] == 0).any()  # some points collide
+    ranges = zslab_ranges(prob.n1[2], 2)
+    slabs = [gpu_ctx.compute_zslab(prob, z0, z1) for z0, z1 in ranges]
+    got = stitch_zslabs(slabs, ranges, prob.n_out, prob.n1)
+    assert np.array_equal(got, whole)
