@@ -402,8 +402,10 @@ __device__ __forceinline__ void far_fix_item(const FarArgs &a, FixSmem &S, uint3
         const float used = __ldg(a.far_tab + kb);
         const float dT = __fsub_rn(__ldg(a.tab_full + min(kx, AG_NDIEL - 1)), used);
         if (dT != 0.f) {
-            const double v = (double)__fmul_rn(__fmul_rn(qa, rs), dT) * FX_SCALE;
-            atomicAdd(&S.corr[sl][owner], (unsigned long long)__double2ll_rn(v));
+            // scaling by 2^40 is exact in FP32 as in FP64 (no overflow or
+            // underflow at these magnitudes), so the float product is rounded once
+            const float v = __fmul_rn(__fmul_rn(__fmul_rn(qa, rs), dT), (float)FX_SCALE);
+            atomicAdd(&S.corr[sl][owner], (unsigned long long)__float2ll_rn(v));
         }
     }
 }
@@ -458,8 +460,8 @@ __device__ __forceinline__ void far_fix_unit(const FarArgs &a, int f, int chunk,
                     list[nlist + __popc(have & below)] = ((uint32_t)(32 * k + b) << 8) | (uint32_t)tid;
                 }
                 nlist += __popc(have);
-                __syncwarp();
-                if (nlist >= 32) {
+                if (nlist >= 32) {  // warp-uniform; the appends become visible here
+                    __syncwarp();
                     far_fix_item<NJ, CLAMP>(a, S, list[lane], a_begin, ox, oy, oz, X0, Y0, Z0, cnt);
                     nlist -= 32;
                     const uint32_t rest = lane < nlist ? list[32 + lane] : 0u;
@@ -469,6 +471,7 @@ __device__ __forceinline__ void far_fix_unit(const FarArgs &a, int f, int chunk,
                 }
             }
         }
+        __syncwarp();
         if (lane < nlist) far_fix_item<NJ, CLAMP>(a, S, list[lane], a_begin, ox, oy, oz, X0, Y0, Z0, cnt);
     }
     __syncwarp();
