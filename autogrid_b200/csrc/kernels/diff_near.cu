@@ -390,7 +390,12 @@ __global__ void __launch_bounds__(CH_THREADS) k_closest_h(DiffArgs a, int *__res
     const int ix = (int)(l % a.n1x), iy = (int)((l / a.n1x) % a.n1y), iz = (int)(l / ((long long)a.n1x * a.n1y));
     const double cx = (double)(ix - a.nex) * a.spacing, cy = (double)(iy - a.ney) * a.spacing,
                  cz = (double)(iz - a.nez) * a.spacing;
-    double rmin = 999999.;
+    // The reference keeps the first H atom in file order with the strictly
+    // smallest r = sqrt(d0^2 + d1^2 + d2^2).  sqrt is monotonic, so only a
+    // strictly smaller square can give a strictly smaller r; when the squares
+    // differ by more than 2^-48 relative, the correctly rounded roots differ
+    // too, and only closer squares need the roots themselves compared.
+    double best2 = 999999. * 999999.;  // rmin = 999999, exactly
     int best = -1;
     for (int h0 = 0; h0 < a.n_h; h0 += CH_THREADS) {
         const int nh = min(CH_THREADS, a.n_h - h0);
@@ -403,8 +408,12 @@ __global__ void __launch_bounds__(CH_THREADS) k_closest_h(DiffArgs a, int *__res
         __syncthreads();
         for (int j = 0; j < nh; j++) {
             const double d0 = __dsub_rn(sx[j], cx), d1 = __dsub_rn(sy[j], cy), d2 = __dsub_rn(sz[j], cz);
-            const double r = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2)));
-            if (r < rmin) { rmin = r; best = sidx[j]; }
+            const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(d0, d0), __dmul_rn(d1, d1)), __dmul_rn(d2, d2));
+            if (r2 < best2 &&
+                (best2 - r2 > best2 * 3.552713678800501e-15 /* 2^-48 */ || __dsqrt_rn(r2) < __dsqrt_rn(best2))) {
+                best2 = r2;
+                best = sidx[j];
+            }
         }
     }
     if (valid) ch[lin] = best;
