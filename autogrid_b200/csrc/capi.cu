@@ -1186,9 +1186,12 @@ ag_status batch_launch(ag_batch *b, cudaStream_t s, int tile, int shape, cudaEve
     }
     if (far && concurrent) AGB_CK(cudaEventRecord(c->join, fs));
     if (e1) AGB_CK(cudaEventRecord(e1, s));
-    if (b->near_begin.back() > 0)
+    if (b->near_begin.back() > 0) {
+        int max_ng = 0;
+        for (const NearInst &ni : b->near) max_ng = std::max(max_ng, ni.g.ng);
         AGB_CK(launch_near_batch(b->d_near, b->d_near_begin, (int)b->near.size(), b->d_counters + 1, shape,
-                                 b->near_ctas_per_sm, s));
+                                 b->near_ctas_per_sm, max_ng, s));
+    }
     if (far && concurrent) AGB_CK(cudaStreamWaitEvent(s, c->join, 0));
     if (!b->red.empty())
         AGB_CK(launch_emap_reduce(b->d_red, b->d_red_begin, (int)b->red.size(), b->red_begin.back(), s));

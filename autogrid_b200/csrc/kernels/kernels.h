@@ -83,8 +83,9 @@ cudaError_t launch_fmap_adjoint(const DevProblem &p, const void *g_fmap, bool fp
 int near_bricks(const DevProblem &p, int shape);
 cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int shape,
                         cudaStream_t s, int bz0 = 0, int bz1 = -1);
+// max_ng: the most maps any instance's group holds (picks the accumulator count)
 cudaError_t launch_near_batch(const NearInst *insts, const long long *unit_begin, int n_inst,
-                              unsigned long long *counter, int shape, int ctas_per_sm, cudaStream_t s);
+                              unsigned long long *counter, int shape, int ctas_per_sm, int max_ng, cudaStream_t s);
 int frames_x(int n1x);
 int frames_y(int n1y);
 int frames_z(int n1z);

@@ -290,13 +290,13 @@ __device__ __forceinline__ double h_dist(const DevProblem &p, int a, double cx, 
 // IEEE addition as a scalar one, so the sums are unchanged.  Indices are
 // compile-time constants wherever the kernels use them (unrolled loops), so
 // the accumulators stay in registers.
-template <class R>
+template <class R, int NGK>
 struct MapAcc {
-    R v[NG_MAX];
+    R v[NGK];
     __device__ __forceinline__ void zero()
     {
 #pragma unroll
-        for (int m = 0; m < NG_MAX; m++) v[m] = (R)0;
+        for (int m = 0; m < NGK; m++) v[m] = (R)0;
     }
     __device__ __forceinline__ R get(int m) const { return v[m]; }
     __device__ __forceinline__ void add(int m, R x) { v[m] += x; }
@@ -306,13 +306,13 @@ struct MapAcc {
         v[4 * m4 + 2] += (R)T.z; v[4 * m4 + 3] += (R)T.w;
     }
 };
-template <>
-struct MapAcc<float> {
-    float2 v[NG_MAX / 2];
+template <int NGK>
+struct MapAcc<float, NGK> {
+    float2 v[NGK / 2];
     __device__ __forceinline__ void zero()
     {
 #pragma unroll
-        for (int k = 0; k < NG_MAX / 2; k++) v[k] = make_float2(0.f, 0.f);
+        for (int k = 0; k < NGK / 2; k++) v[k] = make_float2(0.f, 0.f);
     }
     __device__ __forceinline__ float get(int m) const { return (m & 1) ? v[m >> 1].y : v[m >> 1].x; }
     __device__ __forceinline__ void add(int m, float x)
@@ -327,8 +327,13 @@ struct MapAcc<float> {
     }
 };
 
+// Accumulators a launch holds per point: groups of at most 8 maps (the
+// 8-map sets of batched ensembles, config 0) run with 8, which frees 8 of
+// the 80 registers; larger groups with NG_MAX.
+constexpr int NGK_SMALL = 8;
+
 // One brick `b` of one instance (p, g).
-template <bool EXACT, int BX, int BY, int BZ>
+template <bool EXACT, int BX, int BY, int BZ, int NGK>
 __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &g, const NearPtrs &ptr, int b,
                                           NearSmem &S)
 {
@@ -495,7 +500,8 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     if (!EXACT && ch >= 0) rvh = make_float3(ptr.atomA[ch].x, ptr.atomA[ch].y, ptr.atomA[ch].z);
 
     // ---- B: pair terms
-    MapAcc<R> E;
+    static_assert(NGK % 4 == 0 && NGK >= NG_MM && NGK <= NG_MAX, "accumulator count");
+    MapAcc<R, NGK> E;
     R hmin[NG_MM], hmax[NG_MM];  // the FP64 twin only; FP32 keeps them in S
     E.zero();
 #pragma unroll
@@ -621,7 +627,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                     ? (const float4 *)(ptr.vdwT + ((size_t)p.hydrogen_type * AG_NEINT + q.ih) * ptr.mpad + g.col0) : Trow;
                 if ((g.plain_hb >> hb) & 1u) {  // every map a plain sum for this class (most atoms)
 #pragma unroll
-                    for (int m4 = 0; m4 < NG_MAX / 4; m4++) {
+                    for (int m4 = 0; m4 < NGK / 4; m4++) {
                         if (4 * m4 >= g.ng) break;
                         const float4 T4 = __ldg(Trow + m4);
                         E.add4(m4, T4);
@@ -630,7 +636,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                 }
                 const unsigned long long aw = g.actw[hb];
 #pragma unroll
-                for (int m4 = 0; m4 < NG_MAX / 4; m4++) {
+                for (int m4 = 0; m4 < NGK / 4; m4++) {
                     if (4 * m4 >= g.ng) break;
                     const float4 T4 = __ldg(Trow + m4);
                     float4 H4 = T4;
@@ -674,7 +680,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     // finalise (main.cpp:3420-3431) and store
     if (valid) {
 #pragma unroll
-        for (int m = 0; m < NG_MAX; m++) {
+        for (int m = 0; m < NGK; m++) {
             if (m >= g.ng) break;
             R v = E.get(m);
             if (m < NG_MM && (hflag & (1u << m))) {
@@ -709,7 +715,7 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
 }
 
 // Single instance: one CTA per brick.
-template <bool EXACT, int BX, int BY, int BZ>
+template <bool EXACT, int BX, int BY, int BZ, int NGK>
 __global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS) k_near(DevProblem p, NearGroup g, NearPtrs ptr,
                                                                   int brick0)
 {
@@ -720,12 +726,12 @@ __global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS) k_near(DevProblem p
     __shared__ DevProblem s_p;
     if (threadIdx.x == 0) s_p = p;
     __syncthreads();
-    near_unit<EXACT, BX, BY, BZ>(s_p, g, ptr, brick0 + blockIdx.x, S);
+    near_unit<EXACT, BX, BY, BZ, NGK>(s_p, g, ptr, brick0 + blockIdx.x, S);
 }
 
 // Many instances, persistent: (instance-group, brick) units from an atomic
 // counter; units never wait on each other.
-template <int BX, int BY, int BZ>
+template <int BX, int BY, int BZ, int NGK>
 __global__ void __launch_bounds__(NB_THREADS, NEAR_MIN_CTAS)
 k_near_batch(const NearInst *__restrict__ insts, const long long *__restrict__ unit_begin, int n_inst,
              unsigned long long *__restrict__ counter)
@@ -753,7 +759,7 @@ k_near_batch(const NearInst *__restrict__ insts, const long long *__restrict__ u
             __syncthreads();
             cur = lo;
         }
-        near_unit<false, BX, BY, BZ>(s_i.p, s_i.g, s_i.ptr, (int)(u - unit_begin[lo]), S);
+        near_unit<false, BX, BY, BZ, NGK>(s_i.p, s_i.g, s_i.ptr, (int)(u - unit_begin[lo]), S);
     }
 }
 
@@ -802,37 +808,50 @@ cudaError_t launch_near(bool exact, const DevProblem &p, const NearGroup &g, con
     if (bz0 >= bz1) return cudaSuccess;
     const unsigned nb = (unsigned)(nbx * nby * (bz1 - bz0));
     const int b0 = bz0 * nbx * nby;
+    const bool small = g.ng <= NGK_SMALL;
     if (exact) {
-        k_near<true, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
+        k_near<true, 8, 8, 4, NG_MAX><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     } else if (shape == 1) {
-        k_near<false, 8, 4, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
+        if (small) k_near<false, 8, 4, 8, NGK_SMALL><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
+        else k_near<false, 8, 4, 8, NG_MAX><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     } else if (shape == 2) {
-        k_near<false, 4, 8, 8><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
+        if (small) k_near<false, 4, 8, 8, NGK_SMALL><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
+        else k_near<false, 4, 8, 8, NG_MAX><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     } else {
-        k_near<false, 8, 8, 4><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
+        if (small) k_near<false, 8, 8, 4, NGK_SMALL><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
+        else k_near<false, 8, 8, 4, NG_MAX><<<nb, NB_THREADS, 0, s>>>(p, g, ptr, b0);
     }
     return cudaGetLastError();
 }
 
-template <int BX, int BY, int BZ>
+template <int BX, int BY, int BZ, int NGK>
 static cudaError_t near_batch_t(const NearInst *insts, const long long *unit_begin, int n_inst,
                                 unsigned long long *counter, int ctas_per_sm, cudaStream_t s)
 {
     int dev = 0, sms = 0, occ = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_near_batch<BX, BY, BZ>, NB_THREADS, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_near_batch<BX, BY, BZ, NGK>, NB_THREADS, 0);
     const int per_sm = std::max(1, std::min(ctas_per_sm, occ));
-    k_near_batch<BX, BY, BZ><<<sms * per_sm, NB_THREADS, 0, s>>>(insts, unit_begin, n_inst, counter);
+    k_near_batch<BX, BY, BZ, NGK><<<sms * per_sm, NB_THREADS, 0, s>>>(insts, unit_begin, n_inst, counter);
     return cudaGetLastError();
 }
 
-cudaError_t launch_near_batch(const NearInst *insts, const long long *unit_begin, int n_inst,
-                              unsigned long long *counter, int shape, int ctas_per_sm, cudaStream_t s)
+template <int NGK>
+static cudaError_t near_batch_shape(const NearInst *insts, const long long *unit_begin, int n_inst,
+                                    unsigned long long *counter, int shape, int ctas_per_sm, cudaStream_t s)
 {
-    if (shape == 1) return near_batch_t<8, 4, 8>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
-    if (shape == 2) return near_batch_t<4, 8, 8>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
-    return near_batch_t<8, 8, 4>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+    if (shape == 1) return near_batch_t<8, 4, 8, NGK>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+    if (shape == 2) return near_batch_t<4, 8, 8, NGK>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+    return near_batch_t<8, 8, 4, NGK>(insts, unit_begin, n_inst, counter, ctas_per_sm, s);
+}
+
+cudaError_t launch_near_batch(const NearInst *insts, const long long *unit_begin, int n_inst,
+                              unsigned long long *counter, int shape, int ctas_per_sm, int max_ng, cudaStream_t s)
+{
+    if (max_ng <= NGK_SMALL)
+        return near_batch_shape<NGK_SMALL>(insts, unit_begin, n_inst, counter, shape, ctas_per_sm, s);
+    return near_batch_shape<NG_MAX>(insts, unit_begin, n_inst, counter, shape, ctas_per_sm, s);
 }
 
 }  // namespace agb
