@@ -31,6 +31,7 @@ struct NearSmem {
     // in shared memory, out of the pair loop's 80-register budget)
     float hmin[NG_MM][NB_THREADS_MAX], hmax[NG_MM][NB_THREADS_MAX];
     int seg_start[NB_SEGS_MAX], seg_off[NB_SEGS_MAX + 1];
+    int tcnt[NB_CHUNK_MAX / 32][32];  // staging by receptor type: per 32-candidate slice and type
     int total;
 };
 

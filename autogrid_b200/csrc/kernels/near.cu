@@ -278,7 +278,8 @@ __device__ __forceinline__ double h_dist(const DevProblem &p, int a, double cx, 
 // ----------------------------------------------------------------- near ---
 // One thread per grid point; bricks of 8x8x4 points inside one far-field frame.
 //  stage  candidate atoms of the cells within 8.05 A of the brick, with their
-//         canonical frame-relative FP32 coordinates and packed metadata
+//         canonical frame-relative FP32 coordinates and packed metadata,
+//         ordered by receptor type (cell order within a type)
 //  A      closest DS/D1 atom per point among the candidates (any DS/D1 atom
 //         within 8.05 A of the point is a candidate, so a best distance
 //         <= 8 A is the global minimum); FP32 prefilter, then FP64 with the
@@ -386,22 +387,66 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     const int nrow_y = cyh - cyl + 1;
     const int nseg_total = (need_pairs || need_h) ? nrow_y * (czh - czl + 1) : 0;
 
-    // Stage chunk `c0` of segment batch `sb` (the caller has laid out s_seg_*).
+    // Stage chunk `c0` (nc candidates) of the laid-out segments, ordered by
+    // receptor type by a stable counting sort (cell order within a type), so
+    // that a warp's consecutive pairs read the table rows of one type, which
+    // then stay in L1.  Slice k (candidates [32k, 32k + 32) of the chunk) is
+    // ranked by one warp; S.tcnt[k][t] holds the slice's count of type t,
+    // then the slot of its first such candidate.  All threads call it.
+    static_assert(NB_CHUNK <= 2 * NB_THREADS && NB_CHUNK % 32 == 0, "two candidates per thread at most");
     auto stage = [&](int c0, int nc) {
-        for (int i = tid; i < nc; i += NB_THREADS) {
-            const int c = c0 + i;
-            int s = 0;
-            while (S.seg_off[s + 1] <= c) s++;
-            const int a = p.cell_atoms[S.seg_start[s] + (c - S.seg_off[s])];
-            S.idx[i] = a;
-            S.pos[i] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0), frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
+        constexpr int NSL = NB_CHUNK / 32;
+        for (int i = tid; i < NSL * 32; i += NB_THREADS) S.tcnt[i >> 5][i & 31] = 0;
+        __syncthreads();
+        int ca[2], ct[2], cr[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = u * NB_THREADS + tid;
+            int a = -1, t = 32;  // lanes past the chunk form a group of their own
+            if (i < nc) {
+                const int c = c0 + i;
+                int s = 0;
+                while (S.seg_off[s + 1] <= c) s++;
+                a = p.cell_atoms[S.seg_start[s] + (c - S.seg_off[s])];
+                t = ptr.meta[a] & META_TYPE_MASK;
+            }
+            const unsigned same = __match_any_sync(0xffffffffu, t);
+            cr[u] = __popc(same & ((1u << (tid & 31)) - 1u));
+            if (i < nc && cr[u] == 0) S.tcnt[i >> 5][t] = __popc(same);
+            ca[u] = a;
+            ct[u] = t;
+        }
+        __syncthreads();
+        if (tid < 32) {  // thread t: type t's slots, slices in order, after every lower type
+            int run = 0;
+            for (int k = 0; k < NSL; k++) {
+                const int c = S.tcnt[k][tid];
+                S.tcnt[k][tid] = run;
+                run += c;
+            }
+            int incl = run;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (tid >= o) incl += v;
+            }
+            for (int k = 0; k < NSL; k++) S.tcnt[k][tid] += incl - run;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+            const int i = u * NB_THREADS + tid;
+            if (i >= nc) continue;
+            const int a = ca[u], j = S.tcnt[i >> 5][ct[u]] + cr[u];
+            S.idx[j] = a;
+            S.pos[j] = make_float4(frame_atom_coord(p.x[a] * AG_A_DIV, X0), frame_atom_coord(p.y[a] * AG_A_DIV, Y0),
                                    frame_atom_coord(p.z[a] * AG_A_DIV, Z0), (float)p.q[a]);
-            S.a[i] = ptr.atomA[a];
-            S.b[i] = ptr.atomB[a];
+            S.a[j] = ptr.atomA[a];
+            S.b[j] = ptr.atomB[a];
             const int m = ptr.meta[a];
-            S.meta[i] = m;
+            S.meta[j] = m;
             const int hb = (m >> META_HB_SHIFT) & 7;
-            if (hb == 1 || hb == 2) S.hl[atomicAdd(&S.nh, 1)] = i;
+            if (hb == 1 || hb == 2) S.hl[atomicAdd(&S.nh, 1)] = j;
         }
     };
     auto layout_segments = [&](int sb, int nseg) {
