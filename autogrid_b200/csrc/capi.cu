@@ -642,6 +642,14 @@ ag_status build_plan(ag_plan *pl, const ag_problem *p, cudaStream_t s, bool pipe
                 plain &= (a == ACT_PLAIN || a == ACT_SKIP);
             }
             if (plain) g.plain_hb |= 1u << hb;
+            for (int r = 0; r < NG_MAX / 4; r++) {
+                bool row_plain = true;
+                for (int k = 4 * r; k < 4 * r + 4 && k < g.ng; k++) {
+                    const int a = (int)((g.actw[hb] >> (3 * k)) & 7ull);
+                    row_plain &= (a == ACT_PLAIN || a == ACT_SKIP);
+                }
+                if (row_plain) g.plain4 |= 1u << (4 * hb + r);
+            }
         }
         pl->groups.push_back(g);
     } while (im < mm_maps.size() || ip < plain_maps.size());

@@ -507,30 +507,49 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
     // ---- A: closest DS/D1 hydrogen (main.cpp:2986-3015)
     int ch = -1;
     if (need_h) {
-        float best2 = 3.0e38f;
+        // FP32 prefilter: the two smallest squared distances (bins^2) and the
+        // atom of the smallest.  Every candidate within `lim` of the smallest
+        // is re-checked in FP64; when the second smallest lies beyond `lim`,
+        // that is the smallest's atom alone, and the FP64 pass over the
+        // candidates reduces to its own distance.
+        float best2 = 3.0e38f, next2 = 3.0e38f;
+        int best_a = -1;
         for_each_chunk([&](int) {
             if (!valid) return;
             for (int k = 0; k < S.nh; k++) {
                 const int j = S.hl[k];
                 const float4 A = S.pos[j];
                 const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
-                best2 = fminf(best2, dx * dx + dy * dy + dz * dz);
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 < best2) {
+                    next2 = best2;
+                    best2 = d2;
+                    best_a = S.idx[j];
+                } else {
+                    next2 = fminf(next2, d2);
+                }
             }
         });
         const float lim = best2 * (1.0f + 2.0e-5f) + 4.0f;
         double rmin = 999999.;
-        for_each_chunk([&](int) {
-            if (!valid) return;
-            for (int k = 0; k < S.nh; k++) {
-                const int j = S.hl[k];
-                const float4 A = S.pos[j];
-                const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
-                if (dx * dx + dy * dy + dz * dz > lim) continue;
-                const int a = S.idx[j];
-                const double r = h_dist(p, a, cx(), cy(), cz());
-                if (r < rmin || (r == rmin && a < ch)) { rmin = r; ch = a; }
-            }
-        });
+        const bool several = valid && best_a >= 0 && next2 <= lim;
+        if (valid && best_a >= 0 && !several) {
+            rmin = h_dist(p, best_a, cx(), cy(), cz());
+            ch = best_a;
+        }
+        if (__syncthreads_or(several))
+            for_each_chunk([&](int) {
+                if (!several) return;
+                for (int k = 0; k < S.nh; k++) {
+                    const int j = S.hl[k];
+                    const float4 A = S.pos[j];
+                    const float dx = A.x - PX, dy = A.y - PY, dz = A.z - PZ;
+                    if (dx * dx + dy * dy + dz * dz > lim) continue;
+                    const int a = S.idx[j];
+                    const double r = h_dist(p, a, cx(), cy(), cz());
+                    if (r < rmin || (r == rmin && a < ch)) { rmin = r; ch = a; }
+                }
+            });
         if (valid && !(rmin <= AG_NBC)) {  // nothing within 8 A: scan every DS/D1 atom in file order
             rmin = 999999.;
             ch = -1;
@@ -680,10 +699,15 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                     continue;
                 }
                 const unsigned long long aw = g.actw[hb];
+                const unsigned rows_plain = g.plain4 >> (4 * hb);
 #pragma unroll
                 for (int m4 = 0; m4 < NGK / 4; m4++) {
                     if (4 * m4 >= g.ng) break;
                     const float4 T4 = __ldg(Trow + m4);
+                    if ((rows_plain >> m4) & 1u) {  // the same adds as the per-map chain below
+                        E.add4(m4, T4);
+                        continue;
+                    }
                     float4 H4 = T4;
                     if (dis) H4 = __ldg(Hrow + m4);
                     const float Tv[4] = {T4.x, T4.y, T4.z, T4.w};

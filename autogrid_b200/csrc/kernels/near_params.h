@@ -32,6 +32,8 @@ struct NearGroup {
     unsigned long long actw[8];  // per receptor hbond class: 3-bit action of kernel map m at bits 3m..3m+2
     unsigned plain_hb;         // bit hb: every map of this launch is ACT_PLAIN or ACT_SKIP for class hb
                                // (the table columns of ACT_SKIP maps are zero, so all T can be added)
+    unsigned plain4;           // bit 4*hb + r: kernel maps 4r..4r+3 (one 16-byte table row) are all
+                               // ACT_PLAIN or ACT_SKIP for class hb, so the row adds as a whole
     int out_map[NG_MAX];       // output map index of kernel map m
     uint8_t cov[NG_MAX];
     double sp[NG_MAX], vp[NG_MAX];  // desolvation factors applied to this map's output
