@@ -57,6 +57,16 @@ __device__ __forceinline__ float rsqrt_approx(float x)
     return y;
 }
 
+// Square root of x >= 0 by the hardware approximation (one MUFU operation,
+// a few ulp; sqrt(0) = 0).  Used for the directional factors of H-bond
+// pairs, which are continuous where it is used.
+__device__ __forceinline__ float sqrt_approx(float x)
+{
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // The far kernel's distance (in bins) of a pair, from frame-relative FP32
 // inputs.  Written with explicit round-to-nearest intrinsics so no contraction
 // or reassociation can make two call sites differ.

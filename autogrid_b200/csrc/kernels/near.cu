@@ -227,7 +227,9 @@ __device__ __forceinline__ bool angular_fast(int meta, float4 rvA, float4 rvB, i
             if (ia != ch && ch >= 0) {
                 float ct = rvh.x * rv0 + rvh.y * rv1 + rvh.z * rv2;
                 ct = fminf(fmaxf(ct, -1.f), 1.f);
-                o.Hramp = 0.5f - 0.5f * cosf(acosf(ct) * (120.f / 90.f));
+                // 0.5 - 0.5 cos(x) = 0.5 + 0.5 cos(x - pi), x - pi in [-pi, pi/3]: the
+                // range on which __cosf's absolute error is within 2^-21.4
+                o.Hramp = 0.5f + 0.5f * __cosf(acosf(ct) * (120.f / 90.f) - 3.14159265f);
             }
         }
     } else if (hb == 4) {
@@ -238,7 +240,7 @@ __device__ __forceinline__ bool angular_fast(int meta, float4 rvA, float4 rvB, i
         float t0 = dn0 * w0 + dn1 * w1 + dn2 * w2;
         t0 = fminf(fmaxf(t0, -1.f), 1.f);
         // cos(pi/2 - acos(t0)) = sqrt(1 - t0^2)
-        const float cos_t0 = sqrtf(fmaxf(1.f - t0 * t0, 0.f));
+        const float cos_t0 = sqrt_approx(fmaxf(1.f - t0 * t0, 0.f));
         const float c0 = dn1 * w2 - dn2 * w1, c1 = dn2 * w0 - dn0 * w2, c2 = dn0 * w1 - dn1 * w0;
         float rd2 = c0 * c0 + c1 * c1 + c2 * c2;
         rd2 = fmaxf(rd2, 1.0e-6f);
@@ -248,7 +250,7 @@ __device__ __forceinline__ bool angular_fast(int meta, float4 rvA, float4 rvB, i
         if (cos_theta >= 0.f) {
             ti = fminf(fmaxf(ti, -1.f), 1.f);
             // sin(2|acos(ti) - pi/2|) = |sin(2 acos(ti))| = 2|ti|sqrt(1 - ti^2)
-            const float s2 = 2.f * fabsf(ti) * sqrtf(fmaxf(1.f - ti * ti, 0.f));
+            const float s2 = 2.f * fabsf(ti) * sqrt_approx(fmaxf(1.f - ti * ti, 0.f));
             o.rdon = (0.9f + 0.1f * s2) * cos_t0;
         } else if (cos_theta >= -0.34202f) {
             const float b = 0.116978f - cos_theta * cos_theta;
@@ -719,7 +721,8 @@ __device__ __forceinline__ void near_unit(const DevProblem &p, const NearGroup &
                         if (act == ACT_SKIP) continue;
                         const R T = (R)Tv[u];
                         if (act == ACT_PLAIN) { E.add(m, T); continue; }
-                        R rsph = T / (R)100.;
+                        // FP32: a product with 0.01f (within 1.5 ulp of the quotient)
+                        R rsph = EXACT ? T / (R)100. : T * (R)0.01f;
                         rsph = rsph > (R)0 ? rsph : (R)0;
                         rsph = rsph < (R)1 ? rsph : (R)1;
                         if (act == ACT_SUMA) {
