@@ -43,6 +43,42 @@ DF_HD float sin43(float x)
 #endif
 }
 DF_HD double sin43(double x) { return sin(x); }
+// Square root, reciprocal square root and quotient inside the directional
+// factors, which are continuous where these are used.  FP32 on the device:
+// the hardware approximations (sqrt.approx, rsqrt.approx: a few ulp;
+// __fdividef: 2 ulp for the divisors here, all above 1e-6); elsewhere the
+// correctly rounded operations.
+DF_HD float asqrt(float v)
+{
+#ifdef __CUDA_ARCH__
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(v));
+    return y;
+#else
+    return sqrtf(v);
+#endif
+}
+DF_HD double asqrt(double v) { return sqrt(v); }
+DF_HD float arsqrt(float v)
+{
+#ifdef __CUDA_ARCH__
+    float y;
+    asm("rsqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(v));
+    return y;
+#else
+    return 1.0f / sqrtf(v);
+#endif
+}
+DF_HD double arsqrt(double v) { return 1.0 / sqrt(v); }
+DF_HD float adiv(float a, float b)
+{
+#ifdef __CUDA_ARCH__
+    return __fdividef(a, b);
+#else
+    return a / b;
+#endif
+}
+DF_HD double adiv(double a, double b) { return a / b; }
 template <class R> DF_HD R mn(R a, R b) { return a < b ? a : b; }
 template <class R> DF_HD R mx(R a, R b) { return a > b ? a : b; }
 template <class R> DF_HD R ab(R a) { return a < R(0) ? -a : a; }
@@ -95,8 +131,8 @@ DF_HD void angular(int hb, int rexp, bool dis, bool ramp, const R dn[3], const R
             const R th = acos_(ct);
             o.H = R(0.5) - R(0.5) * cos43(th * R(4.0 / 3.0));
             if (inside) {
-                const R s = sqrt_(R(1) - ct * ct);
-                o.dH_ct = (s > R(DF_TINY)) ? R(-2.0 / 3.0) * sin43(th * R(4.0 / 3.0)) / s
+                const R s = asqrt(R(1) - ct * ct);
+                o.dH_ct = (s > R(DF_TINY)) ? adiv(R(-2.0 / 3.0) * sin43(th * R(4.0 / 3.0)), s)
                                            : (ct > R(0) ? R(-8.0 / 9.0) : R(0));
             }
         }
@@ -107,22 +143,22 @@ DF_HD void angular(int hb, int rexp, bool dis, bool ramp, const R dn[3], const R
         R t0 = dn[0] * rv2[0] + dn[1] * rv2[1] + dn[2] * rv2[2];
         const bool t0_in = t0 < R(1) && t0 > R(-1);
         t0 = mn(mx(t0, R(-1)), R(1));
-        const R ct0 = sqrt_(mx(R(1) - t0 * t0, R(0)));  // cos(pi/2 - acos(t0))
-        const R dct0 = (t0_in && ct0 > R(DF_TINY)) ? -t0 / ct0 : R(0);
+        const R ct0 = asqrt(mx(R(1) - t0 * t0, R(0)));  // cos(pi/2 - acos(t0))
+        const R dct0 = (t0_in && ct0 > R(DF_TINY)) ? adiv(-t0, ct0) : R(0);
         o.cr[0] = dn[1] * rv2[2] - dn[2] * rv2[1];
         o.cr[1] = dn[2] * rv2[0] - dn[0] * rv2[2];
         o.cr[2] = dn[0] * rv2[1] - dn[1] * rv2[0];
         R rd2 = o.cr[0] * o.cr[0] + o.cr[1] * o.cr[1] + o.cr[2] * o.cr[2];
         o.rd_clamped = rd2 < R(DF_TINY);
         rd2 = mx(rd2, R(DF_TINY));
-        o.rdi = R(1) / sqrt_(rd2);
+        o.rdi = arsqrt(rd2);
         o.tin = o.cr[0] * rv[0] + o.cr[1] * rv[1] + o.cr[2] * rv[2];
         R ti = o.tin * o.rdi;
         const bool ti_in = ti < R(1) && ti > R(-1);
         ti = mn(mx(ti, R(-1)), R(1));
-        const R sq = sqrt_(mx(R(1) - ti * ti, R(0)));
+        const R sq = asqrt(mx(R(1) - ti * ti, R(0)));
         const R s2 = R(2) * ab(ti) * sq;  // sin(2 |acos(ti) - pi/2|)
-        const R ds2 = (ti_in && sq > R(DF_TINY)) ? (ti >= R(0) ? R(2) : R(-2)) * (R(1) - R(2) * ti * ti) / sq : R(0);
+        const R ds2 = (ti_in && sq > R(DF_TINY)) ? (ti >= R(0) ? R(2) : R(-2)) * adiv(R(1) - R(2) * ti * ti, sq) : R(0);
         if (c >= R(0)) {
             const R base = R(0.9) + R(0.1) * s2;
             o.rdon = base * ct0;
@@ -130,12 +166,12 @@ DF_HD void angular(int hb, int rexp, bool dis, bool ramp, const R dn[3], const R
             o.ddon_ti = R(0.1) * ds2 * ct0;
         } else if (c >= R(-0.34202)) {
             const R bb = R(0.116978) - c * c;
-            const R k = R(1) + s2 / R(9);  // continuity factor of this mode
+            const R k = R(1) + adiv(s2, R(9));  // continuity factor of this mode
             const R p3 = R(562.25) * bb * bb * bb;
             o.rdon = p3 * ct0 * k;
             o.ddon_c = R(562.25) * R(3) * bb * bb * (R(-2) * c) * ct0 * k;
             o.ddon_t0 = p3 * k * dct0;
-            o.ddon_ti = p3 * ct0 * ds2 / R(9);
+            o.ddon_ti = adiv(p3 * ct0 * ds2, R(9));
         } else {
             o.rdon = R(0);
         }
@@ -144,11 +180,11 @@ DF_HD void angular(int hb, int rexp, bool dis, bool ramp, const R dn[3], const R
         const R ct = mn(mx(c, R(-1)), R(1));
         o.racc = R(0); o.rdon = R(0);
         if (ct >= R(-A2D_SIN)) {
-            const R sq = sqrt_(mx(R(1) - ct * ct, R(0)));
+            const R sq = asqrt(mx(R(1) - ct * ct, R(0)));
             const R cc = ct * R(A2D_COS) + sq * R(A2D_SIN);  // cos(acos(ct) - 1.24791)
             const R c2 = cc * cc;
             o.rdon = o.racc = c2 * c2;
-            const R dcc = (c_in && sq > R(DF_TINY)) ? R(A2D_COS) - ct * R(A2D_SIN) / sq : R(0);
+            const R dcc = (c_in && sq > R(DF_TINY)) ? R(A2D_COS) - adiv(ct * R(A2D_SIN), sq) : R(0);
             o.dacc_c = o.ddon_c = R(4) * c2 * cc * dcc;
         }
     }
